@@ -359,3 +359,73 @@ class RefLib:
         self.lib.dref_run_samples(C.byref(cfg), _ptr(o), nthreads, nsamples, verbose,
                                   C.byref(secs), _ptr(ca), _ptr(ce), _ptr(mm), C.byref(nout))
         return secs.value, float(ca[0]), float(ce[0]), mm[: nout.value].copy()
+
+
+def orientation_solves(O: Oracle, grid, x, materials, nsamples, target=1, b_a=1.0, c_a=1.0,
+                       polarizability=1, solver=0, tau=0.0, err_max=1e-3, max_step=20,
+                       orientation=0, psi=0.0, iota=0.0, kappa=0.0, nplanes=1, theta_min=0.0,
+                       theta_max=180.0, theta_step=10.0, seed=1, occ=None, ahat=None):
+    """The reference's sample loop (main.cpp:777-986, worker 0 only) over the FP64 oracle.
+
+    Returns dict(cabs, cext, mueller) holding SUMS over samples, like the .dst state
+    (main.cpp:961-981).  Used as the CPU 'port' baseline and as the end-to-end checker.
+    """
+    ni, nj, nl = (grid, grid, grid) if np.isscalar(grid) else tuple(grid)
+    kd = 2.0 * x / ni
+    na = int(round((theta_max - theta_min) / theta_step + 1.0))
+    nrm0, ksc0 = O.scattering_geometry(nplanes, na, theta_min, theta_step)
+    if ahat is None:
+        ahat = O.green_hat(ni, nj, nl, kd)
+    if occ is None:
+        occ, _ = O.gen_ellipsoid(ni, nj, nl, 1.0 if target == 1 else b_a,
+                                 1.0 if target == 1 else c_a)
+    nmat = len(materials)
+    mv = np.array([0] + [0 if (m[0] == 1.0 and m[1] == 0.0) else 1 for m in materials], np.int32)
+    base_model = 4 if polarizability == 5 else polarizability
+    alpha0 = np.array([0] + [O.polarizability(base_model, kd, complex(*m)) for m in materials])
+    kinc0 = np.array([0.0, 0.0, 1.0])
+    einc0 = np.array([[1, 0, 0], [0, 1, 0]], np.complex128)
+    if orientation == 0:
+        def rz(a):
+            c, s = np.cos(a), np.sin(a)
+            return np.array([[c, s, 0], [-s, c, 0], [0, 0, 1]])
+
+        def ry(a):
+            c, s = np.cos(a), np.sin(a)
+            return np.array([[c, 0, -s], [0, 1, 0], [s, 0, c]])
+
+        def rx(a):
+            c, s = np.cos(a), np.sin(a)
+            return np.array([[1, 0, 0], [0, c, s], [0, -s, c]])
+        d = np.pi / 180
+        T = rx(-kappa * d) @ ry(-iota * d) @ rz(-psi * d)   # main.cpp:516-541
+        rots = [T] * nsamples
+    else:
+        rots = list(O.mc_rotations(seed, 0, nsamples))
+    cabs = cext = 0.0
+    mm_sum = np.zeros((na, 4, 4))
+    for T in rots:
+        kinc = T @ kinc0
+        einc = [T @ e for e in einc0]
+        ksc = ksc0 @ T.T
+        nrm = nrm0 @ T.T
+        esc = []
+        sa = se = 0.0
+        for q in range(2):
+            alpha = alpha0.copy()
+            if polarizability == 5:
+                alpha[1:] = [O.polarizability(5, kd, complex(*m), kinc, einc[q]) for m in materials]
+            r = O.dda_fft(occ, alpha, mv, kd, kinc, einc[q], ahat, ksc, solver=solver, tau=tau,
+                          max_step=max_step, err_max=err_max)
+            sa += 0.5 * r["cabs"]
+            se += 0.5 * r["cext"]
+            esc.append(r["esc"])
+        for a in range(na):
+            acc = np.zeros((4, 4))
+            for pl in range(nplanes):
+                acc += O.jones_mueller(kinc, ksc[pl, a], nrm[pl], einc[0], einc[1],
+                                       esc[0][pl, a], esc[1][pl, a])[1]
+            mm_sum[a] += acc / nplanes
+        cabs += sa
+        cext += se
+    return dict(cabs=cabs, cext=cext, mueller=mm_sum, n=len(rots))

@@ -1,0 +1,190 @@
+"""Generate the golden fixtures in tests/golden/ from the reference itself.
+
+Every array here is an output of physicist2018/dda-fft's own code: the float build
+(oracle/_ref/libddaref.so: the reference sources compiled where they lie, driven by
+oracle/ref_shim.cpp), its FP64 build (oracle/_ref/libddaref64.so) and its unmodified
+executable (oracle/_ref/dda_fft.out).  Run in a container that has the reference tree:
+
+    make -f oracle/Makefile all && python tests/golden/make_golden.py
+
+The fixtures are small (.npz, a few MB in all) and are committed; the tests read
+them without needing the reference.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+from pyoracle import REF64_SO, REF_EXE, RefLib, make_run_cfg  # noqa: E402
+
+
+def cplx_rand(rng, shape, dt=np.complex64):
+    return (rng.standard_normal(shape) + 1j * rng.standard_normal(shape)).astype(dt)
+
+
+def fft_lines(R, out):
+    rng = np.random.default_rng(101)
+    for N in (8, 16, 32, 64, 128, 256):
+        x = cplx_rand(rng, (N, 3))
+        out[f"fft{N}_in"] = x
+        for kind, name in ((0, "fwd"), (1, "inv"), (2, "legacy_fwd"), (3, "legacy_inv")):
+            out[f"fft{N}_{name}"] = R.fft_line(x, kind)
+
+
+def convolutions(R, R64, out):
+    rng = np.random.default_rng(202)
+    for n, x in ((8, 2.0), (16, 3.0)):
+        kd = 2 * x / n
+        A = R.green(n, n, n, kd)
+        p = cplx_rand(rng, (n, n, n, 3))
+        out[f"conv{n}_kd"] = kd
+        out[f"conv{n}_p"] = p
+        out[f"conv{n}_out"] = R.convolution(A, p)
+        out[f"conv{n}_out_conj"] = R.convolution(A, p, conj=True)
+        out[f"conv{n}_out64"] = R64.convolution(R64.green(n, n, n, kd), p.astype(np.complex128))
+        if n == 8:
+            out["green8_hat"] = A
+            out["green8_hat64"] = R64.green(n, n, n, kd)
+            out["green8_real"] = R.green_realspace(n, n, n, kd)
+    # a non-cubic lattice (the reference's test matrix includes 32x64x32)
+    n3 = (8, 16, 8)
+    kd = 2 * 2.0 / n3[0]
+    p = cplx_rand(rng, n3 + (3,))
+    out["convrect_kd"] = kd
+    out["convrect_p"] = p
+    out["convrect_out"] = R.convolution(R.green(*n3, kd), p)
+
+
+def solves(R, R64, out):
+    """DDA_FFT traces for each solver on a 16^3 sphere (fixed orientation, 2 planes)."""
+    n, x, m = 16, 3.0, 1.5 + 0.01j
+    kd = 2 * x / n
+    occ, nd = R.gen_ellipsoid(n, n, n)
+    out["solve_occ"] = occ
+    out["solve_kd"] = kd
+    nP, nA = 2, 19
+    # plane geometry as main.cpp:336-387 builds it (normal y, directions in xz), in float
+    ksc = np.zeros((nP, nA, 3), np.float32)
+    nrm = np.zeros((nP, 3), np.float32)
+    for pl in range(nP):
+        ang = np.float32(pl * 180.0 / nP) * (np.pi / 180.0)
+        c, s = np.float32(np.cos(ang)), np.float32(np.sin(ang))
+        nrm[pl] = (s, c, 0.0)
+        for a in range(nA):
+            th = np.float32(10.0 * a)
+            k0 = np.array([np.sin(th * np.pi / 180), 0.0, np.cos(th * np.pi / 180)], np.float32)
+            ksc[pl, a] = (c * k0[0] + s * k0[1], -s * k0[0] + c * k0[1], k0[2])
+    out["solve_ksc"] = ksc
+    out["solve_nrm"] = nrm
+    A32 = R.green(n, n, n, kd)
+    A64 = R64.green(n, n, n, kd)
+    cases = [("cg", 0, 0.0, 1, (1, 0, 0)), ("aa", 1, 0.0, 2, (1, 0, 0)),
+             ("bicgstab", 2, 0.0, 5, (0, 1, 0)), ("simple", 3, 0.5, 3, (1, 0, 0)),
+             ("simple_div", 3, 3.0, 1, (1, 0, 0))]
+    for name, solver, tau, model, einc in cases:
+        a32 = R.polarizability(model, kd, m, (0, 0, 1), einc)
+        a64 = R64.polarizability(model, kd, m, (0, 0, 1), einc)
+        alpha32 = np.array([0, a32], np.complex64)
+        alpha64 = np.array([0, a64], np.complex128)
+        mv = np.array([0, 1], np.int32)
+        for tag, L, A, al in (("", R, A32, alpha32), ("64", R64, A64, alpha64)):
+            r = L.dda_fft(occ, al, mv, kd, (0, 0, 1), einc, A, ksc, solver=solver, tau=tau,
+                          max_step=8, err_max=1e-9)
+            out[f"solve_{name}{tag}_alpha"] = al
+            out[f"solve_{name}{tag}_trace"] = r["trace"]
+            out[f"solve_{name}{tag}_step_min"] = r["step_min"]
+            out[f"solve_{name}{tag}_p"] = r["p"]
+            out[f"solve_{name}{tag}_esc"] = r["esc"]
+            out[f"solve_{name}{tag}_cabs"] = r["cabs"]
+            out[f"solve_{name}{tag}_cext"] = r["cext"]
+        out[f"solve_{name}_cfg"] = np.array([solver, tau, model] + list(einc), np.float64)
+
+
+def jones(R, R64, out):
+    rng = np.random.default_rng(303)
+    K = 32
+    ki = rng.standard_normal((K, 3))
+    ki /= np.linalg.norm(ki, axis=1, keepdims=True)
+    ks = rng.standard_normal((K, 3))
+    ks /= np.linalg.norm(ks, axis=1, keepdims=True)
+    nv = np.cross(ki, ks)
+    nv /= np.linalg.norm(nv, axis=1, keepdims=True)
+    e = cplx_rand(rng, (K, 4, 3), np.complex128)
+    M = np.zeros((K, 4, 4))
+    M32 = np.zeros((K, 4, 4), np.float32)
+    for k in range(K):
+        M[k] = R64.jones_mueller(ki[k], ks[k], nv[k], *e[k])[1]
+        M32[k] = R.jones_mueller(ki[k], ks[k], nv[k], *e[k])[1]
+    out.update(jm_kinc=ki, jm_ksc=ks, jm_nrm=nv, jm_e=e, jm_mueller64=M, jm_mueller=M32)
+
+
+def misc(R, R64, out):
+    out["rng_seed7"] = R.rng(7, 64)
+    out["rng_seed0"] = R.rng(0, 16)
+    pols = []
+    for model in range(1, 6):
+        for m in (1.5 + 0.01j, 1.7 + 0.1j, 1.33 + 0.0j):
+            for kd in (0.125, 0.25, 0.5):
+                pols.append((model, m.real, m.imag, kd, R64.polarizability(model, kd, m, (0, 0, 1),
+                                                                        (0.6, 0.8, 0.0))))
+    out["pol_table"] = np.array([(a, b, c, d, e.real, e.imag) for a, b, c, d, e in pols])
+    occ, nd = R.gen_ellipsoid(16, 16, 16, 0.7, 0.5)
+    out["ellipsoid16_occ"] = occ
+
+
+def end_to_end(R, R64, out):
+    """Config 1 through the unmodified executable, and MC sample loops through the shim."""
+    cmd = [REF_EXE, "--target", "sphere", "--grid", "32", "-x", "2", "-m", "1.5", "0.01", "-P",
+           "cm", "-M", "cg", "-e", "1e-3", "-S", "20", "--orientation", "fixed", "--planes", "1",
+           "-a", "0", "-b", "180", "-s", "10", "--seed", "1", "--threads", "1", "--restart"]
+    with tempfile.TemporaryDirectory() as td:
+        subprocess.run(cmd + ["-o", "c1.dat", "-D", "c1.dst"], cwd=td, check=True,
+                       capture_output=True)
+        out["c1_dat"] = np.frombuffer(open(os.path.join(td, "c1.dat"), "rb").read(), np.uint8)
+        out["c1_dst"] = np.frombuffer(open(os.path.join(td, "c1.dst"), "rb").read(), np.uint8)
+    # the same configuration through the shim's sample loop (must equal the executable)
+    cfg = make_run_cfg(grid=32, target=1, x=2.0, seed=1)
+    s, ca, ce, mm = R.run_samples(cfg, 1, 1)
+    out["c1_shim"] = np.concatenate([[ca, ce], mm.ravel()])
+    # Monte-Carlo orientations of an ellipsoid, seed 7 (worker-0 stream), 16^3, x=3
+    cfg = make_run_cfg(grid=16, target=2, b_a=0.7, c_a=0.5, x=3.0, materials=((1.55, 0.005),),
+                       orientation=1, seed=7, nplanes=2, err_max=1e-3, max_step=20)
+    for ns in (1, 4):
+        s, ca, ce, mm = R.run_samples(cfg, ns, 1)
+        out[f"mc16_n{ns}"] = np.concatenate([[ca, ce], mm.ravel()])
+        s, ca, ce, mm = R64.run_samples(cfg, ns, 1)
+        out[f"mc16_n{ns}_64"] = np.concatenate([[ca, ce], mm.ravel()])
+    # LDR + BiCGStab + 3 planes at 16^3, x=4 (a small stand-in for the mid config)
+    cfg = make_run_cfg(grid=16, target=1, x=4.0, polarizability=5, solver=2, nplanes=3,
+                       theta_step=5.0, max_step=100, seed=1)
+    s, ca, ce, mm = R.run_samples(cfg, 1, 1)
+    out["ldr16"] = np.concatenate([[ca, ce], mm.ravel()])
+    s, ca, ce, mm = R64.run_samples(cfg, 1, 1)
+    out["ldr16_64"] = np.concatenate([[ca, ce], mm.ravel()])
+
+
+def main():
+    R = RefLib()
+    R64 = RefLib(REF64_SO)
+    assert R.rdt == np.float32 and R64.rdt == np.float64
+    out: dict = {}
+    fft_lines(R, out)
+    convolutions(R, R64, out)
+    solves(R, R64, out)
+    jones(R, R64, out)
+    misc(R, R64, out)
+    end_to_end(R, R64, out)
+    path = os.path.join(HERE, "reference_v72.npz")
+    np.savez_compressed(path, **out)
+    print(f"wrote {path}: {os.path.getsize(path) / 1e6:.2f} MB, {len(out)} arrays")
+
+
+if __name__ == "__main__":
+    main()
