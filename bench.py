@@ -1,0 +1,358 @@
+"""Benchmark: orientation-solves/s of the DDA-FFT hot path on B200.
+
+Workload (one orientation-solve = one iteration of the reference's sample loop,
+main.cpp:806-985): a 64^3 ellipsoid with b/a = 0.7, c/a = 0.5, x = 6, m = 1.55+0.005i,
+CM polarisability, CG, Error_max 1e-3, Max_Step 20, 1 scattering plane, theta 0..180 step
+10, Monte-Carlo orientations from the reference's own sampler (seed 7).  Both incident
+polarisations are solved to Error_max, then CabsCext, the far field at 19 angles and the
+Jones -> Mueller conversion.  One step = one batch of --batch orientations (2 x batch
+right-hand sides) in one batched call of libddagpu.
+
+Printed line (rank 0): value = batched orientation-solves/s with the occupancy resident
+in HBM (device time, CUDA events on the library's stream, max over ranks); e2e = the same
+through the public C ABI with the host occupancy uploaded and the results read back every
+step; plain_gpu = the drop-in path (one ddagpu_dda_fft call per polarisation); roofline =
+the matvec (K1+K2+K3) on the same batch; cpu_baseline = the reference's own sample loop on
+the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+GRID, X, MAT, BA, CA, SEED = 64, 6.0, (1.55, 0.005), 0.7, 0.5, 7
+METRIC = "orientation-solves/s at 64^3, batched+mixed vs plain GPU at Error_max 1e-3"
+WORKLOAD = ("MC orientations (seed 7) of a 64^3 ellipsoid b/a=0.7 c/a=0.5, x=6, m=1.55+0.005i, "
+            "CM, CG, Error_max 1e-3, Max_Step 20, 1 plane, 19 angles, both polarisations")
+
+
+def ellipsoid_occ(n=GRID, b_a=BA, c_a=CA):
+    """iGenerateEllipsoid (particle.cpp:408-444): cell centres inside the ellipsoid."""
+    f = np.float32
+    c = f(f(n) / f(2.0) - f(0.5))
+    a = f(n)
+    b, cc = f(a * f(b_a)), f(a * f(c_a))
+    a2, b2, c2 = f(a / f(2)) ** 2, f(b / f(2)) ** 2, f(cc / f(2)) ** 2
+    i = np.arange(n, dtype=f)[:, None, None] - c
+    j = np.arange(n, dtype=f)[None, :, None] - c
+    k = np.arange(n, dtype=f)[None, None, :] - c
+    return (((i * i) / a2 + (j * j) / b2) + (k * k) / c2 <= f(1.0)).astype(np.int8)
+
+
+# ----------------------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ reference / CPU arm
+def cpu_reference(n_samples: int, threads: int):
+    """The reference's own sample loop (oracle/_ref, physicist2018/dda-fft compiled from its
+    sources) on this workload; returns (orientation-solves/s, kind, seconds)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as P
+    if os.path.exists(P.REF_SO):
+        R = P.RefLib()
+        cfg = P.make_run_cfg(grid=GRID, target=2, b_a=BA, c_a=CA, x=X, materials=(MAT,),
+                             orientation=1, seed=SEED)
+        secs, *_ = R.run_samples(cfg, n_samples, threads)
+        return n_samples / secs, "reference", secs, threads
+    O = P.Oracle()   # the FP64 restatement, single thread
+    t0 = time.perf_counter()
+    P.orientation_solves(O, GRID, X, [MAT], n_samples, target=2, b_a=BA, c_a=CA, orientation=1,
+                         seed=SEED)
+    secs = time.perf_counter() - t0
+    return n_samples / secs, "port", secs, 1
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    per_step = max(2 * threads, 8)
+    for _ in range(args.warmup):
+        cpu_reference(max(threads, 1), threads)
+    vals, total_s, total_n, kind, used = [], 0.0, 0, "reference", threads
+    for _ in range(args.steps):
+        v, kind, secs, used = cpu_reference(per_step, threads)
+        vals.append(v)
+        total_s += secs
+        total_n += per_step
+    value = total_n / total_s
+    sample = f"{per_step} orientation-solves per step on {used} host threads (setup excluded)"
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "orientation-solves/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000 * total_s / max(args.steps, 1), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "grid": GRID, "orientations_per_step": per_step},
+        "cpu_baseline": {"value": value, "unit": "orientation-solves/s", "cores": used,
+                         "kind": kind, "sample": sample},
+        "e2e": {"value": value, "unit": "orientation-solves/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+# ------------------------------------------------------------------------- our arm
+def load_traffic(nrhs: int):
+    """DRAM bytes per matvec from the committed ncu summary, scaled to nrhs."""
+    path = os.path.join(ROOT, "profiles", "matvec_traffic.json")
+    try:
+        t = json.load(open(path))
+        per_rhs = t["dram_bytes_per_rhs"]
+        return float(t.get("dram_bytes_fixed", 0.0) + per_rhs * nrhs)
+    except Exception:
+        return None
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--batch", type=int, default=64, help="orientations per step")
+    ap.add_argument("--plain", type=int, default=8, help="orientations timed on the plain path")
+    ap.add_argument("--cpu-samples", type=int, default=0)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference_arm(args)
+
+    import torch
+    import torch.distributed as dist
+    import dda_fft_b200 as D
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    dev = local
+
+    B, K, W = args.batch, args.steps, args.warmup
+    occ = ellipsoid_occ()
+    kd = 2 * X / GRID
+    ctx = D.Context(GRID, kd, max_rhs=2 * B, device=dev)
+    stream = torch.cuda.ExternalStream(ctx.stream_ptr, device=dev)
+    # every rank draws its own contiguous run of the reference's MC stream (worker 0)
+    total = (W + K) * B * world
+    rot_all = D.mc_rotations(SEED, total)
+    mine = rot_all[rank * (W + K) * B:(rank + 1) * (W + K) * B]
+    cfg_host = D.BatchConfig(occ=occ, materials=[MAT], nplanes=1)
+    cfg_res = D.BatchConfig(occ=None, materials=[MAT], nplanes=1)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    def maxrank(v):
+        if world == 1:
+            return v
+        t = torch.tensor([v], device=f"cuda:{dev}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # warm-up (also uploads the occupancy, which stays resident)
+    for w in range(W):
+        ctx.orientation_solves(cfg_host if w == 0 else cfg_res, mine[w * B:(w + 1) * B])
+
+    # ---- value: occupancy resident, device time
+    sums = {"cabs": 0.0, "cext": 0.0, "mueller": None}
+    clk = ClockSampler(dev)
+    barrier()
+    l0 = ctx.kernel_launches
+    clk.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for k in range(K):
+        r = ctx.orientation_solves(cfg_res, mine[(W + k) * B:(W + k + 1) * B])
+        sums["cabs"] += float(r["cabs"].sum())
+        sums["cext"] += float(r["cext"].sum())
+        m = r["mueller"].sum(axis=0)
+        sums["mueller"] = m if sums["mueller"] is None else sums["mueller"] + m
+    e1.record(stream)
+    barrier()
+    clocks = clk.stop()
+    launches = ctx.kernel_launches - l0
+    ms = maxrank(e0.elapsed_time(e1))
+    value = K * B * world / (ms / 1000.0)
+
+    # ---- e2e: public API with host buffers every step
+    barrier()
+    t0 = time.perf_counter()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for k in range(K):
+        ctx.orientation_solves(cfg_host, mine[(W + k) * B:(W + k + 1) * B])
+    f1.record(stream)
+    barrier()
+    wall = time.perf_counter() - t0
+    ms_e2e = maxrank(max(f0.elapsed_time(f1), wall * 1000.0))
+    e2e = K * B * world / (ms_e2e / 1000.0)
+    nA = D.num_angles(0, 180, 10)
+    h2d = occ.nbytes + B * 72 + 64
+    d2h = B * (16 + nA * 16 * 8) + 2 * B * 8
+
+    # ---- plain drop-in path: one ddagpu_dda_fft per polarisation + Mueller
+    plain = None
+    if rank == 0 and args.plain > 0:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        pctx = D.Context(GRID, kd, max_rhs=2, device=dev)
+        alpha = np.array([0, _cm_alpha(kd, complex(*MAT))], np.complex64)
+        th = np.deg2rad(np.arange(nA) * 10.0)
+        ksc0 = np.stack([np.sin(th), np.zeros_like(th), np.cos(th)], 1)
+        rots = mine[:args.plain]
+
+        def one(T):
+            kinc = T @ np.array([0, 0, 1.0])
+            e = [T @ np.array([1.0, 0, 0]), T @ np.array([0, 1.0, 0])]
+            ksc = (ksc0 @ T.T)[None]
+            esc = [pctx.dda_fft(occ, alpha, [0, 1], kd, kinc, e[q], ksc, trace=False)["esc"]
+                   for q in range(2)]
+            pctx.mueller(kinc, e[0], e[1], ksc, (T @ np.array([0, 1.0, 0]))[None], esc[0], esc[1])
+        one(rots[0])
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        for T in rots:
+            one(T)
+        torch.cuda.synchronize(dev)
+        plain = len(rots) / (time.perf_counter() - t0)
+        pctx.close()
+
+    # ---- roofline: the matvec (K1+K2+K3) on the batch, device-resident
+    nrhs = 2 * B
+    n3 = GRID ** 3
+    x = torch.randn(nrhs, 3, GRID, GRID, GRID, dtype=torch.complex64, device=f"cuda:{dev}")
+    y = torch.empty_like(x)
+    torch.cuda.synchronize(dev)
+    for _ in range(3):
+        ctx.convolution_dev(x, y, nrhs)
+    reps = 10
+    g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    g0.record(stream)
+    for _ in range(reps):
+        ctx.convolution_dev(x, y, nrhs)
+    g1.record(stream)
+    torch.cuda.synchronize(dev)
+    mv_ms = g0.elapsed_time(g1) / reps
+    alg_bytes = 384.0 * n3 + 624.0 * n3 * nrhs     # B RHS sharing Ahat
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        peak, peak_src = float(peaks["hbm_gbs"]), "measured"
+    except Exception:
+        peak, peak_src = 6650.0, "fallback"
+    achieved = alg_bytes / (mv_ms / 1000.0) / 1e9
+    traffic = load_traffic(nrhs)
+    del x, y
+
+    # ---- CPU baseline (rank 0, N = 1 only)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        threads = os.cpu_count() or 1
+        ns = args.cpu_samples or max(threads, 8)
+        v, kind, secs, used = cpu_reference(ns, threads)
+        cpu = {"value": v, "unit": "orientation-solves/s", "cores": used, "kind": kind,
+               "sample": f"{ns} orientation-solves of the same workload, {secs:.1f} s wall "
+                         f"(setup excluded)"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "orientation-solves/s", "n_gpus": world,
+            "steps": K, "warmup": W, "ms_per_step": ms / K, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "grid": GRID, "orientations_per_step": B,
+                       "rhs_per_step": 2 * B, "parallelism": f"orientations sharded over {world} GPU(s)",
+                       "l2": "working set per step >> L2 (126 MB): no flush needed",
+                       "tiling": list(ctx.tiling())},
+            "e2e": {"value": e2e, "unit": "orientation-solves/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "plain_gpu": {"value": plain, "unit": "orientation-solves/s",
+                          "path": "ddagpu_dda_fft per polarisation + ddagpu_mueller"},
+            "speedup_vs_plain": (value / plain) if plain else None,
+            "roofline": {"kernel": "matvec K1+K2+K3", "bound": "hbm", "achieved": achieved,
+                         "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_source": peak_src, "traffic": traffic,
+                         "algorithmic_bytes": alg_bytes, "ms_per_launch": mv_ms,
+                         "rhs_per_launch": nrhs},
+            "cpu_baseline": cpu,
+            "clocks": clocks,
+            "gpu_launches": launches,
+            "check": {"cext_mean": sums["cext"] / (K * B), "cabs_mean": sums["cabs"] / (K * B)},
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def _cm_alpha(d0, m):
+    """Polarizability_CM (dda_func.cpp:1631-1637)."""
+    return d0 ** 3 * (0.75 / np.pi) * (m * m - 1) / (m * m + 2)
+
+
+if __name__ == "__main__":
+    main()

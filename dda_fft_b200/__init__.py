@@ -1,0 +1,21 @@
+"""B200-native DDA-FFT hot path (libddagpu) -- Python bindings over the C ABI.
+
+The product is the C-ABI shared library dda_fft_b200/lib/libddagpu.so (include/ddagpu.h);
+this module loads it with ctypes and mirrors the reference's DDA_FFT interface for tests
+and benchmarks.  There is no CPU fallback: if the library cannot be loaded, every call
+raises.
+"""
+from .api import (  # noqa: F401
+    BatchConfig,
+    Context,
+    DDAGPUError,
+    build,
+    fixed_rotation,
+    lib,
+    library_path,
+    mc_rotations,
+    num_angles,
+)
+
+__all__ = ["Context", "BatchConfig", "DDAGPUError", "build", "lib", "library_path",
+           "mc_rotations", "fixed_rotation", "num_angles"]

@@ -1,0 +1,290 @@
+"""ctypes mirror of include/ddagpu.h.
+
+Host arrays use numpy in the reference's layouts: a field is complex64 (ni, nj, nl, 3)
+(cvector), the Green tensor complex64 (2ni, 2nj, 2nl, 6) (cmatrix), the occupancy int8
+(ni, nj, nl) (cAlpha).  Device entry points take torch CUDA tensors in the
+structure-of-arrays layout (nrhs, 3, ni, nj, nl) complex64.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+import threading
+from dataclasses import dataclass, field
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+
+
+def library_path() -> str:
+    return os.path.join(HERE, "lib", "libddagpu.so")
+
+
+def build(force: bool = False) -> str:
+    """Compile libddagpu.so for sm_100a with nvcc (dda_fft_b200/csrc/Makefile)."""
+    path = library_path()
+    args = ["make", "-C", os.path.join(HERE, "csrc"), "-j4"]
+    if force:
+        args.insert(1, "-B")
+    out = subprocess.run(args, capture_output=True, text=True)
+    if out.returncode != 0 or not os.path.exists(path):
+        raise RuntimeError("libddagpu build failed:\n" + out.stdout[-4000:] + out.stderr[-4000:])
+    return path
+
+
+class DDAGPUError(RuntimeError):
+    pass
+
+
+_lib = None
+_lock = threading.Lock()
+_p, _i, _f, _d = C.c_void_p, C.c_int, C.c_float, C.c_double
+
+
+class SolveInfo(C.Structure):
+    _fields_ = [("steps", _i), ("step_min", _i), ("rolled_back", _i), ("matvecs", _i),
+                ("err", _d), ("err_min", _d)]
+
+
+class _BatchCfg(C.Structure):
+    _fields_ = [("solver", _i), ("tau", _f), ("max_step", _i), ("err_max", _f),
+                ("polarizability", _i), ("n_mat", _i), ("m", _p), ("occ", _p), ("nplanes", _i),
+                ("theta_min", _f), ("theta_max", _f), ("theta_step", _f)]
+
+
+class BatchInfo(C.Structure):
+    _fields_ = [("n_rhs", _i), ("max_steps", _i), ("rolled_back", _i), ("max_err", _d)]
+
+
+def lib():
+    """Load libddagpu.so (building it first if it is absent); raises if that fails."""
+    global _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        path = library_path()
+        if not os.path.exists(path):
+            build()
+        L = C.CDLL(path)
+        L.ddagpu_version.restype = C.c_char_p
+        L.ddagpu_last_error.restype = C.c_char_p
+        L.ddagpu_create.argtypes = [C.POINTER(_p), _i, _i, _i, _i, _d, _i]
+        L.ddagpu_destroy.argtypes = [_p]
+        L.ddagpu_set_green.argtypes = [_p, _p]
+        L.ddagpu_convolution.argtypes = [_p, _p, _p, _i]
+        L.ddagpu_dda_fft.argtypes = [_p, _i, _i, _f, _i, _i, _i, _p, _p, _i, _p, _i, _f, _f, _p,
+                                     _p, _i, _i, _i, _p, _p, _p, _p, C.POINTER(SolveInfo), _p]
+        L.ddagpu_farfield.argtypes = [_p, _p, _i, _p, _f, _p, _i, _p, _p]
+        L.ddagpu_cabscext.argtypes = [_p, _f, _p, _p, _p, _i, _p, _p, _p, _p]
+        L.ddagpu_mueller.argtypes = [_p, _p, _p, _p, _i, _i, _p, _p, _p, _p, _p]
+        L.ddagpu_orientation_solves.argtypes = [_p, C.POINTER(_BatchCfg), _i, _p, _p, _p, _p,
+                                                C.POINTER(BatchInfo)]
+        L.ddagpu_num_angles.argtypes = [_f, _f, _f]
+        L.ddagpu_mc_rotations.argtypes = [C.c_ulonglong, _i, _i, _p]
+        L.ddagpu_fixed_rotation.argtypes = [_d, _d, _d, _p]
+        L.ddagpu_convolution_dev.argtypes = [_p, _p, _p, _i, _i]
+        L.ddagpu_stream.argtypes = [_p]
+        L.ddagpu_stream.restype = _p
+        L.ddagpu_kernel_launches.argtypes = [_p]
+        L.ddagpu_kernel_launches.restype = C.c_longlong
+        L.ddagpu_set_tiling.argtypes = [_p, _i, _i]
+        L.ddagpu_get_tiling.argtypes = [_p, C.POINTER(_i), C.POINTER(_i)]
+        L.ddagpu_autotune.argtypes = [_p, _i]
+        _lib = L
+        return L
+
+
+def _check(rc: int) -> None:
+    if rc != 0:
+        msg = lib().ddagpu_last_error().decode(errors="replace")
+        raise DDAGPUError(f"libddagpu error {rc}: {msg}")
+
+
+def _ptr(a: np.ndarray):
+    return C.c_void_p(a.ctypes.data)
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, np.float32)
+
+
+def _cvec(a):
+    """complex (..., 3) -> float32 interleaved cvector layout."""
+    return np.ascontiguousarray(np.asarray(a, np.complex64)).view(np.float32)
+
+
+def num_angles(theta_min, theta_max, theta_step) -> int:
+    return int(lib().ddagpu_num_angles(theta_min, theta_max, theta_step))
+
+
+def mc_rotations(base_seed: int, count: int, worker: int = 0) -> np.ndarray:
+    out = np.zeros((count, 3, 3))
+    _check(lib().ddagpu_mc_rotations(C.c_ulonglong(base_seed), worker, count, _ptr(out)))
+    return out
+
+
+def fixed_rotation(psi=0.0, iota=0.0, kappa=0.0) -> np.ndarray:
+    out = np.zeros((3, 3))
+    _check(lib().ddagpu_fixed_rotation(psi, iota, kappa, _ptr(out)))
+    return out
+
+
+@dataclass
+class BatchConfig:
+    occ: np.ndarray | None     # None: reuse the occupancy resident from the previous call
+    materials: list = field(default_factory=lambda: [(1.5, 0.01)])
+    solver: int = 0
+    tau: float = 0.0
+    max_step: int = 20
+    err_max: float = 1e-3
+    polarizability: int = 1
+    nplanes: int = 1
+    theta_min: float = 0.0
+    theta_max: float = 180.0
+    theta_step: float = 10.0
+
+
+class Context:
+    """One lattice on one GPU (ddagpu_create)."""
+
+    def __init__(self, grid, kd: float, max_rhs: int = 1, device: int = 0):
+        self.grid = (grid,) * 3 if np.isscalar(grid) else tuple(int(g) for g in grid)
+        self.kd = float(kd)
+        self.max_rhs = max_rhs
+        h = C.c_void_p()
+        _check(lib().ddagpu_create(C.byref(h), device, *self.grid, self.kd, max_rhs))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().ddagpu_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    @property
+    def kernel_launches(self) -> int:
+        return int(lib().ddagpu_kernel_launches(self._h))
+
+    @property
+    def stream_ptr(self) -> int:
+        return int(lib().ddagpu_stream(self._h) or 0)
+
+    def set_green(self, cmA: np.ndarray) -> None:
+        a = np.ascontiguousarray(np.asarray(cmA, np.complex64))
+        _check(lib().ddagpu_set_green(self._h, _ptr(a)))
+
+    def convolution(self, p: np.ndarray, conj: bool = False) -> np.ndarray:
+        x = _cvec(p)
+        out = np.zeros_like(x)
+        _check(lib().ddagpu_convolution(self._h, _ptr(x), _ptr(out), int(conj)))
+        return out.view(np.complex64).reshape(np.shape(p))
+
+    def dda_fft(self, occ, alpha, listmv, d0, kinc, einc, ksc, solver=0, tau=0.0, max_step=20,
+                err_max=1e-3, fft_mode=0, trace=True):
+        """DDA_FFT for one polarisation; returns dict(esc, cabs, cext, info, trace)."""
+        o = np.ascontiguousarray(occ, np.int8)
+        a = _cvec(np.asarray(alpha, np.complex64).reshape(-1, 1)).ravel()
+        mv = np.ascontiguousarray(listmv, np.int32)
+        ks = _f32(ksc)
+        npl, nang = ks.shape[:2]
+        esc = np.zeros((npl, nang, 3), np.complex64)
+        k = _f32(kinc)
+        e = _cvec(np.asarray(einc, np.complex64))
+        ca, ce = C.c_float(), C.c_float()
+        info = SolveInfo()
+        tr = np.zeros(max_step + 1) if trace else None
+        _check(lib().ddagpu_dda_fft(self._h, 0, solver, tau, *self.grid, _ptr(a), _ptr(mv),
+                                    len(mv) - 1, _ptr(o), max_step, err_max, d0, _ptr(k), _ptr(e),
+                                    fft_mode, npl, nang, _ptr(ks), _ptr(esc.view(np.float32)),
+                                    C.byref(ca), C.byref(ce), C.byref(info),
+                                    _ptr(tr) if trace else None))
+        out = dict(esc=esc, cabs=ca.value, cext=ce.value, steps=info.steps,
+                   step_min=info.step_min if info.rolled_back else -1, matvecs=info.matvecs,
+                   err=info.err, err_min=info.err_min, rolled_back=info.rolled_back)
+        if trace:
+            out["trace"] = tr[: info.steps + 1]
+        return out
+
+    def farfield(self, occ, listmv, d0, p, ksc) -> np.ndarray:
+        o = np.ascontiguousarray(occ, np.int8)
+        mv = np.ascontiguousarray(listmv, np.int32)
+        x = _cvec(p)
+        ks = _f32(np.asarray(ksc).reshape(-1, 3))
+        out = np.zeros((ks.shape[0], 3), np.complex64)
+        _check(lib().ddagpu_farfield(self._h, _ptr(mv), len(mv) - 1, _ptr(o), d0, _ptr(x),
+                                     ks.shape[0], _ptr(ks), _ptr(out.view(np.float32))))
+        return out
+
+    def cabscext(self, occ, alpha, d0, kinc, einc, p):
+        o = np.ascontiguousarray(occ, np.int8)
+        a = _cvec(np.asarray(alpha, np.complex64).reshape(-1, 1)).ravel()
+        x = _cvec(p)
+        ca, ce = C.c_float(), C.c_float()
+        _check(lib().ddagpu_cabscext(self._h, d0, _ptr(_f32(kinc)), _ptr(_cvec(einc)), _ptr(a),
+                                     len(alpha) - 1, _ptr(o), _ptr(x), C.byref(ca), C.byref(ce)))
+        return ca.value, ce.value
+
+    def mueller(self, kinc, einc0, einc1, ksc, normals, esc0, esc1) -> np.ndarray:
+        ks = _f32(ksc)
+        npl, nang = ks.shape[:2]
+        out = np.zeros((nang, 4, 4), np.float32)
+        _check(lib().ddagpu_mueller(self._h, _ptr(_f32(kinc)), _ptr(_cvec(einc0)),
+                                    _ptr(_cvec(einc1)), npl, nang, _ptr(ks), _ptr(_f32(normals)),
+                                    _ptr(_cvec(esc0)), _ptr(_cvec(esc1)), _ptr(out)))
+        return out
+
+    def orientation_solves(self, cfg: BatchConfig, rot: np.ndarray):
+        """Both polarisations of every orientation rot[k] (3x3), batched on the GPU."""
+        rot = np.ascontiguousarray(rot, np.float64).reshape(-1, 3, 3)
+        n = rot.shape[0]
+        na = num_angles(cfg.theta_min, cfg.theta_max, cfg.theta_step)
+        occ = None if cfg.occ is None else np.ascontiguousarray(cfg.occ, np.int8)
+        m = np.ascontiguousarray(np.asarray(cfg.materials, np.float32).ravel())
+        c = _BatchCfg(cfg.solver, cfg.tau, cfg.max_step, cfg.err_max, cfg.polarizability,
+                      len(cfg.materials), _ptr(m), None if occ is None else _ptr(occ),
+                      cfg.nplanes, cfg.theta_min, cfg.theta_max, cfg.theta_step)
+        cabs = np.zeros(n)
+        cext = np.zeros(n)
+        mm = np.zeros((n, na, 4, 4))
+        info = BatchInfo()
+        _check(lib().ddagpu_orientation_solves(self._h, C.byref(c), n, _ptr(rot), _ptr(cabs),
+                                               _ptr(cext), _ptr(mm), C.byref(info)))
+        return dict(cabs=cabs, cext=cext, mueller=mm, n_rhs=info.n_rhs, max_steps=info.max_steps,
+                    rolled_back=info.rolled_back, max_err=info.max_err)
+
+    # ------------------------------------------------------------ device-resident
+    def convolution_dev(self, p_dev, out_dev, nrhs: int = 1, conj: bool = False) -> None:
+        """G * p for torch CUDA tensors (nrhs, 3, ni, nj, nl) complex64, on this
+        context's stream."""
+        _check(lib().ddagpu_convolution_dev(self._h, C.c_void_p(p_dev.data_ptr()),
+                                            C.c_void_p(out_dev.data_ptr()), nrhs, int(conj)))
+
+    def set_tiling(self, tile_x=0, rows_g=0):
+        _check(lib().ddagpu_set_tiling(self._h, tile_x, rows_g))
+
+    def tiling(self):
+        a, b = C.c_int(), C.c_int()
+        _check(lib().ddagpu_get_tiling(self._h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def autotune(self, nrhs: int = 4):
+        _check(lib().ddagpu_autotune(self._h, nrhs))
+        return self.tiling()

@@ -1,0 +1,1047 @@
+// Host side of libddagpu: contexts, the DDA_FFT driver over the device kernels, the
+// batched orientation solves and the C ABI of include/ddagpu.h.
+//
+// The solver driver mirrors DDA_FFT (dda_func.cpp:1075-1570) step by step: step 0, the
+// per-method recurrences, the absolute Error_max test and the best-iterate rollback.  All
+// fields, reductions and coefficients stay on the device; the host only launches kernels
+// and reads one flag per right-hand side per iteration to stop when all have converged.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/ddagpu.h"
+#include "internal.h"
+#include "post.h"
+#include "solver.h"
+
+using namespace ddagpu;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string &msg)
+{
+    g_err = msg;
+    return code;
+}
+
+#define CK(expr)                                                                            \
+    do {                                                                                    \
+        cudaError_t _e = (expr);                                                            \
+        if (_e != cudaSuccess)                                                              \
+            return fail(_e == cudaErrorMemoryAllocation ? DDAGPU_ENOMEM : DDAGPU_ECUDA,     \
+                        std::string(#expr) + ": " + cudaGetErrorString(_e));                \
+    } while (0)
+
+#define RET(expr)                                                                           \
+    do {                                                                                    \
+        int _r = (expr);                                                                    \
+        if (_r != DDAGPU_OK) return _r;                                                     \
+    } while (0)
+
+bool pow2_in(int n) { return n >= kMinEdge && n <= kMaxEdge && (n & (n - 1)) == 0; }
+
+template <class T>
+cudaError_t dalloc(T **p, size_t n)
+{
+    return cudaMalloc((void **)p, (n ? n : 1) * sizeof(T));
+}
+
+}  // namespace
+
+struct ddagpu_ctx {
+    int dev = 0;
+    int ni = 0, nj = 0, nl = 0;
+    size_t N = 0;
+    double kd = 0;
+    int cap = 0;
+    cudaStream_t st = nullptr;
+    Lat L{};
+    int tile_x = 32, rows_g = 16;
+    float2 *ahat = nullptr, *tw = nullptr;
+    float2 *work = nullptr, *p = nullptr, *pmin = nullptr, *r = nullptr, *s = nullptr,
+           *g = nullptr, *h = nullptr, *w = nullptr;
+    RhsState *state = nullptr;
+    int *active = nullptr;
+    double *trace = nullptr;
+    int trace_len = 0;
+    signed char *occ = nullptr;
+    int *mv = nullptr;
+    float2 *alpha = nullptr;
+    int nmat_cap = kMaxMaterials + 1;
+    double *kinc = nullptr, *einc = nullptr;
+    // post-processing buffers, grown on demand
+    int ndir_cap = 0;
+    double *ksc = nullptr, *esc_acc = nullptr, *cc_acc = nullptr, *normals = nullptr,
+           *mueller = nullptr;
+    float2 *esc = nullptr;
+    float *cabs = nullptr, *cext = nullptr;
+    int nplane_cap = 0, nangle_cap = 0;
+    bool occ_valid = false;      // occupancy of the last batched call is resident
+    int occ_nmat1 = 0, occ_nact = 0;
+    long long launches = 0;      // kernels launched by this context
+    std::mutex mu;
+};
+
+namespace {
+
+struct DevGuard {
+    int prev = -1;
+    explicit DevGuard(int dev)
+    {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DevGuard()
+    {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
+// W_n^k (k < n) followed by W_2n^j (j < n), forward sign, built in FP64.
+void twiddles(int n, float2 *out)
+{
+    const double pi = 3.14159265358979323846264338327950288;
+    for (int k = 0; k < n; k++)
+        out[k] = make_float2((float)std::cos(-2.0 * pi * k / n), (float)std::sin(-2.0 * pi * k / n));
+    for (int j = 0; j < n; j++)
+        out[n + j] = make_float2((float)std::cos(-pi * j / n), (float)std::sin(-pi * j / n));
+}
+
+int ensure_post(ddagpu_ctx *c, int ndir, int nplanes, int nangles)
+{
+    if (ndir > c->ndir_cap) {
+        cudaFree(c->ksc);
+        cudaFree(c->esc_acc);
+        cudaFree(c->esc);
+        c->ksc = nullptr;
+        c->esc_acc = nullptr;
+        c->esc = nullptr;
+        CK(dalloc(&c->ksc, (size_t)c->cap * ndir * 3));
+        CK(dalloc(&c->esc_acc, (size_t)c->cap * ndir * 6));
+        CK(dalloc(&c->esc, (size_t)c->cap * ndir * 3));
+        c->ndir_cap = ndir;
+    }
+    if (nplanes > c->nplane_cap || nangles > c->nangle_cap) {
+        cudaFree(c->normals);
+        cudaFree(c->mueller);
+        c->normals = nullptr;
+        c->mueller = nullptr;
+        const int np = std::max(nplanes, c->nplane_cap), na = std::max(nangles, c->nangle_cap);
+        CK(dalloc(&c->normals, (size_t)c->cap * np * 3));
+        CK(dalloc(&c->mueller, (size_t)c->cap * na * 16));
+        c->nplane_cap = np;
+        c->nangle_cap = na;
+    }
+    return DDAGPU_OK;
+}
+
+MatvecArgs mv_args(ddagpu_ctx *c, int nrhs, const float2 *src, float2 *out, int epmode, float sv,
+                   const float2 *v, int conj, int nmat1, bool gate)
+{
+    MatvecArgs a{};
+    a.L = c->L;
+    a.nrhs = nrhs;
+    a.src = src;
+    a.fstride = 3 * c->N;
+    a.work = c->work;
+    a.wstride = (size_t)3 * c->ni * (2 * c->nj) * (2 * c->nl);
+    a.ahat = c->ahat;
+    a.conj = conj;
+    a.out = out;
+    a.ep.mode = epmode;
+    a.ep.conj = conj;
+    a.ep.sv = sv;
+    a.ep.v = v;
+    a.ep.occ = c->occ;
+    a.ep.alpha = c->alpha;
+    a.ep.mv = c->mv;
+    a.ep.nmat1 = nmat1;
+    a.rhs_active = gate ? c->active : nullptr;
+    a.tile_x = c->tile_x;
+    a.rows_g = c->rows_g;
+    return a;
+}
+
+FieldArgs fa_args(ddagpu_ctx *c, int nrhs, int nmat1, double d0, float tau)
+{
+    FieldArgs f{};
+    f.N = c->N;
+    f.nrhs = nrhs;
+    f.ni = c->ni;
+    f.nj = c->nj;
+    f.nl = c->nl;
+    f.occ = c->occ;
+    f.mv = c->mv;
+    f.alpha = c->alpha;
+    f.nmat1 = nmat1;
+    f.st = c->state;
+    f.rhs_active = c->active;
+    f.p = c->p;
+    f.pmin = c->pmin;
+    f.r = c->r;
+    f.s = c->s;
+    f.g = c->g;
+    f.h = c->h;
+    f.w = c->w;
+    f.kinc = c->kinc;
+    f.einc = c->einc;
+    f.d0 = d0;
+    f.tau = tau;
+    return f;
+}
+
+struct SolveResult {
+    std::vector<RhsState> st;
+    std::vector<double> trace;
+    int matvec0 = 0, matvec_it = 0;
+};
+
+// The solver of DDA_FFT for nrhs right-hand sides whose occ, mv, alpha, kinc and einc are
+// already on the device.  Leaves the final (or rolled-back) dipoles in c->p.
+int run_solver(ddagpu_ctx *c, int nrhs, int solver, float tau, int max_step, float err_max,
+               int nmat1, double d0, int nact, SolveResult &res, bool want_trace)
+{
+    if (solver < 0 || solver > 3) return fail(DDAGPU_EINVAL, "solver must be 0..3");
+    if (max_step < 0) return fail(DDAGPU_EINVAL, "Max_Step must be >= 0");
+    if (solver == 2 && (!c->g || !c->h)) return fail(DDAGPU_EINVAL, "no BiCGStab work space");
+    cudaStream_t st = c->st;
+    const int tl = max_step + 1;
+    if (want_trace && tl > c->trace_len) {
+        cudaFree(c->trace);
+        c->trace = nullptr;
+        CK(dalloc(&c->trace, (size_t)c->cap * tl));
+        c->trace_len = tl;
+    }
+    double *trace = want_trace ? c->trace : nullptr;
+    const int tlen = want_trace ? tl : 0;
+    std::vector<RhsState> init((size_t)nrhs);
+    for (auto &S : init) {
+        std::memset(&S, 0, sizeof S);
+        S.err_max = (double)err_max;
+        S.active = 1;
+        S.nact = nact;
+    }
+    CK(cudaMemcpyAsync(c->state, init.data(), nrhs * sizeof(RhsState), cudaMemcpyHostToDevice, st));
+    std::vector<int> ones((size_t)nrhs, 1);
+    CK(cudaMemcpyAsync(c->active, ones.data(), nrhs * sizeof(int), cudaMemcpyHostToDevice, st));
+
+    FieldArgs F = fa_args(c, nrhs, nmat1, d0, tau);
+    auto field = [&](int op) {
+        c->launches += 1;
+        return launch_field_op(op, F, st);
+    };
+    auto scal = [&](int stage, int step) {
+        c->launches += 1;
+        return launch_scalar(c->state, c->active, c->active, nrhs, stage, step, trace, tlen, st);
+    };
+    // out = sv v - alpha conv(src) on active cells, gated by the active flags
+    auto matvec = [&](const float2 *src, float2 *out, float sv, const float2 *v, int conj) {
+        c->launches += 3;
+        return launch_matvec(mv_args(c, nrhs, src, out, 1, sv, v, conj, nmat1, true), st);
+    };
+
+    // ---- step 0 (dda_func.cpp:1102-1293)
+    CK(launch_first_approx(F, st));
+    c->launches += 1;
+    CK(matvec(c->p, c->r, 0.f, nullptr, 0));   // r = -alpha (G * p_inc)
+    res.matvec0 = 1;
+    switch (solver) {
+    case 0:
+        CK(field(OP_STEP0_CG));
+        CK(scal(SC_STEP0_ERR1, 0));
+        break;
+    case 1:
+        CK(field(OP_STEP0_AA));
+        CK(scal(SC_STEP0_AA, 0));
+        CK(matvec(c->r, c->s, 1.f, c->r, 1));   // s = r - conj(alpha) conv*(r)
+        res.matvec0 = 2;
+        break;
+    case 2:
+        CK(field(OP_STEP0_BICG));
+        CK(scal(SC_B_RHO1, 0));
+        CK(matvec(c->s, c->h, 1.f, c->s, 0));
+        CK(field(OP_B_GH));
+        CK(scal(SC_B2, 0));
+        CK(field(OP_B_R));
+        CK(matvec(c->r, c->w, 1.f, c->r, 0));
+        CK(field(OP_B_WW));
+        CK(scal(SC_B3, 0));
+        CK(field(OP_B_P));
+        CK(scal(SC_B4, 0));
+        res.matvec0 = 3;
+        break;
+    case 3:
+        CK(field(OP_STEP0_SIMPLE));
+        CK(scal(SC_STEP0_ERR1, 0));
+        break;
+    }
+    CK(scal(SC_START, 0));
+    // p_min = p at step 0
+    {
+        for (int k = 0; k < nrhs; k++)
+            CK(cudaMemcpyAsync(c->pmin + (size_t)k * 3 * c->N, c->p + (size_t)k * 3 * c->N,
+                               3 * c->N * sizeof(float2), cudaMemcpyDeviceToDevice, st));
+    }
+    res.matvec_it = (solver == 1 || solver == 2) ? 2 : 1;
+
+    // ---- iterations (dda_func.cpp:1301-1535)
+    std::vector<int> act((size_t)nrhs);
+    for (int o = 1; o <= max_step; o++) {
+        CK(scal(SC_TOP, o));
+        CK(launch_gated_copy(F, 0, st));   // p -> p_min where this step improved
+        c->launches += 1;
+        CK(cudaMemcpyAsync(act.data(), c->active, nrhs * sizeof(int), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        bool any = false;
+        for (int k = 0; k < nrhs; k++) any = any || act[(size_t)k];
+        if (!any) break;
+        switch (solver) {
+        case 0:
+            CK(matvec(c->s, c->w, 1.f, c->s, 0));
+            CK(field(OP_CG1));
+            CK(scal(SC_CG1, o));
+            CK(field(OP_CG2));
+            CK(scal(SC_CG2, o));
+            CK(field(OP_CG3));
+            break;
+        case 1:
+            CK(matvec(c->s, c->w, 1.f, c->s, 0));
+            CK(field(OP_AA1));
+            CK(scal(SC_AA1, o));
+            CK(field(OP_AA2));
+            CK(scal(SC_AA2, o));
+            CK(matvec(c->r, c->w, 1.f, c->r, 1));
+            CK(field(OP_AA3));
+            break;
+        case 2:
+            CK(field(OP_B_RHO));
+            CK(scal(SC_B1, o));
+            CK(field(OP_B_S));
+            CK(matvec(c->s, c->h, 1.f, c->s, 0));
+            CK(field(OP_B_GH));
+            CK(scal(SC_B2, o));
+            CK(field(OP_B_R));
+            CK(matvec(c->r, c->w, 1.f, c->r, 0));
+            CK(field(OP_B_WW));
+            CK(scal(SC_B3, o));
+            CK(field(OP_B_P));
+            CK(scal(SC_B4, o));
+            break;
+        case 3:
+            CK(matvec(c->p, c->w, 1.f, c->p, 0));
+            CK(field(OP_SIMPLE));
+            CK(scal(SC_ERR1, o));
+            break;
+        }
+    }
+    // ---- rollback (dda_func.cpp:1537-1548), for every right-hand side
+    CK(launch_scalar(c->state, nullptr, nullptr, nrhs, SC_FINAL, 0, nullptr, 0, st));
+    CK(launch_gated_copy(F, 1, st));
+    c->launches += 2;
+    res.st.resize((size_t)nrhs);
+    CK(cudaMemcpyAsync(res.st.data(), c->state, nrhs * sizeof(RhsState), cudaMemcpyDeviceToHost, st));
+    if (want_trace) {
+        res.trace.assign((size_t)nrhs * tl, 0.0);
+        CK(cudaMemcpyAsync(res.trace.data(), c->trace, res.trace.size() * sizeof(double),
+                           cudaMemcpyDeviceToHost, st));
+    }
+    CK(cudaStreamSynchronize(st));
+    return DDAGPU_OK;
+}
+
+int count_active(const signed char *occ, size_t N, const int *mv, int nmat1)
+{
+    int n = 0;
+    for (size_t q = 0; q < N; q++) {
+        const int m = (unsigned char)occ[q];
+        if (m < nmat1 && mv[m]) n++;
+    }
+    return n;
+}
+
+int check_occ(const signed char *occ, size_t N, int nmat1)
+{
+    for (size_t q = 0; q < N; q++)
+        if ((int)occ[q] < 0 || (int)occ[q] >= nmat1)
+            return fail(DDAGPU_EINVAL, "cAlpha holds a material index outside 0..n_mat");
+    return DDAGPU_OK;
+}
+
+// Polarisabilities (dda_func.cpp:1631-1677) in double.
+struct cd {
+    double r, i;
+};
+cd cmuld(cd a, cd b) { return {a.r * b.r - a.i * b.i, a.r * b.i + a.i * b.r}; }
+cd cdivd(cd a, cd b)
+{
+    const double d = b.r * b.r + b.i * b.i;
+    return {(a.r * b.r + a.i * b.i) / d, (a.i * b.r - a.r * b.i) / d};
+}
+cd polarizability(int model, double d0, cd m, const double *kinc, const double *einc)
+{
+    const double pi = 3.14159265358979323846264338327950288;
+    const cd eps = cmuld(m, m);
+    cd a = cdivd({eps.r - 1.0, eps.i}, {eps.r + 2.0, eps.i});
+    const double f = d0 * d0 * d0 * (0.75 / pi);
+    a = {a.r * f, a.i * f};
+    auto rr = [](cd x) { // x / (1 - (2/3) i x)
+        return cdivd(x, {1.0 + (2.0 / 3.0) * x.i, -(2.0 / 3.0) * x.r});
+    };
+    if (model == 2) return rr(a);
+    if (model == 3) {
+        const double b = -std::sqrt(4.0 * pi / 3.0) / d0;
+        return rr(cdivd(a, {1.0 + a.r * b, a.i * b}));
+    }
+    if (model == 4 || model == 5) {
+        const double b1 = -1.8915316, b2 = 0.1648469, b3 = -1.7700004;
+        double S = 0.2;
+        if (model == 5) {
+            const double rx = kinc[0] * einc[0], ry = kinc[1] * einc[2], rz = kinc[2] * einc[4];
+            S = rx * rx + ry * ry + rz * rz;
+        }
+        const cd t = {b1 + b2 * eps.r + S * b3 * eps.r, b2 * eps.i + S * b3 * eps.i - (2.0 / 3.0) * d0};
+        const cd ad = {a.r / d0, a.i / d0};
+        const cd q = cmuld(ad, t);
+        return cdivd(a, {1.0 + q.r, q.i});
+    }
+    return a;
+}
+
+int rounding_ref(float r0)
+{ // complex.cpp:213-223
+    double ip;
+    const double fr = std::modf((double)r0, &ip);
+    return fr > 0.5 ? (int)ip + 1 : (int)ip;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *ddagpu_version(void) { return "ddagpu 1.0 (sm_100a)"; }
+const char *ddagpu_last_error(void) { return g_err.c_str(); }
+
+int ddagpu_num_angles(float theta_min, float theta_max, float theta_step)
+{
+    return rounding_ref(((theta_max - theta_min) / theta_step) + 1.f);
+}
+
+int ddagpu_create(ddagpu_ctx **out, int device, int i_max, int j_max, int l_max, double kd,
+                  int max_rhs)
+{
+    if (!out) return fail(DDAGPU_EINVAL, "null context pointer");
+    *out = nullptr;
+    if (!pow2_in(i_max) || !pow2_in(j_max) || !pow2_in(l_max))
+        return fail(DDAGPU_EINVAL, "lattice edges must be powers of two in [2, 128]");
+    if (max_rhs < 1) return fail(DDAGPU_EINVAL, "max_rhs must be >= 1");
+    if (!(kd > 0.0)) return fail(DDAGPU_EINVAL, "kd must be positive");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return fail(DDAGPU_ENOTBUILT, "no CUDA device");
+    if (device < 0 || device >= ndev) return fail(DDAGPU_EINVAL, "bad device index");
+    DevGuard dg(device);
+    ddagpu_ctx *c = new ddagpu_ctx();
+    c->dev = device;
+    c->ni = i_max;
+    c->nj = j_max;
+    c->nl = l_max;
+    c->N = (size_t)i_max * j_max * l_max;
+    c->kd = kd;
+    c->cap = max_rhs;
+    c->tile_x = std::min(i_max <= 64 ? 32 : 16, 2 * l_max);
+    c->rows_g = std::min(16, j_max);
+    auto bail = [&](int code) {
+        ddagpu_destroy(c);
+        return code;
+    };
+    if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess)
+        return bail(fail(DDAGPU_ECUDA, "stream creation failed"));
+    const size_t n3 = 3 * c->N, wst = (size_t)3 * i_max * (2 * j_max) * (2 * l_max);
+    cudaError_t e = cudaSuccess;
+    auto A = [&](cudaError_t x) {
+        if (x != cudaSuccess && e == cudaSuccess) e = x;
+    };
+    A(dalloc(&c->ahat, ahat_elems(i_max, j_max, l_max)));
+    A(dalloc(&c->tw, (size_t)2 * (i_max + j_max + l_max)));
+    A(dalloc(&c->work, wst * max_rhs));
+    A(dalloc(&c->p, n3 * max_rhs));
+    A(dalloc(&c->pmin, n3 * max_rhs));
+    A(dalloc(&c->r, n3 * max_rhs));
+    A(dalloc(&c->s, n3 * max_rhs));
+    A(dalloc(&c->w, n3 * max_rhs));
+    A(dalloc(&c->g, n3 * max_rhs));
+    A(dalloc(&c->h, n3 * max_rhs));
+    A(dalloc(&c->state, (size_t)max_rhs));
+    A(dalloc(&c->active, (size_t)max_rhs));
+    A(dalloc(&c->occ, c->N));
+    A(dalloc(&c->mv, (size_t)c->nmat_cap));
+    A(dalloc(&c->alpha, (size_t)c->nmat_cap * max_rhs));
+    A(dalloc(&c->kinc, (size_t)3 * max_rhs));
+    A(dalloc(&c->einc, (size_t)6 * max_rhs));
+    A(dalloc(&c->cc_acc, (size_t)2 * max_rhs));
+    A(dalloc(&c->cabs, (size_t)max_rhs));
+    A(dalloc(&c->cext, (size_t)max_rhs));
+    if (e != cudaSuccess)
+        return bail(fail(e == cudaErrorMemoryAllocation ? DDAGPU_ENOMEM : DDAGPU_ECUDA,
+                         std::string("allocation: ") + cudaGetErrorString(e)));
+    std::vector<float2> tw((size_t)2 * (i_max + j_max + l_max));
+    twiddles(i_max, tw.data());
+    twiddles(j_max, tw.data() + 2 * i_max);
+    twiddles(l_max, tw.data() + 2 * (i_max + j_max));
+    c->L.ni = i_max;
+    c->L.nj = j_max;
+    c->L.nl = l_max;
+    c->L.N = c->N;
+    c->L.tw_i = c->tw;
+    c->L.tw_j = c->tw + 2 * i_max;
+    c->L.tw_l = c->tw + 2 * (i_max + j_max);
+    if ((e = cudaMemcpyAsync(c->tw, tw.data(), tw.size() * sizeof(float2), cudaMemcpyHostToDevice,
+                             c->st)) != cudaSuccess ||
+        (e = matvec_prepare(c->L, c->tile_x, c->rows_g)) != cudaSuccess ||
+        (e = post_prepare(j_max, l_max)) != cudaSuccess ||
+        (e = green_build_octant(i_max, j_max, l_max, kd, c->ahat, c->st)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(c->st)) != cudaSuccess)
+        return bail(fail(DDAGPU_ECUDA, std::string("setup: ") + cudaGetErrorString(e)));
+    *out = c;
+    return DDAGPU_OK;
+}
+
+int ddagpu_destroy(ddagpu_ctx *c)
+{
+    if (!c) return DDAGPU_OK;
+    DevGuard dg(c->dev);
+    if (c->st) cudaStreamSynchronize(c->st);
+    void *ptrs[] = {c->ahat, c->tw,     c->work,   c->p,       c->pmin,   c->r,     c->s,
+                    c->w,    c->g,      c->h,      c->state,   c->active, c->trace, c->occ,
+                    c->mv,   c->alpha,  c->kinc,   c->einc,    c->ksc,    c->esc_acc,
+                    c->cc_acc, c->normals, c->mueller, c->esc, c->cabs,   c->cext};
+    for (void *q : ptrs)
+        if (q) cudaFree(q);
+    if (c->st) cudaStreamDestroy(c->st);
+    delete c;
+    return DDAGPU_OK;
+}
+
+int ddagpu_set_green(ddagpu_ctx *c, const float *cmA)
+{
+    if (!c || !cmA) return fail(DDAGPU_EINVAL, "null argument");
+    std::lock_guard<std::mutex> lk(c->mu);
+    DevGuard dg(c->dev);
+    const size_t n = (size_t)8 * c->N * 6;
+    float2 *dense = nullptr;
+    CK(dalloc(&dense, n));
+    cudaError_t e = cudaMemcpyAsync(dense, cmA, n * sizeof(float2), cudaMemcpyHostToDevice, c->st);
+    if (e == cudaSuccess) e = green_project_dense(c->ni, c->nj, c->nl, dense, c->ahat, c->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
+    cudaFree(dense);
+    CK(e);
+    return DDAGPU_OK;
+}
+
+void *ddagpu_stream(ddagpu_ctx *c) { return c ? (void *)c->st : nullptr; }
+
+long long ddagpu_kernel_launches(ddagpu_ctx *c) { return c ? c->launches : -1; }
+
+int ddagpu_set_tiling(ddagpu_ctx *c, int tile_x, int rows_g)
+{
+    if (!c) return fail(DDAGPU_EINVAL, "null context");
+    std::lock_guard<std::mutex> lk(c->mu);
+    DevGuard dg(c->dev);
+    int tx = tile_x ? tile_x : c->tile_x, rg = rows_g ? rows_g : c->rows_g;
+    if (tx < 1 || (2 * c->nl) % tx != 0 || (tx & (tx - 1)) != 0)
+        return fail(DDAGPU_EINVAL, "tile_x must be a power of two dividing 2 l_max");
+    if (rg < 1 || c->nj % rg != 0 || (rg & (rg - 1)) != 0)
+        return fail(DDAGPU_EINVAL, "rows_g must be a power of two dividing j_max");
+    if (matvec_smem_x(c->L, tx) > 227 * 1024 || matvec_smem_yz(c->L, rg) > 227 * 1024)
+        return fail(DDAGPU_EINVAL, "tiling exceeds shared memory");
+    CK(matvec_prepare(c->L, tx, rg));
+    c->tile_x = tx;
+    c->rows_g = rg;
+    return DDAGPU_OK;
+}
+
+int ddagpu_get_tiling(ddagpu_ctx *c, int *tile_x, int *rows_g)
+{
+    if (!c) return fail(DDAGPU_EINVAL, "null context");
+    if (tile_x) *tile_x = c->tile_x;
+    if (rows_g) *rows_g = c->rows_g;
+    return DDAGPU_OK;
+}
+
+int ddagpu_convolution_dev(ddagpu_ctx *c, const void *p_dev, void *out_dev, int nrhs, int conj)
+{
+    if (!c || !p_dev || !out_dev) return fail(DDAGPU_EINVAL, "null argument");
+    if (nrhs < 1 || nrhs > c->cap) return fail(DDAGPU_EINVAL, "nrhs outside 1..max_rhs");
+    DevGuard dg(c->dev);
+    MatvecArgs a = mv_args(c, nrhs, (const float2 *)p_dev, (float2 *)out_dev, 0, 0.f, nullptr,
+                           conj ? 1 : 0, 1, false);
+    CK(launch_matvec(a, c->st));
+    c->launches += 3;
+    return DDAGPU_OK;
+}
+
+int ddagpu_autotune(ddagpu_ctx *c, int nrhs)
+{
+    if (!c) return fail(DDAGPU_EINVAL, "null context");
+    if (nrhs < 1 || nrhs > c->cap) nrhs = std::min(c->cap, 4);
+    DevGuard dg(c->dev);
+    // candidates: x-pass columns per CTA and y/z staging rows
+    std::vector<int> txs, rgs;
+    for (int tx = 8; tx <= 64; tx *= 2)
+        if ((2 * c->nl) % tx == 0 && matvec_smem_x(c->L, tx) <= 200 * 1024) txs.push_back(tx);
+    for (int rg = 4; rg <= 32; rg *= 2)
+        if (c->nj % rg == 0 && matvec_smem_yz(c->L, rg) <= 220 * 1024) rgs.push_back(rg);
+    if (txs.empty() || rgs.empty()) return DDAGPU_OK;
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    float best = 1e30f;
+    int btx = c->tile_x, brg = c->rows_g;
+    for (int tx : txs)
+        for (int rg : rgs) {
+            RET(ddagpu_set_tiling(c, tx, rg));
+            MatvecArgs a = mv_args(c, nrhs, c->p, c->r, 0, 0.f, nullptr, 0, 1, false);
+            for (int k = 0; k < 2; k++) CK(launch_matvec(a, c->st));
+            CK(cudaEventRecord(e0, c->st));
+            for (int k = 0; k < 5; k++) CK(launch_matvec(a, c->st));
+            CK(cudaEventRecord(e1, c->st));
+            CK(cudaEventSynchronize(e1));
+            float ms = 0;
+            CK(cudaEventElapsedTime(&ms, e0, e1));
+            if (ms < best) {
+                best = ms;
+                btx = tx;
+                brg = rg;
+            }
+        }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return ddagpu_set_tiling(c, btx, brg);
+}
+
+int ddagpu_convolution(ddagpu_ctx *c, const float *p, float *out, int conj)
+{
+    if (!c || !p || !out) return fail(DDAGPU_EINVAL, "null argument");
+    std::lock_guard<std::mutex> lk(c->mu);
+    DevGuard dg(c->dev);
+    const size_t N = c->N;
+    // AoS cvector -> SoA complex planes on the host side of the copy
+    std::vector<float2> soa(3 * N);
+    for (size_t q = 0; q < N; q++)
+        for (int k = 0; k < 3; k++) soa[k * N + q] = make_float2(p[6 * q + 2 * k], p[6 * q + 2 * k + 1]);
+    CK(cudaMemcpyAsync(c->p, soa.data(), 3 * N * sizeof(float2), cudaMemcpyHostToDevice, c->st));
+    MatvecArgs a = mv_args(c, 1, c->p, c->r, 0, 0.f, nullptr, conj ? 1 : 0, 1, false);
+    CK(launch_matvec(a, c->st));
+    CK(cudaMemcpyAsync(soa.data(), c->r, 3 * N * sizeof(float2), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    for (size_t q = 0; q < N; q++)
+        for (int k = 0; k < 3; k++) {
+            out[6 * q + 2 * k] = soa[k * N + q].x;
+            out[6 * q + 2 * k + 1] = soa[k * N + q].y;
+        }
+    return DDAGPU_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// Upload the per-solve material tables and occupancy.
+int upload_materials(ddagpu_ctx *c, const int *mv, int nmat1, const signed char *occ)
+{
+    if (nmat1 < 1 || nmat1 > c->nmat_cap) return fail(DDAGPU_EINVAL, "n_mat outside 0..254");
+    RET(check_occ(occ, c->N, nmat1));
+    c->occ_valid = false;
+    CK(cudaMemcpyAsync(c->mv, mv, nmat1 * sizeof(int), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->occ, occ, c->N, cudaMemcpyHostToDevice, c->st));
+    return DDAGPU_OK;
+}
+
+int run_post(ddagpu_ctx *c, int nrhs, int nmat1, double d0, int ndir)
+{
+    PostArgs pa{};
+    pa.N = c->N;
+    pa.nrhs = nrhs;
+    pa.ni = c->ni;
+    pa.nj = c->nj;
+    pa.nl = c->nl;
+    pa.occ = c->occ;
+    pa.mv = c->mv;
+    pa.alpha = c->alpha;
+    pa.nmat1 = nmat1;
+    pa.p = c->p;
+    pa.kinc = c->kinc;
+    pa.einc = c->einc;
+    pa.d0 = d0;
+    pa.ndir = ndir;
+    pa.ksc = c->ksc;
+    pa.esc_acc = c->esc_acc;
+    pa.cc_acc = c->cc_acc;
+    CK(launch_post(pa, c->esc, c->cabs, c->cext, c->st));
+    c->launches += ndir > 0 ? 3 : 2;
+    return DDAGPU_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ddagpu_dda_fft(ddagpu_ctx *c, int iNoIllumination, int solver, float rTau, int i_max,
+                   int j_max, int l_max, const float *cListMaterials, const int *iListMV, int n_mat,
+                   const signed char *cAlpha, int Max_Step, float Error_max, float d0,
+                   const float *kinc, const float *Einc, int iMode_FFT, int iNoScPl, int iNoA,
+                   const float *ksc, float *Esc, float *rCabs, float *rCext,
+                   ddagpu_solve_info *info, double *trace)
+{
+    (void)iNoIllumination;
+    if (!c) return fail(DDAGPU_EINVAL, "null context");
+    if (i_max != c->ni || j_max != c->nj || l_max != c->nl)
+        return fail(DDAGPU_EMISMATCH, "The workspace does not match the lattice dimensions");
+    if (!cListMaterials || !iListMV || !cAlpha || !kinc || !Einc || !rCabs || !rCext)
+        return fail(DDAGPU_EINVAL, "null argument");
+    if (iMode_FFT != 0 && iMode_FFT != 1) return fail(DDAGPU_EINVAL, "iMode_FFT must be 0 or 1");
+    if (iNoScPl < 0 || iNoA < 0 || ((size_t)iNoScPl * iNoA > 0 && (!ksc || !Esc)))
+        return fail(DDAGPU_EINVAL, "bad scattering directions");
+    std::lock_guard<std::mutex> lk(c->mu);
+    DevGuard dg(c->dev);
+    const int nmat1 = n_mat + 1, ndir = iNoScPl * iNoA;
+    RET(upload_materials(c, iListMV, nmat1, cAlpha));
+    RET(ensure_post(c, std::max(ndir, 1), std::max(iNoScPl, 1), std::max(iNoA, 1)));
+    std::vector<float2> al((size_t)nmat1);
+    for (int m = 0; m < nmat1; m++) al[(size_t)m] = make_float2(cListMaterials[2 * m], cListMaterials[2 * m + 1]);
+    double kd3[3] = {kinc[0], kinc[1], kinc[2]};
+    double ed6[6];
+    for (int k = 0; k < 6; k++) ed6[k] = Einc[k];
+    std::vector<double> kd((size_t)ndir * 3);
+    for (size_t k = 0; k < kd.size(); k++) kd[k] = ksc[k];
+    CK(cudaMemcpyAsync(c->alpha, al.data(), nmat1 * sizeof(float2), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->kinc, kd3, sizeof kd3, cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->einc, ed6, sizeof ed6, cudaMemcpyHostToDevice, c->st));
+    if (ndir) CK(cudaMemcpyAsync(c->ksc, kd.data(), kd.size() * sizeof(double), cudaMemcpyHostToDevice, c->st));
+    const int nact = count_active(cAlpha, c->N, iListMV, nmat1);
+    if (nact == 0) return fail(DDAGPU_EINVAL, "no active dipoles");
+    SolveResult res;
+    RET(run_solver(c, 1, solver, rTau, Max_Step, Error_max, nmat1, d0, nact, res, trace != nullptr));
+    RET(run_post(c, 1, nmat1, d0, ndir));
+    std::vector<float2> esc((size_t)ndir * 3);
+    float ca = 0, ce = 0;
+    if (ndir) CK(cudaMemcpyAsync(esc.data(), c->esc, esc.size() * sizeof(float2), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaMemcpyAsync(&ca, c->cabs, sizeof(float), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaMemcpyAsync(&ce, c->cext, sizeof(float), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    for (size_t k = 0; k < esc.size(); k++) {
+        Esc[2 * k] = esc[k].x;
+        Esc[2 * k + 1] = esc[k].y;
+    }
+    *rCabs = ca;
+    *rCext = ce;
+    const RhsState &S = res.st[0];
+    if (info) {
+        info->steps = S.steps;
+        info->step_min = S.step_min;
+        info->rolled_back = S.restored;
+        info->matvecs = res.matvec0 + res.matvec_it * S.steps;
+        info->err = S.err;
+        info->err_min = S.err_min;
+    }
+    if (trace)
+        for (int k = 0; k <= Max_Step; k++) trace[k] = k <= S.steps ? res.trace[(size_t)k] : 0.0;
+    return DDAGPU_OK;
+}
+
+int ddagpu_farfield(ddagpu_ctx *c, const int *iListMV, int n_mat, const signed char *cAlpha,
+                    float d0, const float *p, int ndir, const float *ksc, float *Esc)
+{
+    if (!c || !iListMV || !cAlpha || !p || (ndir > 0 && (!ksc || !Esc)) || ndir < 0)
+        return fail(DDAGPU_EINVAL, "null or bad argument");
+    std::lock_guard<std::mutex> lk(c->mu);
+    DevGuard dg(c->dev);
+    const int nmat1 = n_mat + 1;
+    RET(upload_materials(c, iListMV, nmat1, cAlpha));
+    RET(ensure_post(c, std::max(ndir, 1), 1, 1));
+    const size_t N = c->N;
+    std::vector<float2> soa(3 * N);
+    for (size_t q = 0; q < N; q++)
+        for (int k = 0; k < 3; k++) soa[k * N + q] = make_float2(p[6 * q + 2 * k], p[6 * q + 2 * k + 1]);
+    CK(cudaMemcpyAsync(c->p, soa.data(), 3 * N * sizeof(float2), cudaMemcpyHostToDevice, c->st));
+    std::vector<double> kd((size_t)ndir * 3);
+    for (size_t k = 0; k < kd.size(); k++) kd[k] = ksc[k];
+    std::vector<float2> zero_alpha((size_t)nmat1, make_float2(0.f, 0.f));
+    double z6[6] = {1, 0, 0, 0, 0, 0}, z3[3] = {0, 0, 1};
+    CK(cudaMemcpyAsync(c->alpha, zero_alpha.data(), nmat1 * sizeof(float2), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->kinc, z3, sizeof z3, cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->einc, z6, sizeof z6, cudaMemcpyHostToDevice, c->st));
+    if (ndir) CK(cudaMemcpyAsync(c->ksc, kd.data(), kd.size() * sizeof(double), cudaMemcpyHostToDevice, c->st));
+    RET(run_post(c, 1, nmat1, d0, ndir));
+    std::vector<float2> esc((size_t)ndir * 3);
+    if (ndir) CK(cudaMemcpyAsync(esc.data(), c->esc, esc.size() * sizeof(float2), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    for (size_t k = 0; k < esc.size(); k++) {
+        Esc[2 * k] = esc[k].x;
+        Esc[2 * k + 1] = esc[k].y;
+    }
+    return DDAGPU_OK;
+}
+
+int ddagpu_cabscext(ddagpu_ctx *c, float d0, const float *kinc, const float *Einc,
+                    const float *cListMaterials, int n_mat, const signed char *cAlpha,
+                    const float *p, float *Cabs, float *Cext)
+{
+    if (!c || !kinc || !Einc || !cListMaterials || !cAlpha || !p || !Cabs || !Cext)
+        return fail(DDAGPU_EINVAL, "null argument");
+    std::lock_guard<std::mutex> lk(c->mu);
+    DevGuard dg(c->dev);
+    const int nmat1 = n_mat + 1;
+    std::vector<int> mv((size_t)nmat1, 1);
+    RET(upload_materials(c, mv.data(), nmat1, cAlpha));
+    RET(ensure_post(c, 1, 1, 1));
+    const size_t N = c->N;
+    std::vector<float2> soa(3 * N);
+    for (size_t q = 0; q < N; q++)
+        for (int k = 0; k < 3; k++) soa[k * N + q] = make_float2(p[6 * q + 2 * k], p[6 * q + 2 * k + 1]);
+    CK(cudaMemcpyAsync(c->p, soa.data(), 3 * N * sizeof(float2), cudaMemcpyHostToDevice, c->st));
+    std::vector<float2> al((size_t)nmat1);
+    for (int m = 0; m < nmat1; m++) al[(size_t)m] = make_float2(cListMaterials[2 * m], cListMaterials[2 * m + 1]);
+    double kd3[3] = {kinc[0], kinc[1], kinc[2]}, ed6[6];
+    for (int k = 0; k < 6; k++) ed6[k] = Einc[k];
+    CK(cudaMemcpyAsync(c->alpha, al.data(), nmat1 * sizeof(float2), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->kinc, kd3, sizeof kd3, cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->einc, ed6, sizeof ed6, cudaMemcpyHostToDevice, c->st));
+    RET(run_post(c, 1, nmat1, d0, 0));
+    CK(cudaMemcpyAsync(Cabs, c->cabs, sizeof(float), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaMemcpyAsync(Cext, c->cext, sizeof(float), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return DDAGPU_OK;
+}
+
+int ddagpu_mueller(ddagpu_ctx *c, const float *kinc, const float *einc0, const float *einc1,
+                   int nplanes, int nangles, const float *ksc, const float *normals,
+                   const float *esc0, const float *esc1, float *out)
+{
+    if (!c || !kinc || !einc0 || !einc1 || !ksc || !normals || !esc0 || !esc1 || !out ||
+        nplanes < 1 || nangles < 1)
+        return fail(DDAGPU_EINVAL, "null or bad argument");
+    if (c->cap < 2) return fail(DDAGPU_EINVAL, "the context needs max_rhs >= 2");
+    std::lock_guard<std::mutex> lk(c->mu);
+    DevGuard dg(c->dev);
+    const int ndir = nplanes * nangles;
+    RET(ensure_post(c, ndir, nplanes, nangles));
+    std::vector<double> kd(6), ed(12), ks((size_t)2 * ndir * 3), nv((size_t)nplanes * 3);
+    for (int k = 0; k < 3; k++) kd[k] = kd[3 + k] = kinc[k];
+    for (int k = 0; k < 6; k++) {
+        ed[k] = einc0[k];
+        ed[6 + k] = einc1[k];
+    }
+    for (int k = 0; k < ndir * 3; k++) ks[k] = ks[(size_t)ndir * 3 + k] = ksc[k];
+    for (int k = 0; k < nplanes * 3; k++) nv[k] = normals[k];
+    std::vector<float2> es((size_t)2 * ndir * 3);
+    for (int k = 0; k < ndir * 3; k++) {
+        es[k] = make_float2(esc0[2 * k], esc0[2 * k + 1]);
+        es[(size_t)ndir * 3 + k] = make_float2(esc1[2 * k], esc1[2 * k + 1]);
+    }
+    CK(cudaMemcpyAsync(c->kinc, kd.data(), kd.size() * sizeof(double), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->einc, ed.data(), ed.size() * sizeof(double), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->ksc, ks.data(), ks.size() * sizeof(double), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->normals, nv.data(), nv.size() * sizeof(double), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->esc, es.data(), es.size() * sizeof(float2), cudaMemcpyHostToDevice, c->st));
+    MuellerArgs m{1, nplanes, nangles, ndir, c->kinc, c->einc, c->ksc, c->normals, c->esc, c->mueller};
+    CK(launch_mueller(m, c->st));
+    std::vector<double> mo((size_t)nangles * 16);
+    CK(cudaMemcpyAsync(mo.data(), c->mueller, mo.size() * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    for (size_t k = 0; k < mo.size(); k++) out[k] = (float)mo[k];
+    return DDAGPU_OK;
+}
+
+int ddagpu_mc_rotations(unsigned long long base_seed, int worker, int count, double *rot)
+{
+    if (!rot || count < 0 || worker < 0) return fail(DDAGPU_EINVAL, "bad argument");
+    // per-worker stream (main.cpp:803-804), xorshift64* (randomize.cpp:44-58)
+    unsigned long long s = base_seed + 0x9E3779B97F4A7C15ULL * (unsigned long long)(worker + 1);
+    if (!s) s = 0x9E3779B97F4A7C15ULL;
+    auto next = [&]() {
+        s ^= s >> 12;
+        s ^= s << 25;
+        s ^= s >> 27;
+        return (double)(int)((s * 2685821657736338717ULL) >> 33);
+    };
+    const double pi = 3.14159265358979323846264338327950288, RMAX = 2147483647.0;
+    for (int k = 0; k < count; k++) {
+        // Euler draw and rotation matrix, main.cpp:876-898
+        const double cps = next() * 2.0 / RMAX - 1.0, psi = std::acos(cps), sps = std::sin(psi);
+        const double io = next() * 2.0 * pi / RMAX, ka = next() * 2.0 * pi / RMAX;
+        const double cio = std::cos(io), sio = std::sin(io), cka = std::cos(ka), ska = std::sin(ka);
+        double *t = rot + 9 * (size_t)k;
+        t[0] = cio * cka - cps * sio * ska;
+        t[1] = sio * cka + cps * cio * ska;
+        t[2] = sps * ska;
+        t[3] = -cio * ska - cps * sio * cka;
+        t[4] = -sio * ska + cps * cio * cka;
+        t[5] = sps * cka;
+        t[6] = sps * sio;
+        t[7] = -sps * cio;
+        t[8] = cps;
+    }
+    return DDAGPU_OK;
+}
+
+int ddagpu_fixed_rotation(double psi, double iota, double kappa, double *rot)
+{
+    if (!rot) return fail(DDAGPU_EINVAL, "null argument");
+    // Z(-psi), then Y(-iota), then X(-kappa) (main.cpp:516-541, Rotation_* dda_func.cpp:7-34)
+    const double d = 3.14159265358979323846264338327950288 / 180.0;
+    const double a = -psi * d, b = -iota * d, g = -kappa * d;
+    const double Z[9] = {std::cos(a), std::sin(a), 0, -std::sin(a), std::cos(a), 0, 0, 0, 1};
+    const double Y[9] = {std::cos(b), 0, -std::sin(b), 0, 1, 0, std::sin(b), 0, std::cos(b)};
+    const double X[9] = {1, 0, 0, 0, std::cos(g), std::sin(g), 0, -std::sin(g), std::cos(g)};
+    double YZ[9];
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) {
+            YZ[3 * i + j] = 0;
+            for (int k = 0; k < 3; k++) YZ[3 * i + j] += Y[3 * i + k] * Z[3 * k + j];
+        }
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) {
+            rot[3 * i + j] = 0;
+            for (int k = 0; k < 3; k++) rot[3 * i + j] += X[3 * i + k] * YZ[3 * k + j];
+        }
+    return DDAGPU_OK;
+}
+
+int ddagpu_orientation_solves(ddagpu_ctx *c, const ddagpu_batch_cfg *cfg, int n_orient,
+                              const double *rot, double *cabs, double *cext, double *mueller,
+                              ddagpu_batch_info *info)
+{
+    if (!c || !cfg || !rot || n_orient < 0) return fail(DDAGPU_EINVAL, "null or bad argument");
+    if (c->cap < 2) return fail(DDAGPU_EINVAL, "the context needs max_rhs >= 2");
+    if (cfg->n_mat < 1 || !cfg->m || cfg->nplanes < 1 || !(cfg->theta_step > 0.f))
+        return fail(DDAGPU_EINVAL, "bad batch configuration");
+    if (cfg->polarizability < 1 || cfg->polarizability > 5)
+        return fail(DDAGPU_EINVAL, "polarizability must be 1..5");
+    std::lock_guard<std::mutex> lk(c->mu);
+    DevGuard dg(c->dev);
+    const int nA = ddagpu_num_angles(cfg->theta_min, cfg->theta_max, cfg->theta_step);
+    const int nP = cfg->nplanes, ndir = nA * nP, nmat1 = cfg->n_mat + 1;
+    if (nA < 1) return fail(DDAGPU_EINVAL, "no scattering angles");
+    RET(ensure_post(c, ndir, nP, nA));
+    // material activity (main.cpp:610-613) and occupancy, shared by every orientation
+    std::vector<int> mv((size_t)nmat1, 0);
+    for (int k = 0; k < cfg->n_mat; k++)
+        mv[(size_t)k + 1] = (cfg->m[2 * k] == 1.f && cfg->m[2 * k + 1] == 0.f) ? 0 : 1;
+    int nact = 0;
+    if (cfg->occ) {
+        RET(upload_materials(c, mv.data(), nmat1, cfg->occ));
+        nact = count_active(cfg->occ, c->N, mv.data(), nmat1);
+        c->occ_valid = true;
+        c->occ_nmat1 = nmat1;
+        c->occ_nact = nact;
+    } else {
+        // occupancy of the previous batched call, still on the device
+        if (!c->occ_valid || c->occ_nmat1 != nmat1)
+            return fail(DDAGPU_EINVAL, "cfg->occ is null and no occupancy is resident");
+        CK(cudaMemcpyAsync(c->mv, mv.data(), nmat1 * sizeof(int), cudaMemcpyHostToDevice, c->st));
+        nact = c->occ_nact;
+    }
+    if (nact == 0) return fail(DDAGPU_EINVAL, "no active dipoles");
+    const double d0 = c->kd;
+    // scattering geometry before rotation (main.cpp:336-387)
+    const double pi = 3.14159265358979323846264338327950288;
+    std::vector<double> ksc0((size_t)ndir * 3), nrm0((size_t)nP * 3);
+    for (int pl = 0; pl < nP; pl++) {
+        const double ang = pl * (180.0 / nP) * pi / 180.0, cs = std::cos(ang), sn = std::sin(ang);
+        nrm0[3 * pl + 0] = sn;
+        nrm0[3 * pl + 1] = cs;
+        nrm0[3 * pl + 2] = 0.0;
+        for (int a = 0; a < nA; a++) {
+            const double th = ((double)cfg->theta_min + (double)cfg->theta_step * a) * pi / 180.0;
+            const double k0[3] = {std::sin(th), 0.0, std::cos(th)};
+            double *k = ksc0.data() + 3 * ((size_t)pl * nA + a);
+            k[0] = cs * k0[0] + sn * k0[1];
+            k[1] = -sn * k0[0] + cs * k0[1];
+            k[2] = k0[2];
+        }
+    }
+    const int per = c->cap / 2;
+    ddagpu_batch_info bi{0, 0, 0, 0.0};
+    std::vector<double> kin, ein, ks, nv;
+    std::vector<float2> al;
+    std::vector<float> ca, ce;
+    std::vector<double> mo;
+    for (int o0 = 0; o0 < n_orient; o0 += per) {
+        const int no = std::min(per, n_orient - o0), nr = 2 * no;
+        kin.assign((size_t)nr * 3, 0.0);
+        ein.assign((size_t)nr * 6, 0.0);
+        ks.assign((size_t)nr * ndir * 3, 0.0);
+        nv.assign((size_t)no * nP * 3, 0.0);
+        al.assign((size_t)nr * nmat1, make_float2(0.f, 0.f));
+        for (int o = 0; o < no; o++) {
+            const double *T = rot + 9 * (size_t)(o0 + o);
+            auto R = [&](const double *v, double *out) {
+                for (int i = 0; i < 3; i++) out[i] = T[3 * i] * v[0] + T[3 * i + 1] * v[1] + T[3 * i + 2] * v[2];
+            };
+            const double kz[3] = {0, 0, 1}, ex[3] = {1, 0, 0}, ey[3] = {0, 1, 0};
+            double k[3], e0[3], e1[3];
+            R(kz, k);
+            R(ex, e0);
+            R(ey, e1);
+            for (int q = 0; q < 2; q++) {
+                const int rr = 2 * o + q;
+                const double *e = q ? e1 : e0;
+                for (int i = 0; i < 3; i++) {
+                    kin[3 * rr + i] = k[i];
+                    ein[6 * rr + 2 * i] = e[i];
+                    ein[6 * rr + 2 * i + 1] = 0.0;
+                }
+                for (int d = 0; d < ndir; d++) R(ksc0.data() + 3 * d, ks.data() + ((size_t)rr * ndir + d) * 3);
+                for (int mm = 0; mm < cfg->n_mat; mm++) {
+                    const cd a = polarizability(cfg->polarizability, d0, {cfg->m[2 * mm], cfg->m[2 * mm + 1]},
+                                                kin.data() + 3 * rr, ein.data() + 6 * rr);
+                    al[(size_t)rr * nmat1 + mm + 1] = make_float2((float)a.r, (float)a.i);
+                }
+            }
+            for (int pl = 0; pl < nP; pl++) R(nrm0.data() + 3 * pl, nv.data() + ((size_t)o * nP + pl) * 3);
+        }
+        CK(cudaMemcpyAsync(c->kinc, kin.data(), kin.size() * sizeof(double), cudaMemcpyHostToDevice, c->st));
+        CK(cudaMemcpyAsync(c->einc, ein.data(), ein.size() * sizeof(double), cudaMemcpyHostToDevice, c->st));
+        CK(cudaMemcpyAsync(c->ksc, ks.data(), ks.size() * sizeof(double), cudaMemcpyHostToDevice, c->st));
+        CK(cudaMemcpyAsync(c->normals, nv.data(), nv.size() * sizeof(double), cudaMemcpyHostToDevice, c->st));
+        CK(cudaMemcpyAsync(c->alpha, al.data(), al.size() * sizeof(float2), cudaMemcpyHostToDevice, c->st));
+        SolveResult res;
+        RET(run_solver(c, nr, cfg->solver, cfg->tau, cfg->max_step, cfg->err_max, nmat1, d0, nact, res, false));
+        RET(run_post(c, nr, nmat1, d0, ndir));
+        MuellerArgs m{no, nP, nA, ndir, c->kinc, c->einc, c->ksc, c->normals, c->esc, c->mueller};
+        CK(launch_mueller(m, c->st));
+        c->launches += 1;
+        ca.resize((size_t)nr);
+        ce.resize((size_t)nr);
+        mo.resize((size_t)no * nA * 16);
+        CK(cudaMemcpyAsync(ca.data(), c->cabs, nr * sizeof(float), cudaMemcpyDeviceToHost, c->st));
+        CK(cudaMemcpyAsync(ce.data(), c->cext, nr * sizeof(float), cudaMemcpyDeviceToHost, c->st));
+        if (mueller)
+            CK(cudaMemcpyAsync(mo.data(), c->mueller, mo.size() * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+        CK(cudaStreamSynchronize(c->st));
+        for (int o = 0; o < no; o++) {
+            if (cabs) cabs[o0 + o] = 0.5 * ca[2 * o] + 0.5 * ca[2 * o + 1];
+            if (cext) cext[o0 + o] = 0.5 * ce[2 * o] + 0.5 * ce[2 * o + 1];
+        }
+        if (mueller) std::memcpy(mueller + (size_t)o0 * nA * 16, mo.data(), mo.size() * sizeof(double));
+        bi.n_rhs += nr;
+        for (const RhsState &S : res.st) {
+            bi.max_steps = std::max(bi.max_steps, S.steps);
+            bi.rolled_back += S.restored;
+            bi.max_err = std::max(bi.max_err, S.restored ? S.err_min : S.err);
+        }
+    }
+    if (info) *info = bi;
+    return DDAGPU_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,292 @@
+// Post-processing of the solved dipoles: extinction and absorption cross sections
+// (CabsCext, dda_func.cpp:1679-1727), the far-field amplitude sums (FarField,
+// dda_func.cpp:1576-1625), and the Jones -> Mueller conversion averaged over scattering
+// planes (BuildMatrixJones and JonesToMuller, mmuller.cpp:175-314; averaging
+// main.cpp:943-954).
+//
+// The far field is computed as S(k) = sum_d exp(i k.(r_d - c)) P_d followed by one
+// projection S - k (k.S), equal by linearity to the reference's per-dipole projection.
+// The phase is separable, exp(i kx x) exp(i ky y) exp(i kz z), so each CTA builds small
+// tables and the inner loop is three complex multiply-adds per dipole and direction.
+#include "common.cuh"
+#include "internal.h"
+#include "post.h"
+
+namespace ddagpu {
+
+namespace {
+
+constexpr int FF_DIRS = 32;   // directions per CTA (one per lane)
+constexpr int FF_ROWS = 16;   // lattice rows staged per round
+
+// grid (dir chunks, ni, nrhs), 256 threads: lane = direction, warp = row of the slab
+__global__ void __launch_bounds__(256) farfield_sum(PostArgs a)
+{
+    extern __shared__ float2 sm[];
+    const int nj = a.nj, nl = a.nl;
+    const int dbase = blockIdx.x * FF_DIRS, i = blockIdx.y, rhs = blockIdx.z;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    float2 *ez = sm;                       // [nl][32]
+    float2 *ey = ez + nl * FF_DIRS;        // [nj][32]
+    float2 *P = ey + nj * FF_DIRS;         // [FF_ROWS][nl][3]
+    __shared__ float2 ex[FF_DIRS];
+    __shared__ double red[8][FF_DIRS][6];
+    const double cx = (a.ni - 1) * a.d0 / 2, cy = (nj - 1) * a.d0 / 2, cz = (nl - 1) * a.d0 / 2;
+    const double *K = a.ksc + (size_t)rhs * a.ndir * 3;
+    for (int e = threadIdx.x; e < (nl + nj + 1) * FF_DIRS; e += blockDim.x) {
+        const int dl = e % FF_DIRS, pos = e / FF_DIRS, d = dbase + dl;
+        float2 val = czero();
+        if (d < a.ndir) {
+            double ph;
+            if (pos < nl) ph = K[3 * d + 2] * (pos * a.d0 - cz);
+            else if (pos < nl + nj) ph = K[3 * d + 1] * ((pos - nl) * a.d0 - cy);
+            else ph = K[3 * d + 0] * (i * a.d0 - cx);
+            double s, c;
+            sincos(ph, &s, &c);
+            val = make_float2((float)c, (float)s);
+        }
+        if (pos < nl) ez[pos * FF_DIRS + dl] = val;
+        else if (pos < nl + nj) ey[(pos - nl) * FF_DIRS + dl] = val;
+        else ex[dl] = val;
+    }
+    const size_t N = a.N;
+    const float2 *p = a.p + (size_t)rhs * 3 * N + (size_t)i * nj * nl;
+    const signed char *occ = a.occ + (size_t)i * nj * nl;
+    float2 acc0 = czero(), acc1 = czero(), acc2 = czero();
+    for (int j0 = 0; j0 < nj; j0 += FF_ROWS) {
+        const int rows = nj - j0 < FF_ROWS ? nj - j0 : FF_ROWS;
+        __syncthreads();
+        for (int e = threadIdx.x; e < rows * nl; e += blockDim.x) {
+            const size_t q = (size_t)j0 * nl + e;
+            const bool act = a.mv[(int)occ[q]] != 0;
+#pragma unroll
+            for (int c = 0; c < 3; c++) P[e * 3 + c] = act ? p[c * N + q] : czero();
+        }
+        __syncthreads();
+        for (int rr = warp; rr < rows; rr += nw) {
+            float2 t0 = czero(), t1 = czero(), t2 = czero();
+            const float2 *row = P + (size_t)rr * nl * 3;
+#pragma unroll 4
+            for (int l = 0; l < nl; l++) {
+                const float2 e = ez[l * FF_DIRS + lane];
+                t0 = cadd(t0, cmul(e, row[3 * l + 0]));
+                t1 = cadd(t1, cmul(e, row[3 * l + 1]));
+                t2 = cadd(t2, cmul(e, row[3 * l + 2]));
+            }
+            const float2 eyv = ey[(j0 + rr) * FF_DIRS + lane];
+            acc0 = cadd(acc0, cmul(eyv, t0));
+            acc1 = cadd(acc1, cmul(eyv, t1));
+            acc2 = cadd(acc2, cmul(eyv, t2));
+        }
+    }
+    const float2 exv = ex[lane];
+    acc0 = cmul(exv, acc0);
+    acc1 = cmul(exv, acc1);
+    acc2 = cmul(exv, acc2);
+    red[warp][lane][0] = acc0.x; red[warp][lane][1] = acc0.y;
+    red[warp][lane][2] = acc1.x; red[warp][lane][3] = acc1.y;
+    red[warp][lane][4] = acc2.x; red[warp][lane][5] = acc2.y;
+    __syncthreads();
+    if (threadIdx.x < FF_DIRS * 6) {
+        const int dl = threadIdx.x / 6, k = threadIdx.x % 6, d = dbase + dl;
+        double s = 0.0;
+        for (int w = 0; w < nw; w++) s += red[w][dl][k];
+        if (d < a.ndir && s != 0.0) atomicAdd(a.esc_acc + ((size_t)rhs * a.ndir + d) * 6 + k, s);
+    }
+}
+
+// Cext and Cabs sums (before the 4 pi / |E|^2 factor), grid (ni, nrhs)
+__global__ void __launch_bounds__(256) cabs_cext_sum(PostArgs a)
+{
+    extern __shared__ float2 tab[];   // [nj] then [nl]
+    __shared__ double scratch[8 * 2];
+    const int i = blockIdx.x, rhs = blockIdx.y, nj = a.nj, nl = a.nl;
+    const double *k = a.kinc + 3 * rhs, *E = a.einc + 6 * rhs;
+    // centre n d0 / 2 (dda_func.cpp:1685), phase -k.(r - c')
+    const double cx = a.ni * a.d0 / 2, cy = nj * a.d0 / 2, cz = nl * a.d0 / 2;
+    for (int e = threadIdx.x; e < nj + nl; e += blockDim.x) {
+        const double ph = e < nj ? -k[1] * (e * a.d0 - cy) : -k[2] * ((e - nj) * a.d0 - cz);
+        double s, c;
+        sincos(ph, &s, &c);
+        tab[e] = make_float2((float)c, (float)s);
+    }
+    __syncthreads();
+    double sx, cxx;
+    sincos(-k[0] * (i * a.d0 - cx), &sx, &cxx);
+    const float2 exv = make_float2((float)cxx, (float)sx);
+    const size_t N = a.N;
+    const float2 *p = a.p + (size_t)rhs * 3 * N;
+    const float2 *al = a.alpha + (size_t)rhs * a.nmat1;
+    double v[2] = {0.0, 0.0};
+    for (int e = threadIdx.x; e < nj * nl; e += blockDim.x) {
+        const size_t q = (size_t)i * nj * nl + e;
+        const int m = a.occ[q];
+        const float2 alpha = al[m];
+        if (alpha.x == 0.f && alpha.y == 0.f) continue;
+        const int j = e / nl, l = e - j * nl;
+        double per = 0.0, pei = 0.0, pp = 0.0;
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            const float2 P = p[c * N + q];
+            const double er = E[2 * c], ei = -E[2 * c + 1];   // conj(E)
+            per += P.x * er - P.y * ei;
+            pei += P.x * ei + P.y * er;
+            pp += (double)P.x * P.x + (double)P.y * P.y;
+        }
+        const float2 ph = cmul(cmul(exv, tab[j]), tab[nj + l]);
+        v[0] += (double)ph.x * pei + (double)ph.y * per;   // Im(ph * (P . conj E))
+        const double ar = alpha.x, ai = alpha.y;
+        v[1] += pp * ai / (ar * ar + ai * ai) - (2.0 / 3.0) * pp;   // Im(pp / conj(alpha)) - 2/3 pp
+    }
+    block_sum_atomic<2>(v, scratch, a.cc_acc + 2 * rhs);
+}
+
+// Esc = S - k (k.S); Cext, Cabs = 4 pi / |E|^2 * sums
+__global__ void post_finalize(PostArgs a, float2 *esc, float *cabs, float *cext)
+{
+    const size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    const size_t nd = (size_t)a.nrhs * a.ndir;
+    if (q < nd) {
+        const double *K = a.ksc + 3 * q, *S = a.esc_acc + 6 * q;
+        const double kr = K[0] * S[0] + K[1] * S[2] + K[2] * S[4];
+        const double ki = K[0] * S[1] + K[1] * S[3] + K[2] * S[5];
+        for (int c = 0; c < 3; c++)
+            esc[3 * q + c] = make_float2((float)(S[2 * c] - K[c] * kr), (float)(S[2 * c + 1] - K[c] * ki));
+    }
+    if (q < (size_t)a.nrhs && cabs && cext) {
+        const double *E = a.einc + 6 * q;
+        double e2 = 0.0;
+        for (int c = 0; c < 6; c++) e2 += E[c] * E[c];
+        const double r0 = 4.0 * 3.14159265358979323846 / e2;
+        cext[q] = (float)(r0 * a.cc_acc[2 * q]);
+        cabs[q] = (float)(r0 * a.cc_acc[2 * q + 1]);
+    }
+}
+
+struct dc {
+    double r, i;
+};
+__device__ inline dc dcm(dc a, dc b) { return {a.r * b.r - a.i * b.i, a.r * b.i + a.i * b.r}; }
+__device__ inline dc dcs(dc a, dc b) { return {a.r - b.r, a.i - b.i}; }
+__device__ inline dc dca(dc a, dc b) { return {a.r + b.r, a.i + b.i}; }
+__device__ inline dc dcc(dc a) { return {a.r, -a.i}; }
+__device__ inline dc dcdiv(dc a, dc b)
+{
+    const double d = b.r * b.r + b.i * b.i;
+    return {(a.r * b.r + a.i * b.i) / d, (a.i * b.r - a.r * b.i) / d};
+}
+__device__ inline dc rdotc(const double *v, const dc *e)
+{
+    return {v[0] * e[0].r + v[1] * e[1].r + v[2] * e[2].r, v[0] * e[0].i + v[1] * e[1].i + v[2] * e[2].i};
+}
+
+// One Mueller matrix per (orientation, angle), averaged over the scattering planes.
+// The two polarisations of orientation o are right-hand sides 2o and 2o+1.
+__global__ void mueller_avg(MuellerArgs m)
+{
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= m.norient * m.nangles) return;
+    const int o = q / m.nangles, ang = q % m.nangles;
+    const double *ki = m.kinc + 6 * o;      // rhs 2o
+    double M[16];
+    for (int k = 0; k < 16; k++) M[k] = 0.0;
+    dc E0[3], E1[3];
+    for (int c = 0; c < 3; c++) {
+        E0[c] = {m.einc[12 * o + 2 * c], m.einc[12 * o + 2 * c + 1]};
+        E1[c] = {m.einc[12 * o + 6 + 2 * c], m.einc[12 * o + 6 + 2 * c + 1]};
+    }
+    for (int pl = 0; pl < m.nplanes; pl++) {
+        const size_t dir = (size_t)pl * m.nangles + ang;
+        const double *ks = m.ksc + ((size_t)(2 * o) * m.ndir + dir) * 3;
+        const double *nv = m.normals + ((size_t)o * m.nplanes + pl) * 3;
+        const float2 *s0 = m.esc + ((size_t)(2 * o) * m.ndir + dir) * 3;
+        const float2 *s1 = m.esc + ((size_t)(2 * o + 1) * m.ndir + dir) * 3;
+        dc S0[3], S1[3];
+        for (int c = 0; c < 3; c++) {
+            S0[c] = {s0[c].x, s0[c].y};
+            S1[c] = {s1[c].x, s1[c].y};
+        }
+        // plane basis: across = normal, along = (k x n)/|k x n| for the incident beam and
+        // -(k_sc x n)/|k_sc x n| for the scattered one (mmuller.cpp:181-182)
+        double pin[3] = {ki[1] * nv[2] - ki[2] * nv[1], ki[2] * nv[0] - ki[0] * nv[2],
+                         ki[0] * nv[1] - ki[1] * nv[0]};
+        double psc[3] = {ks[1] * nv[2] - ks[2] * nv[1], ks[2] * nv[0] - ks[0] * nv[2],
+                         ks[0] * nv[1] - ks[1] * nv[0]};
+        const double a1 = sqrt(pin[0] * pin[0] + pin[1] * pin[1] + pin[2] * pin[2]);
+        const double a2 = sqrt(psc[0] * psc[0] + psc[1] * psc[1] + psc[2] * psc[2]);
+        for (int c = 0; c < 3; c++) {
+            pin[c] /= a1;
+            psc[c] = -psc[c] / a2;
+        }
+        const dc i0n = rdotc(nv, E0), i1n = rdotc(nv, E1), i0p = rdotc(pin, E0), i1p = rdotc(pin, E1);
+        const dc det = dcs(dcm(i0n, i1p), dcm(i1n, i0p));
+        const dc den = {-det.i, det.r};   // i * det
+        const dc s0n = rdotc(nv, S0), s1n = rdotc(nv, S1), s0p = rdotc(psc, S0), s1p = rdotc(psc, S1);
+        const dc A = dcdiv(dcs(dcm(s1p, i0n), dcm(s0p, i1n)), den);
+        const dc B = dcdiv(dcs(dcm(s0p, i1p), dcm(s1p, i0p)), den);
+        const dc C = dcdiv(dcs(dcm(s1n, i0n), dcm(s0n, i1n)), den);
+        const dc D = dcdiv(dcs(dcm(s0n, i1p), dcm(s1n, i0p)), den);
+        const double aa = A.r * A.r + A.i * A.i, bb = B.r * B.r + B.i * B.i,
+                     cc = C.r * C.r + C.i * C.i, dd = D.r * D.r + D.i * D.i;
+        const dc ab = dcm(A, dcc(B)), dc_ = dcm(D, dcc(C)), ac = dcm(A, dcc(C)),
+                 db = dcm(D, dcc(B)), da = dcm(D, dcc(A)), bc = dcm(B, dcc(C)),
+                 ad = dcm(A, dcc(D)), cb = dcm(C, dcc(B)), ca = dcm(C, dcc(A));
+        // JonesToMuller, mmuller.cpp:254-314
+        M[0] += 0.5 * (aa + bb + cc + dd);
+        M[1] += 0.5 * (aa - bb + cc - dd);
+        M[2] += dca(ab, dc_).r;
+        M[3] += dcs(ab, dc_).i;
+        M[4] += 0.5 * (aa + bb - cc - dd);
+        M[5] += 0.5 * (aa - bb - cc + dd);
+        M[6] += dcs(ab, dc_).r;
+        M[7] += dca(ab, dc_).i;
+        M[8] += dca(ac, db).r;
+        M[9] += dcs(ac, db).r;
+        M[10] += dca(da, bc).r;
+        M[11] += dca(ad, cb).i;
+        M[12] += dca(ca, db).i;
+        M[13] += dcs(ca, db).i;
+        M[14] += dcs(da, bc).i;
+        M[15] += dcs(da, bc).r;
+    }
+    for (int k = 0; k < 16; k++) m.out[(size_t)q * 16 + k] = M[k] / m.nplanes;
+}
+
+inline unsigned nblk(size_t n, int t) { return (unsigned)((n + t - 1) / t); }
+
+}  // namespace
+
+size_t farfield_smem(int nj, int nl)
+{
+    return ((size_t)(nl + nj) * FF_DIRS + (size_t)FF_ROWS * nl * 3) * sizeof(float2);
+}
+
+cudaError_t post_prepare(int nj, int nl)
+{
+    return cudaFuncSetAttribute(farfield_sum, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)farfield_smem(nj, nl));
+}
+
+cudaError_t launch_post(const PostArgs &a, float2 *esc, float *cabs, float *cext, cudaStream_t st)
+{
+    cudaError_t e;
+    if ((e = cudaMemsetAsync(a.esc_acc, 0, (size_t)a.nrhs * a.ndir * 6 * sizeof(double), st))) return e;
+    if ((e = cudaMemsetAsync(a.cc_acc, 0, (size_t)a.nrhs * 2 * sizeof(double), st))) return e;
+    if (a.ndir > 0)
+        farfield_sum<<<dim3(nblk(a.ndir, FF_DIRS), a.ni, a.nrhs), 256, farfield_smem(a.nj, a.nl), st>>>(a);
+    cabs_cext_sum<<<dim3(a.ni, a.nrhs), 256, (a.nj + a.nl) * sizeof(float2), st>>>(a);
+    const size_t nd = (size_t)a.nrhs * a.ndir;
+    const size_t nt = nd > (size_t)a.nrhs ? nd : (size_t)a.nrhs;
+    post_finalize<<<nblk(nt, 256), 256, 0, st>>>(a, esc, cabs, cext);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_mueller(const MuellerArgs &m, cudaStream_t st)
+{
+    const size_t n = (size_t)m.norient * m.nangles;
+    if (n == 0) return cudaSuccess;
+    mueller_avg<<<nblk(n, 128), 128, 0, st>>>(m);
+    return cudaGetLastError();
+}
+
+}  // namespace ddagpu

@@ -1,0 +1,44 @@
+// Solver kernels of libddagpu: operation codes and launchers.
+#pragma once
+#include "internal.h"
+
+namespace ddagpu {
+
+enum FieldOp {
+    OP_STEP0_CG = 1, OP_STEP0_AA, OP_STEP0_BICG, OP_STEP0_SIMPLE,
+    OP_CG1, OP_CG2, OP_CG3,
+    OP_AA1, OP_AA2, OP_AA3,
+    OP_B_RHO, OP_B_S, OP_B_GH, OP_B_R, OP_B_WW, OP_B_P,
+    OP_SIMPLE, OP_ERR
+};
+
+enum ScalarStage {
+    SC_STEP0_ERR1 = 1, SC_STEP0_AA, SC_B_RHO1,
+    SC_CG1, SC_CG2, SC_AA1, SC_AA2, SC_B1, SC_B2, SC_B3, SC_B4, SC_ERR1,
+    SC_START, SC_TOP, SC_FINAL
+};
+
+struct FieldArgs {
+    size_t N;
+    int nrhs;
+    int ni, nj, nl;
+    const signed char *occ;   // [N]
+    const int *mv;            // [nmat1]
+    const float2 *alpha;      // [nrhs][nmat1]
+    int nmat1;
+    RhsState *st;             // [nrhs]
+    const int *rhs_active;    // [nrhs] or null
+    float2 *p, *pmin, *r, *s, *g, *h, *w;  // [nrhs][3][N]
+    const double *kinc;       // [nrhs][3]
+    const double *einc;       // [nrhs][6]
+    double d0;
+    float tau;
+};
+
+cudaError_t launch_field_op(int op, const FieldArgs &a, cudaStream_t st);
+cudaError_t launch_first_approx(const FieldArgs &a, cudaStream_t st);
+cudaError_t launch_scalar(RhsState *st_, const int *act_in, int *act_out, int nrhs, int stage,
+                          int step, double *trace, int trace_len, cudaStream_t st);
+cudaError_t launch_gated_copy(const FieldArgs &a, int dir, cudaStream_t st);
+
+}  // namespace ddagpu

@@ -1,0 +1,166 @@
+/*
+ * ddagpu.h -- C ABI of libddagpu, the B200 (sm_100a) implementation of the DDA-FFT hot
+ * path of physicist2018/dda-fft v7.2: the zero-padded FFT convolution A*p inside the
+ * CG / AA* / BiCGStab / simple-iteration solvers, the solver updates and reductions,
+ * the far-field sums, the cross sections and the Jones -> Mueller averaging.
+ *
+ * Plain pointers and sizes only.  Unless a name ends in _dev, array arguments are HOST
+ * memory in the reference's own layouts:
+ *   field    [i_max][j_max][l_max] cvector  = 6 floats per cell (x.re x.im y.re y.im z.re z.im)
+ *   cmA      [2 i_max][2 j_max][2 l_max] cmatrix = 12 floats per cell (e00 e01 e02 e11 e12 e22)
+ *   cAlpha   [i_max][j_max][l_max] signed char material index, 0 = empty cell
+ *   ksc      [planes][angles] vector (3 floats), Esc [planes][angles] cvector (6 floats)
+ * _dev entry points take DEVICE pointers in the structure-of-arrays layout
+ * [rhs][component][i][j][l] of complex float.
+ *
+ * Every function returns DDAGPU_OK (0) or a negative code; ddagpu_last_error() gives the
+ * message of the last failure on the calling thread.  The reference never returns an error
+ * (it exits on out-of-memory and on a workspace mismatch, dda_func.cpp:1006-1008,
+ * 1091-1094); a host adapter maps the codes to those exits.  A context may be used from one
+ * thread at a time (calls on one context are serialised by a lock); separate contexts on
+ * the same device run concurrently, like the reference's worker workspaces
+ * (main.cpp:777-995).
+ */
+#ifndef DDAGPU_H
+#define DDAGPU_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DDAGPU_OK 0
+#define DDAGPU_EINVAL (-1)     /* invalid argument (sizes, solver, null pointer)          */
+#define DDAGPU_ENOMEM (-2)     /* device allocation failed (reference: exit(1))          */
+#define DDAGPU_ECUDA (-3)      /* a CUDA call failed                                       */
+#define DDAGPU_EMISMATCH (-4)  /* lattice differs from the context (reference: exit(1)) */
+#define DDAGPU_ENOTBUILT (-5)  /* no CUDA device / library built without kernels           */
+
+typedef struct ddagpu_ctx ddagpu_ctx;
+
+/* Result details of one solve (the reference prints these, dda_func.cpp:1281,1524-1548). */
+typedef struct {
+    int steps;          /* iterations performed after step 0                           */
+    int step_min;       /* step of the best iterate                                     */
+    int rolled_back;    /* 1 if the final iterate was replaced by the best one          */
+    int matvecs;        /* convolutions performed                                       */
+    double err;         /* final discrepancy (mean residual norm, ldError)              */
+    double err_min;     /* smallest discrepancy seen                                    */
+} ddagpu_solve_info;
+
+const char *ddagpu_version(void);
+const char *ddagpu_last_error(void);
+
+/* Creates a context for one lattice on one CUDA device, builds the Green tensor FFT from kd
+ * on the device, and reserves work space for up to max_rhs right-hand sides solved
+ * together.  Replaces CreateAMatrix + FFT_3D(cmA) (main.cpp:466-486, dda_func.cpp:85-148,
+ * fft_func.cpp:317-416) and dda_workspace_create (dda_func.cpp:1031-1054).
+ * Lattice edges: powers of two in [2, 128]. */
+int ddagpu_create(ddagpu_ctx **ctx, int device, int i_max, int j_max, int l_max, double kd,
+                  int max_rhs);
+int ddagpu_destroy(ddagpu_ctx *ctx);
+
+/* Replaces the Green tensor with a host-built cmA (the reference's own, main.cpp:466-486),
+ * e.g. for bit-level comparisons.  It is projected on the symmetric octant the kernels
+ * store; the projection changes only convolution outputs outside the lattice. */
+int ddagpu_set_green(ddagpu_ctx *ctx, const float *cmA);
+
+/* Convolution sub-seam (dda_func.cpp:150-187; conj != 0: Convolution_conj, 227-437):
+ * out = G * p on the lattice, p and out host fields. */
+int ddagpu_convolution(ddagpu_ctx *ctx, const float *p, float *out, int conj);
+
+/* The DDA_FFT seam (function.hpp:153-160, dda_func.cpp:1075-1570): solves one
+ * polarisation with solver 0 CG, 1 AA*, 2 BiCGStab, 3 simple iteration (weight rTau), to
+ * the reference's absolute Error_max rule with best-iterate rollback, then CabsCext and the
+ * far field at every (plane, angle).  cListMaterials: n_mat+1 complex polarisabilities
+ * (index 0 = empty); iListMV: n_mat+1 active flags.  The FFT tables of the reference's
+ * signature are not needed; iMode_FFT is accepted for both CT (0) and RB (1), which give
+ * the same convolution.  trace (optional, Max_Step+1 doubles) receives the discrepancy of
+ * every step. */
+int ddagpu_dda_fft(ddagpu_ctx *ctx, int iNoIllumination, int iMode_SolutionMethod, float rTau,
+                   int i_max, int j_max, int l_max, const float *cListMaterials,
+                   const int *iListMV, int n_mat, const signed char *cAlpha, int Max_Step,
+                   float Error_max, float d0, const float *kinc, const float *Einc,
+                   int iMode_FFT, int iNoScPl, int iNoA, const float *ksc, float *Esc,
+                   float *rCabs, float *rCext, ddagpu_solve_info *info, double *trace);
+
+/* FarField sub-seam (dda_func.cpp:1576-1625) for ndir directions at once. */
+int ddagpu_farfield(ddagpu_ctx *ctx, const int *iListMV, int n_mat, const signed char *cAlpha,
+                    float d0, const float *p, int ndir, const float *ksc, float *Esc);
+
+/* CabsCext sub-seam (dda_func.cpp:1679-1727). */
+int ddagpu_cabscext(ddagpu_ctx *ctx, float d0, const float *kinc, const float *Einc,
+                    const float *cListMaterials, int n_mat, const signed char *cAlpha,
+                    const float *p, float *Cabs, float *Cext);
+
+/* BuildMatrixJones + JonesToMuller averaged over planes (mmuller.cpp:175-314,
+ * main.cpp:943-954) for one orientation: esc0/esc1 [planes][angles] cvector of the two
+ * polarisations, ksc [planes][angles] vector, normals [planes] vector; out [angles][16]. */
+int ddagpu_mueller(ddagpu_ctx *ctx, const float *kinc, const float *einc0, const float *einc1,
+                   int nplanes, int nangles, const float *ksc, const float *normals,
+                   const float *esc0, const float *esc1, float *out);
+
+/* ---------------------------------------------------------------- batched solves
+ * One call runs many orientations of one target: both polarisations of every orientation
+ * are right-hand sides of one batched solve that shares the Green tensor, the occupancy
+ * and the FFT passes (the sample loop of main.cpp:806-985 for targets whose geometry does
+ * not change between samples). */
+typedef struct {
+    int solver;              /* 0..3                                                   */
+    float tau;               /* simple-iteration weight                                */
+    int max_step;            /* Max_Step                                               */
+    float err_max;           /* Error_max (absolute, dda_func.cpp:1302)                */
+    int polarizability;      /* 1 CM, 2 CMRR, 3 CMNR, 4 ILDR, 5 LDR                    */
+    int n_mat;               /* materials 1..n_mat                                     */
+    const float *m;          /* refractive indices, 2 n_mat floats (re, im)            */
+    const signed char *occ;  /* host occupancy [i][j][l]; NULL reuses the occupancy of
+                                the previous batched call, still resident on the device */
+    int nplanes;             /* scattering planes (main.cpp:377-387)                   */
+    float theta_min, theta_max, theta_step; /* degrees (main.cpp:195-200)              */
+} ddagpu_batch_cfg;
+
+typedef struct {
+    int n_rhs;               /* right-hand sides solved                               */
+    int max_steps;           /* largest iteration count of any right-hand side        */
+    int rolled_back;         /* right-hand sides whose best iterate was restored      */
+    double max_err;          /* largest final discrepancy                              */
+} ddagpu_batch_info;
+
+/* n_orient rotations rot[n_orient][9] (row-major VectTrans of main.cpp:885-898, or the
+ * fixed Z(-psi) Y(-iota) X(-kappa) product of main.cpp:516-541) -> per orientation
+ * Cabs, Cext (averages of the two polarisations, main.cpp:939) and the plane-averaged
+ * Mueller matrix mueller[n_orient][angles][16]. */
+int ddagpu_orientation_solves(ddagpu_ctx *ctx, const ddagpu_batch_cfg *cfg, int n_orient,
+                              const double *rot, double *cabs, double *cext, double *mueller,
+                              ddagpu_batch_info *info);
+
+/* Number of scattering angles for a configuration (rounding of main.cpp:201). */
+int ddagpu_num_angles(float theta_min, float theta_max, float theta_step);
+
+/* Rotation matrices of the reference's Monte-Carlo orientation sampler: worker `worker` of
+ * a run seeded base_seed (main.cpp:803-804, 876-898, randomize.cpp:44-58). */
+int ddagpu_mc_rotations(unsigned long long base_seed, int worker, int count, double *rot);
+/* Fixed orientation (degrees), main.cpp:516-541. */
+int ddagpu_fixed_rotation(double psi, double iota, double kappa, double *rot);
+
+/* ---------------------------------------------------------------- device-resident form
+ * G*p for nrhs fields already in device memory ([nrhs][3][i][j][l] complex float, SoA),
+ * on the context's stream; nrhs <= max_rhs. */
+int ddagpu_convolution_dev(ddagpu_ctx *ctx, const void *p_dev, void *out_dev, int nrhs, int conj);
+/* The context's CUDA stream (cudaStream_t), for callers that time or order work on it. */
+void *ddagpu_stream(ddagpu_ctx *ctx);
+/* Number of CUDA kernels this context has launched so far. */
+long long ddagpu_kernel_launches(ddagpu_ctx *ctx);
+/* Kernel launch parameters: columns per CTA of the x pass and rows per staging group of
+ * the y/z passes; 0 keeps the current value.  ddagpu_autotune times the candidates on the
+ * context's lattice and keeps the fastest. */
+int ddagpu_set_tiling(ddagpu_ctx *ctx, int tile_x, int rows_g);
+int ddagpu_get_tiling(ddagpu_ctx *ctx, int *tile_x, int *rows_g);
+int ddagpu_autotune(ddagpu_ctx *ctx, int nrhs);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DDAGPU_H */

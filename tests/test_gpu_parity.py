@@ -1,0 +1,265 @@
+"""GPU parity: libddagpu (through its C ABI) against the FP64 oracle and the reference's
+golden outputs.  Tolerances are written per test: the kernels compute in float32 with
+FP64 reductions, so a single convolution agrees with the FP64 oracle to ~1e-6 of its
+largest element; solver outputs are compared under the float-noise gate
+max(1e-4 relative, 2 x |float reference - FP64 reference|)."""
+import numpy as np
+import pytest
+
+from pyoracle import orientation_solves
+
+pytestmark = pytest.mark.gpu
+
+CONV_TOL = 2e-5     # max |gpu - fp64| / max |fp64| for one convolution
+
+
+def rel(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+def crand(rng, shape):
+    return (rng.standard_normal(shape) + 1j * rng.standard_normal(shape)).astype(np.complex64)
+
+
+@pytest.fixture(scope="module")
+def D():
+    import dda_fft_b200
+    return dda_fft_b200
+
+
+@pytest.mark.parametrize("grid", [(2, 2, 2), (4, 4, 4), (8, 8, 8), (16, 16, 16), (32, 32, 32),
+                                  (8, 16, 8), (16, 4, 32), (64, 64, 64)])
+@pytest.mark.parametrize("conj", [False, True])
+def test_convolution_vs_oracle(D, oracle, grid, conj):
+    rng = np.random.default_rng(sum(grid) + conj)
+    kd = 2 * 3.0 / grid[0]
+    p = crand(rng, grid + (3,))
+    with D.Context(grid, kd) as ctx:
+        out = ctx.convolution(p, conj=conj)
+    ref = oracle.convolution(oracle.green_hat(*grid, kd), p.astype(np.complex128), conj=conj)
+    assert rel(out, ref) < CONV_TOL
+
+
+@pytest.mark.parametrize("n", [8, 16])
+def test_convolution_vs_reference_golden(D, golden, n):
+    """Against the reference's own float Convolution (CT) on the golden inputs."""
+    kd = float(golden[f"conv{n}_kd"])
+    p = golden[f"conv{n}_p"]
+    with D.Context(n, kd) as ctx:
+        out = ctx.convolution(p)
+        outc = ctx.convolution(p, conj=True)
+    assert rel(out, golden[f"conv{n}_out"]) < CONV_TOL
+    assert rel(outc, golden[f"conv{n}_out_conj"]) < CONV_TOL
+
+
+def test_set_green_from_reference_cmA(D, golden):
+    """Uploading the reference's own cmA (its float Green tensor FFT) gives its output."""
+    kd = float(golden["conv8_kd"])
+    with D.Context(8, kd) as ctx:
+        ctx.set_green(golden["green8_hat"])
+        out = ctx.convolution(golden["conv8_p"])
+    assert rel(out, golden["conv8_out"]) < 2e-6
+
+
+def test_convolution_rectangular_golden(D, golden):
+    p = golden["convrect_p"]
+    with D.Context(p.shape[:3], float(golden["convrect_kd"])) as ctx:
+        out = ctx.convolution(p)
+    assert rel(out, golden["convrect_out"]) < CONV_TOL
+
+
+def _green_point(r):
+    """G(r) of CreateAMatrix (dda_func.cpp:110-141) in FP64, as a 3x3 matrix."""
+    r = np.asarray(r, float)
+    r2 = r @ r
+    r1 = np.sqrt(r2)
+    c2 = np.exp(1j * r1) / (r1 * r2)
+    return c2 * (r2 - 1 + 1j * r1) * np.eye(3) + c2 * (3 - r2 - 3j * r1) / r2 * np.outer(r, r)
+
+
+def test_convolution_128_impulse(D):
+    """Size-independent check at 128^3: the response to a point dipole is the Green tensor
+    itself, G(r - r0) e, sampled at scattered lattice points."""
+    n, kd = 128, 2 * 16.0 / 128
+    p = np.zeros((n, n, n, 3), np.complex64)
+    r0 = (37, 90, 64)
+    e = np.array([0.3 + 0.1j, -0.7, 0.2j])
+    p[r0] = e
+    with D.Context(n, kd) as ctx:
+        out = ctx.convolution(p)
+    rng = np.random.default_rng(5)
+    pts = [tuple(rng.integers(0, n, 3)) for _ in range(64)] + [(0, 0, 0), (127, 127, 127)]
+    worst, scale = 0.0, 0.0
+    for q in pts:
+        if q == r0:
+            continue
+        g = _green_point((np.array(q) - np.array(r0)) * kd) @ e
+        worst = max(worst, np.abs(out[q] - g).max())
+        scale = max(scale, np.abs(g).max())
+    assert worst < 1e-4 * scale + 1e-7
+    assert np.abs(out[r0]).max() < 1e-4 * scale + 1e-7     # G(0) = 0
+
+
+def test_convolution_linearity_128(D):
+    n, kd = 128, 0.25
+    rng = np.random.default_rng(9)
+    x = crand(rng, (n, n, n, 3))
+    y = crand(rng, (n, n, n, 3))
+    with D.Context(n, kd) as ctx:
+        a, b, c = ctx.convolution(x), ctx.convolution(y), ctx.convolution(x + 2 * y)
+    assert rel(c, a + 2 * b) < 1e-5
+
+
+@pytest.mark.parametrize("name", ["cg", "aa", "bicgstab", "simple", "simple_div"])
+def test_solver_vs_oracle_and_reference(D, golden, oracle, name):
+    g = golden
+    solver, tau, model, *einc = g[f"solve_{name}_cfg"]
+    kd = float(g["solve_kd"])
+    occ = g["solve_occ"]
+    n = occ.shape[0]
+    ksc = g["solve_ksc"]
+    alpha = g[f"solve_{name}_alpha"]
+    mv = np.array([0, 1])
+    with D.Context(n, kd) as ctx:
+        r = ctx.dda_fft(occ, alpha, mv, kd, (0, 0, 1), einc, ksc, solver=int(solver), tau=tau,
+                        max_step=8, err_max=1e-9)
+    o = oracle.dda_fft(occ, alpha.astype(np.complex128), mv, kd, (0, 0, 1), einc,
+                       oracle.green_hat(n, n, n, kd), ksc.astype(np.float64), solver=int(solver),
+                       tau=tau, max_step=8, err_max=1e-9)
+    assert len(r["trace"]) == len(o["trace"])
+    # per-step discrepancy: float solver vs FP64 oracle
+    assert np.abs(r["trace"] - o["trace"]).max() <= 2e-3 * np.abs(o["trace"]).max()
+    assert r["step_min"] == o["step_min"]
+    for q in ("cext", "cabs"):
+        ref32, ref64 = float(g[f"solve_{name}_{q}"]), float(g[f"solve_{name}64_{q}"])
+        gate = max(1e-4 * abs(ref64), 2 * abs(ref32 - ref64))
+        assert abs(r[q] - ref64) <= gate, (q, r[q], ref32, ref64)
+    assert rel(r["esc"], o["esc"]) < 2e-3
+
+
+def test_farfield_cabscext_mueller_vs_oracle(D, oracle):
+    rng = np.random.default_rng(3)
+    n, kd = 16, 0.4
+    occ, _ = oracle.gen_ellipsoid(n, n, n, 0.7, 0.5)
+    occ[occ == 1] = rng.integers(1, 3, size=int((occ == 1).sum()))
+    alpha = np.array([0, 0.01 + 0.001j, 0.02 + 0.004j], np.complex64)
+    mv = np.array([0, 1, 1])
+    p = crand(rng, (n, n, n, 3))
+    p[occ == 0] = 0
+    nrm, ksc = oracle.scattering_geometry(3, 19, 0.0, 10.0)
+    kinc = np.array([0.0, 0.6, 0.8])
+    e0 = np.array([1.0, 0, 0], complex)
+    e1 = np.array([0, 0.8, -0.6], complex)
+    with D.Context(n, kd, max_rhs=2) as ctx:
+        esc = ctx.farfield(occ, mv, kd, p, ksc)
+        ca, ce = ctx.cabscext(occ, alpha, kd, kinc, e0, p)
+        escb = ctx.farfield(occ, mv, kd, p * (0.3 - 0.2j), ksc)
+        M = ctx.mueller(kinc, e0, e1, ksc, nrm, esc.reshape(3, 19, 3), escb.reshape(3, 19, 3))
+    ref = np.array([oracle.farfield(occ, mv, kd, p, k) for k in ksc.reshape(-1, 3)])
+    assert rel(esc, ref) < 1e-5
+    oca, oce = oracle.cabscext(occ, alpha, kd, kinc, e0, p)
+    assert abs(ca - oca) < 1e-5 * abs(oca) and abs(ce - oce) < 1e-5 * max(abs(oce), 1e-3)
+    Mo = np.zeros((19, 4, 4))
+    for a in range(19):
+        for pl in range(3):
+            Mo[a] += oracle.jones_mueller(kinc, ksc[pl, a], nrm[pl], e0, e1, esc.reshape(3, 19, 3)[pl, a],
+                                          escb.reshape(3, 19, 3)[pl, a])[1] / 3
+    assert rel(M, Mo) < 1e-5
+
+
+def test_monte_carlo_batch_vs_reference(D, golden, oracle):
+    """4 MC orientations (seed 7) of a 16^3 ellipsoid, batched: vs the FP64 reference."""
+    n, x = 16, 3.0
+    occ, _ = oracle.gen_ellipsoid(n, n, n, 0.7, 0.5)
+    rot = D.mc_rotations(7, 4)
+    cfg = D.BatchConfig(occ=occ, materials=[(1.55, 0.005)], nplanes=2, err_max=1e-3)
+    with D.Context(n, 2 * x / n, max_rhs=8) as ctx:
+        r = ctx.orientation_solves(cfg, rot)
+    ref64, ref32 = golden["mc16_n4_64"], golden["mc16_n4"]
+    for k, q in ((0, "cabs"), (1, "cext")):
+        gate = max(1e-4 * abs(ref64[k]), 2 * abs(ref32[k] - ref64[k]))
+        assert abs(r[q].sum() - ref64[k]) <= gate, (q, r[q].sum(), ref32[k], ref64[k])
+    M = r["mueller"].sum(axis=0).ravel()
+    scale = np.abs(ref64[2:]).max()
+    sig = np.abs(ref64[2:]) > 1e-3 * scale
+    err = np.abs(M - ref64[2:]) / np.abs(ref64[2:])
+    assert err[sig].max() < 1e-3
+
+
+def test_config1_end_to_end(D, golden, oracle):
+    """Config 1 (32^3 sphere, x=2, CM, CG, 19 angles, fixed orientation) against the
+    reference executable's .dat."""
+    txt = bytes(golden["c1_dat"]).decode().strip().split("\n")
+    head = txt[0].replace("\t", " ").split()
+    ca, ce = float(head[0].split("=")[1]), float(head[1].split("=")[1])
+    rows = np.array([[float(v) for v in ln.split()] for ln in txt[1:]])[:, 1:]
+    occ, _ = oracle.gen_ellipsoid(32, 32, 32)
+    cfg = D.BatchConfig(occ=occ, materials=[(1.5, 0.01)])
+    with D.Context(32, 2 * 2.0 / 32, max_rhs=2) as ctx:
+        r = ctx.orientation_solves(cfg, D.fixed_rotation(0, 0, 0)[None])
+    o = orientation_solves(oracle, 32, 2.0, [(1.5, 0.01)], 1)
+    assert abs(r["cabs"][0] - o["cabs"]) < 1e-4 * o["cabs"]
+    assert abs(r["cext"][0] - o["cext"]) < 1e-4 * o["cext"]
+    assert abs(r["cabs"][0] - ca) < 1e-4 * ca
+    assert abs(r["cext"][0] - ce) < 3e-4 * ce
+    M = r["mueller"][0].reshape(-1, 16)
+    scale = np.abs(rows).max()
+    sig = np.abs(rows) > 1e-3 * scale
+    assert (np.abs(M - rows) / np.maximum(np.abs(rows), 1e-30))[sig].max() < 1e-3
+    Mo = o["mueller"].reshape(-1, 16)
+    sig = np.abs(Mo) > 1e-3 * np.abs(Mo).max()
+    assert (np.abs(M - Mo) / np.maximum(np.abs(Mo), 1e-30))[sig].max() < 1e-4
+
+
+def test_ldr_bicgstab_batch(D, golden, oracle):
+    """LDR (per-polarisation alpha) + BiCGStab + 3 planes at 16^3 vs the FP64 reference."""
+    occ, _ = oracle.gen_ellipsoid(16, 16, 16)
+    cfg = D.BatchConfig(occ=occ, materials=[(1.5, 0.01)], polarizability=5, solver=2,
+                        nplanes=3, theta_step=5.0, max_step=100)
+    with D.Context(16, 2 * 4.0 / 16, max_rhs=2) as ctx:
+        r = ctx.orientation_solves(cfg, D.fixed_rotation(0, 0, 0)[None])
+    ref64, ref32 = golden["ldr16_64"], golden["ldr16"]
+    for k, q in ((0, "cabs"), (1, "cext")):
+        gate = max(1e-4 * abs(ref64[k]), 2 * abs(ref32[k] - ref64[k]))
+        assert abs(r[q][0] - ref64[k]) <= gate
+    M = r["mueller"][0].ravel()
+    sig = np.abs(ref64[2:]) > 1e-3 * np.abs(ref64[2:]).max()
+    assert (np.abs(M - ref64[2:]) / np.abs(ref64[2:]))[sig].max() < 1e-3
+
+
+def test_workspace_mismatch_and_bad_material(D):
+    """A lattice that differs from the context is rejected like the reference's workspace
+    check (dda_func.cpp:1091-1094); so is an occupancy index outside the material table."""
+    import ctypes as C
+    L = D.lib()
+    n = 8
+    occ = np.ones((n, n, n), np.int8)
+    alpha = np.array([0, 0, 0.01, 0.0], np.float32)
+    mv = np.array([0, 1], np.int32)
+    k = np.array([0, 0, 1], np.float32)
+    e = np.array([1, 0, 0, 0, 0, 0], np.float32)
+    ksc = np.array([0, 0, 1], np.float32)
+    esc = np.zeros(6, np.float32)
+    ca, ce = C.c_float(), C.c_float()
+    P = lambda a: C.c_void_p(a.ctypes.data)
+    with D.Context(n, 0.5) as ctx:
+        rc = L.ddagpu_dda_fft(ctx.handle, 0, 0, 0.0, 16, n, n, P(alpha), P(mv), 1, P(occ), 2,
+                              1e-3, 0.5, P(k), P(e), 0, 1, 1, P(ksc), P(esc), C.byref(ca),
+                              C.byref(ce), None, None)
+        assert rc == -4
+        bad = occ.copy()
+        bad[0, 0, 0] = 5
+        rc = L.ddagpu_dda_fft(ctx.handle, 0, 0, 0.0, n, n, n, P(alpha), P(mv), 1, P(bad), 2,
+                              1e-3, 0.5, P(k), P(e), 0, 1, 1, P(ksc), P(esc), C.byref(ca),
+                              C.byref(ce), None, None)
+        assert rc == -1
+        rc = L.ddagpu_dda_fft(ctx.handle, 0, 7, 0.0, n, n, n, P(alpha), P(mv), 1, P(occ), 2,
+                              1e-3, 0.5, P(k), P(e), 0, 1, 1, P(ksc), P(esc), C.byref(ca),
+                              C.byref(ce), None, None)
+        assert rc == -1
+        # the context stays usable after rejected calls
+        rc = L.ddagpu_dda_fft(ctx.handle, 0, 0, 0.0, n, n, n, P(alpha), P(mv), 1, P(occ), 2,
+                              1e-3, 0.5, P(k), P(e), 0, 1, 1, P(ksc), P(esc), C.byref(ca),
+                              C.byref(ce), None, None)
+        assert rc == 0 and np.isfinite(ce.value) and ce.value != 0.0
