@@ -173,7 +173,12 @@ def main():
     ap.add_argument("--plain", type=int, default=8, help="orientations timed on the plain path")
     ap.add_argument("--cpu-samples", type=int, default=0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--profile-matvec", type=int, default=0, metavar="NRHS",
+                    help="only run the matvec on NRHS right-hand sides (for ncu captures)")
+    ap.add_argument("--grid", type=int, default=GRID)
     args = ap.parse_args()
+    if args.profile_matvec:
+        return profile_matvec(args)
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
@@ -347,6 +352,22 @@ def main():
     ctx.close()
     if world > 1:
         dist.destroy_process_group()
+
+
+def profile_matvec(args):
+    """Launch the matvec (K1+K2+K3) args.steps times on NRHS device-resident fields."""
+    import torch
+    import dda_fft_b200 as D
+    n, nrhs = args.grid, args.profile_matvec
+    ctx = D.Context(n, 2 * X / n, max_rhs=nrhs)
+    x = torch.randn(nrhs, 3, n, n, n, dtype=torch.complex64, device="cuda")
+    y = torch.empty_like(x)
+    torch.cuda.synchronize()
+    for _ in range(args.warmup + args.steps):
+        ctx.convolution_dev(x, y, nrhs)
+    torch.cuda.synchronize()
+    print(json.dumps({"profile_matvec": nrhs, "grid": n, "launches": ctx.kernel_launches}))
+    ctx.close()
 
 
 def _cm_alpha(d0, m):

@@ -93,6 +93,8 @@ def lib():
         L.ddagpu_set_tiling.argtypes = [_p, _i, _i]
         L.ddagpu_get_tiling.argtypes = [_p, C.POINTER(_i), C.POINTER(_i)]
         L.ddagpu_autotune.argtypes = [_p, _i]
+        L.ddagpu_set_kernels.argtypes = [_p, _i]
+        L.ddagpu_get_kernels.argtypes = [_p]
         _lib = L
         return L
 
@@ -237,18 +239,21 @@ class Context:
         o = np.ascontiguousarray(occ, np.int8)
         a = _cvec(np.asarray(alpha, np.complex64).reshape(-1, 1)).ravel()
         x = _cvec(p)
+        k = _f32(kinc)      # keep every temporary alive across the call
+        e = _cvec(einc)
         ca, ce = C.c_float(), C.c_float()
-        _check(lib().ddagpu_cabscext(self._h, d0, _ptr(_f32(kinc)), _ptr(_cvec(einc)), _ptr(a),
-                                     len(alpha) - 1, _ptr(o), _ptr(x), C.byref(ca), C.byref(ce)))
+        _check(lib().ddagpu_cabscext(self._h, d0, _ptr(k), _ptr(e), _ptr(a), len(alpha) - 1,
+                                     _ptr(o), _ptr(x), C.byref(ca), C.byref(ce)))
         return ca.value, ce.value
 
     def mueller(self, kinc, einc0, einc1, ksc, normals, esc0, esc1) -> np.ndarray:
         ks = _f32(ksc)
         npl, nang = ks.shape[:2]
         out = np.zeros((nang, 4, 4), np.float32)
-        _check(lib().ddagpu_mueller(self._h, _ptr(_f32(kinc)), _ptr(_cvec(einc0)),
-                                    _ptr(_cvec(einc1)), npl, nang, _ptr(ks), _ptr(_f32(normals)),
-                                    _ptr(_cvec(esc0)), _ptr(_cvec(esc1)), _ptr(out)))
+        k, e0, e1, nv = _f32(kinc), _cvec(einc0), _cvec(einc1), _f32(normals)
+        s0, s1 = _cvec(esc0), _cvec(esc1)
+        _check(lib().ddagpu_mueller(self._h, _ptr(k), _ptr(e0), _ptr(e1), npl, nang, _ptr(ks),
+                                    _ptr(nv), _ptr(s0), _ptr(s1), _ptr(out)))
         return out
 
     def orientation_solves(self, cfg: BatchConfig, rot: np.ndarray):
@@ -279,6 +284,13 @@ class Context:
 
     def set_tiling(self, tile_x=0, rows_g=0):
         _check(lib().ddagpu_set_tiling(self._h, tile_x, rows_g))
+
+    def set_kernels(self, fast: bool):
+        _check(lib().ddagpu_set_kernels(self._h, int(fast)))
+
+    @property
+    def fast_kernels(self) -> bool:
+        return lib().ddagpu_get_kernels(self._h) == 1
 
     def tiling(self):
         a, b = C.c_int(), C.c_int()

@@ -65,6 +65,7 @@ struct ddagpu_ctx {
     cudaStream_t st = nullptr;
     Lat L{};
     int tile_x = 32, rows_g = 16;
+    int fast = 0;                // compile-time-sized passes in use
     float2 *ahat = nullptr, *tw = nullptr;
     float2 *work = nullptr, *p = nullptr, *pmin = nullptr, *r = nullptr, *s = nullptr,
            *g = nullptr, *h = nullptr, *w = nullptr;
@@ -167,6 +168,7 @@ MatvecArgs mv_args(ddagpu_ctx *c, int nrhs, const float2 *src, float2 *out, int 
     a.rhs_active = gate ? c->active : nullptr;
     a.tile_x = c->tile_x;
     a.rows_g = c->rows_g;
+    a.fast = c->fast;
     return a;
 }
 
@@ -506,10 +508,12 @@ int ddagpu_create(ddagpu_ctx **out, int device, int i_max, int j_max, int l_max,
     if ((e = cudaMemcpyAsync(c->tw, tw.data(), tw.size() * sizeof(float2), cudaMemcpyHostToDevice,
                              c->st)) != cudaSuccess ||
         (e = matvec_prepare(c->L, c->tile_x, c->rows_g)) != cudaSuccess ||
+        (matvec_fast_supported(c->L) && (e = matvec_fast_prepare(c->L)) != cudaSuccess) ||
         (e = post_prepare(j_max, l_max)) != cudaSuccess ||
         (e = green_build_octant(i_max, j_max, l_max, kd, c->ahat, c->st)) != cudaSuccess ||
         (e = cudaStreamSynchronize(c->st)) != cudaSuccess)
         return bail(fail(DDAGPU_ECUDA, std::string("setup: ") + cudaGetErrorString(e)));
+    c->fast = matvec_fast_supported(c->L) ? 1 : 0;
     *out = c;
     return DDAGPU_OK;
 }
@@ -568,6 +572,17 @@ int ddagpu_set_tiling(ddagpu_ctx *c, int tile_x, int rows_g)
     return DDAGPU_OK;
 }
 
+int ddagpu_set_kernels(ddagpu_ctx *c, int fast)
+{
+    if (!c) return fail(DDAGPU_EINVAL, "null context");
+    if (fast && !matvec_fast_supported(c->L))
+        return fail(DDAGPU_EINVAL, "compile-time-sized passes need edges in {16, 32, 64}");
+    c->fast = fast ? 1 : 0;
+    return DDAGPU_OK;
+}
+
+int ddagpu_get_kernels(ddagpu_ctx *c) { return c ? c->fast : -1; }
+
 int ddagpu_get_tiling(ddagpu_ctx *c, int *tile_x, int *rows_g)
 {
     if (!c) return fail(DDAGPU_EINVAL, "null context");
@@ -603,28 +618,47 @@ int ddagpu_autotune(ddagpu_ctx *c, int nrhs)
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
+    auto time_it = [&](float *ms) -> int {
+        MatvecArgs a = mv_args(c, nrhs, c->p, c->r, 0, 0.f, nullptr, 0, 1, false);
+        for (int k = 0; k < 2; k++) CK(launch_matvec(a, c->st));
+        CK(cudaEventRecord(e0, c->st));
+        for (int k = 0; k < 5; k++) CK(launch_matvec(a, c->st));
+        CK(cudaEventRecord(e1, c->st));
+        CK(cudaEventSynchronize(e1));
+        CK(cudaEventElapsedTime(ms, e0, e1));
+        return DDAGPU_OK;
+    };
     float best = 1e30f;
-    int btx = c->tile_x, brg = c->rows_g;
+    int btx = c->tile_x, brg = c->rows_g, bfast = 0;
+    const int had_fast = c->fast;
+    c->fast = 0;
     for (int tx : txs)
         for (int rg : rgs) {
             RET(ddagpu_set_tiling(c, tx, rg));
-            MatvecArgs a = mv_args(c, nrhs, c->p, c->r, 0, 0.f, nullptr, 0, 1, false);
-            for (int k = 0; k < 2; k++) CK(launch_matvec(a, c->st));
-            CK(cudaEventRecord(e0, c->st));
-            for (int k = 0; k < 5; k++) CK(launch_matvec(a, c->st));
-            CK(cudaEventRecord(e1, c->st));
-            CK(cudaEventSynchronize(e1));
             float ms = 0;
-            CK(cudaEventElapsedTime(&ms, e0, e1));
+            RET(time_it(&ms));
             if (ms < best) {
                 best = ms;
                 btx = tx;
                 brg = rg;
             }
         }
+    if (matvec_fast_supported(c->L)) {
+        c->fast = 1;
+        float ms = 0;
+        RET(time_it(&ms));
+        if (ms < best) {
+            best = ms;
+            bfast = 1;
+        }
+    }
+    (void)had_fast;
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    return ddagpu_set_tiling(c, btx, brg);
+    c->fast = 0;
+    RET(ddagpu_set_tiling(c, btx, brg));
+    c->fast = bfast;
+    return DDAGPU_OK;
 }
 
 int ddagpu_convolution(ddagpu_ctx *c, const float *p, float *out, int conj)

@@ -64,8 +64,9 @@ struct MatvecArgs {
     float2 *out;            // [nrhs][3][N]
     Epilogue ep;
     const int *rhs_active;  // [nrhs] or null
-    int tile_x;             // columns per CTA of the x pass (autotuned)
-    int rows_g;             // rows per staging group of the y/z passes
+    int tile_x;             // columns per CTA of the x pass (generic kernels)
+    int rows_g;             // rows per staging group of the y/z passes (generic kernels)
+    int fast;               // 1: compile-time-sized kernels of matvec_fast.cu
 };
 
 // kernels (matvec.cu)
@@ -73,6 +74,11 @@ cudaError_t launch_matvec(const MatvecArgs &a, cudaStream_t st);
 size_t matvec_smem_yz(const Lat &L, int rows_g);
 size_t matvec_smem_x(const Lat &L, int tile_x);
 cudaError_t matvec_prepare(const Lat &L, int tile_x, int rows_g);
+
+// compile-time-sized passes for edges in {16, 32, 64} (matvec_fast.cu)
+bool matvec_fast_supported(const Lat &L);
+cudaError_t matvec_fast_prepare(const Lat &L);
+cudaError_t launch_matvec_fast(const MatvecArgs &a, cudaStream_t st);
 
 // Green tensor (green.cu)
 cudaError_t green_build_octant(int ni, int nj, int nl, double kd, float2 *ahat, cudaStream_t st);

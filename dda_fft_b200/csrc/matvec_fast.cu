@@ -1,0 +1,552 @@
+// Fast matvec passes for lattice edges in {16, 32, 64}: the same three passes and the same
+// split-order spectral layout as matvec.cu, with every size a compile-time constant.
+//
+// Every n-point FFT uses the factorisation n = R1 R2 (fft_split): a thread holds R1
+// elements of a line for step A and R2 elements for step B, and the steps exchange data
+// through shared memory.  Two thread roles occur:
+//   row role    -- the RM = max(R1,R2) lanes of one warp-aligned group own one line whose
+//                  elements are contiguous in shared memory (z lines); the exchange is
+//                  warp-local (__syncwarp);
+//   column role -- thread (sub, col) with consecutive lanes on consecutive lines; the
+//                  exchange needs the block (__syncthreads) but every access is a
+//                  contiguous run of the warp.
+// Shared planes use the swizzled row layout pos(p) = p + p/8 with a row stride PS = RM
+// (mod 16) float2, which keeps both roles free of bank conflicts.
+#include <cooperative_groups.h>
+
+#include "common.cuh"
+#include "internal.h"
+
+namespace cg = cooperative_groups;
+
+namespace ddagpu {
+
+namespace {
+
+template <int N>
+struct Sp {
+    static constexpr int R1 = fft_split<N>::R1, R2 = fft_split<N>::R2;
+    static constexpr int RM = R1 > R2 ? R1 : R2;
+    // swizzled row stride: N + N/8 rounded up to RM (mod 16)
+    static constexpr int base = N + N / 8;
+    static constexpr int PS = base + ((RM % 16) - (base % 16) + 16) % 16;
+};
+
+DDA_DEV int spos(int p) { return p + (p >> 3); }
+
+DDA_DEV int zmapf(int oz, int nl) { return (oz & 1) ? (nl / 2 + 1 + (oz >> 1)) : (oz >> 1); }
+
+template <bool INV>
+DDA_DEV float2 twid(const float2 *__restrict__ tw, int k)
+{
+    float2 w = __ldg(&tw[k]);
+    if (INV) w.y = -w.y;
+    return w;
+}
+
+// Row role, one line of N elements at `row` (swizzled), in place, natural order out.
+// lane_sub in [0, RM).  v: the R1 step-A inputs of this lane (positions t2 + R2 r), loaded
+// by the caller for lane_sub < R2.  Every lane of the warp calls this (it synchronises the
+// warp); `valid` guards the shared-memory accesses of lanes without a line.
+template <int N, bool INV>
+DDA_DEV void row_fft_from_regs(float2 *row, int lane_sub, bool valid, float2 (&v)[Sp<N>::R1],
+                               const float2 *__restrict__ tw)
+{
+    constexpr int R1 = Sp<N>::R1, R2 = Sp<N>::R2;
+    static_assert(R2 > 1, "single-step sizes are not on the fast path");
+    if (valid && lane_sub < R2) {
+        const int t2 = lane_sub;
+        dft_reg<R1, INV>(v);
+#pragma unroll
+        for (int k1 = 1; k1 < R1; k1++) v[k1] = cmul(v[k1], twid<INV>(tw, t2 * k1));
+#pragma unroll
+        for (int k1 = 0; k1 < R1; k1++) row[spos(t2 + R2 * k1)] = v[k1];
+    }
+    __syncwarp();
+    float2 u[R2];
+    if (valid && lane_sub < R1) {
+        const int k1 = lane_sub;
+#pragma unroll
+        for (int t = 0; t < R2; t++) u[t] = row[spos(R2 * k1 + t)];
+        dft_reg<R2, INV>(u);
+    }
+    __syncwarp();
+    if (valid && lane_sub < R1) {
+        const int k1 = lane_sub;
+#pragma unroll
+        for (int k2 = 0; k2 < R2; k2++) row[spos(k1 + R1 * k2)] = u[k2];
+    }
+    __syncwarp();
+}
+
+// ------------------------------------------------------------------------------ K1
+// CTA (i, component, z half hl): z-forward of the NJ rows of plane i (half hl only), then
+// y-forward of the NL columns for both y halves; writes work rows in split order.
+template <int NJ, int NL, int NT>
+__global__ void __launch_bounds__(NT) k1f(MatvecArgs a)
+{
+    using SJ = Sp<NJ>;
+    using SL = Sp<NL>;
+    constexpr int PS = SL::PS;
+    __shared__ float2 Z[NJ * PS];
+    const int hl = blockIdx.x & 1, i = blockIdx.x >> 1, c = blockIdx.y, rhs = blockIdx.z;
+    if (a.rhs_active && !a.rhs_active[rhs]) return;
+    const int ni = a.L.ni;
+    const float2 *src = a.src + (size_t)rhs * a.fstride + ((size_t)c * ni + i) * (NJ * NL);
+    const float2 *twl = a.L.tw_l, *hwl = a.L.tw_l + NL, *twj = a.L.tw_j, *hwj = a.L.tw_j + NJ;
+
+    // ---- z: rows, row role
+    {
+        constexpr int RM = SL::RM, RPP = NT / RM;   // rows per pass
+        const int sub = threadIdx.x % RM, rr = threadIdx.x / RM;
+#pragma unroll 1
+        for (int r0 = 0; r0 < NJ; r0 += RPP) {
+            const int row = r0 + rr;
+            float2 v[SL::R1];
+            if (row < NJ && sub < SL::R2) {
+#pragma unroll
+                for (int r = 0; r < SL::R1; r++) {
+                    const int l = sub + SL::R2 * r;
+                    float2 x = src[row * NL + l];
+                    if (hl) x = cmul(x, __ldg(&hwl[l]));
+                    v[r] = x;
+                }
+            }
+            row_fft_from_regs<NL, false>(Z + (row < NJ ? row : 0) * PS, sub, row < NJ, v, twl);
+        }
+    }
+    __syncthreads();
+
+    // ---- y: columns, column role, both halves from the same registers
+    {
+        constexpr int R1 = SJ::R1, R2 = SJ::R2, RM = SJ::RM;
+        constexpr int CPP = NT / RM;   // columns per pass
+        static_assert(CPP >= 1, "block too small");
+        const int col0 = threadIdx.x % CPP, sub = threadIdx.x / CPP;
+        float2 *dst = a.work + (size_t)rhs * a.wstride + ((size_t)c * ni + i) * (2 * NJ) * (2 * NL);
+#pragma unroll 1
+        for (int cbase = 0; cbase < NL; cbase += CPP) {
+            const int col = cbase + col0;
+            const bool ok = col < NL;
+            float2 orig[R1];
+            if (ok && sub < R2) {
+#pragma unroll
+                for (int r = 0; r < R1; r++) orig[r] = Z[(sub + R2 * r) * PS + spos(col)];
+            }
+            __syncthreads();
+#pragma unroll 1
+            for (int hy = 0; hy < 2; hy++) {
+                if (ok && sub < R2) {
+                    float2 v[R1];
+#pragma unroll
+                    for (int r = 0; r < R1; r++)
+                        v[r] = hy ? cmul(orig[r], __ldg(&hwj[sub + R2 * r])) : orig[r];
+                    dft_reg<R1, false>(v);
+#pragma unroll
+                    for (int k1 = 1; k1 < R1; k1++) v[k1] = cmul(v[k1], twid<false>(twj, sub * k1));
+#pragma unroll
+                    for (int k1 = 0; k1 < R1; k1++) Z[(sub + R2 * k1) * PS + spos(col)] = v[k1];
+                }
+                __syncthreads();
+                if (ok && sub < R1) {
+                    float2 u[R2];
+#pragma unroll
+                    for (int t = 0; t < R2; t++) u[t] = Z[(R2 * sub + t) * PS + spos(col)];
+                    dft_reg<R2, false>(u);
+                    float2 *d = dst + (size_t)(hy * NJ) * (2 * NL) + hl * NL + col;
+#pragma unroll
+                    for (int k2 = 0; k2 < R2; k2++) d[(size_t)(sub + R1 * k2) * (2 * NL)] = u[k2];
+                }
+                __syncthreads();
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------ K2
+// CTA (spectral row js, TL spectral columns): forward x (both halves), 3x3 product,
+// inverse x, in place.  Shared B[c][h][pos][t].
+template <int NI, int TL>
+__global__ void __launch_bounds__(Sp<NI>::RM * TL) k2f(MatvecArgs a)
+{
+    using S = Sp<NI>;
+    constexpr int R1 = S::R1, R2 = S::R2, RM = S::RM;
+    extern __shared__ float2 B[];   // [6][NI][TL]
+    const int js = blockIdx.x, rhs = blockIdx.z;
+    if (a.rhs_active && !a.rhs_active[rhs]) return;
+    const int nj = a.L.nj, nl = a.L.nl;
+    const int l0 = blockIdx.y * TL;
+    const int t = threadIdx.x % TL, sub = threadIdx.x / TL;
+    const size_t plane = (size_t)(2 * nj) * (2 * nl), cstr = (size_t)NI * plane;
+    float2 *base = a.work + (size_t)rhs * a.wstride + (size_t)js * (2 * nl) + l0 + t;
+    const float2 *tw = a.L.tw_i, *hw = a.L.tw_i + NI;
+    auto Bat = [&](int c, int h, int pos) -> float2 & { return B[((c * 2 + h) * NI + pos) * TL + t]; };
+
+    // ---- forward step A (both halves from one load)
+    if (R2 == 1) {
+        if (sub == 0) {
+#pragma unroll 1
+            for (int c = 0; c < 3; c++) {
+                float2 v[R1], w[R1];
+#pragma unroll
+                for (int r = 0; r < R1; r++) {
+                    v[r] = base[c * cstr + r * plane];
+                    w[r] = cmul(v[r], __ldg(&hw[r]));
+                }
+                dft_reg<R1, false>(v);
+                dft_reg<R1, false>(w);
+#pragma unroll
+                for (int k = 0; k < R1; k++) {
+                    Bat(c, 0, k) = v[k];
+                    Bat(c, 1, k) = w[k];
+                }
+            }
+        }
+    } else if (sub < R2) {
+#pragma unroll 1
+        for (int c = 0; c < 3; c++) {
+            float2 v[R1], w[R1];
+#pragma unroll
+            for (int r = 0; r < R1; r++) {
+                const int i = sub + R2 * r;
+                v[r] = base[c * cstr + i * plane];
+                w[r] = cmul(v[r], __ldg(&hw[i]));
+            }
+            dft_reg<R1, false>(v);
+            dft_reg<R1, false>(w);
+#pragma unroll
+            for (int k1 = 0; k1 < R1; k1++) {
+                const float2 tk = k1 ? twid<false>(tw, sub * k1) : make_float2(1.f, 0.f);
+                Bat(c, 0, sub + R2 * k1) = k1 ? cmul(v[k1], tk) : v[k1];
+                Bat(c, 1, sub + R2 * k1) = k1 ? cmul(w[k1], tk) : w[k1];
+            }
+        }
+    }
+    __syncthreads();
+
+    // ---- forward step B, product with the Green tensor, inverse step A
+    const int hj = js >= nj, kj = js - hj * nj, jp = 2 * kj + hj;
+    const int my = jp > nj, oy = my ? 2 * nj - jp : jp;
+    const int ls = l0 + t, hl = ls >= nl, kl = ls - hl * nl, lp = 2 * kl + hl;
+    const int mz = lp > nl, oz = mz ? 2 * nl - lp : lp;
+    const size_t sz = (size_t)(nl + 1), sy = (size_t)(nj + 1) * sz, sx = (size_t)(NI + 1) * sy;
+    const float2 *Ayz = a.ahat + (size_t)oy * sz + zmapf(oz, nl);
+#pragma unroll 1
+    for (int h = 0; h < 2; h++) {
+        float2 X[3][R2];
+        const bool act = (R2 == 1) ? (sub == 0) : (sub < R1);
+        const int k1 = sub;
+        if (act) {
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                if (R2 == 1) {
+                    X[c][0] = czero();
+                } else {
+#pragma unroll
+                    for (int q = 0; q < R2; q++) X[c][q] = Bat(c, h, R2 * k1 + q);
+                    dft_reg<R2, false>(X[c]);
+                }
+            }
+        }
+        __syncthreads();
+        if (act) {
+            if (R2 == 1) {
+                // single-step sizes: the whole line is in shared memory; this lane does all
+#pragma unroll 1
+                for (int k = 0; k < R1; k++) {
+                    const int kx = 2 * k + h, mx = kx > NI, ox = mx ? 2 * NI - kx : kx;
+                    const float2 *A = Ayz + (size_t)ox * sy;
+                    float2 g0 = __ldg(A), g1 = __ldg(A + sx), g2 = __ldg(A + 2 * sx),
+                           g3 = __ldg(A + 3 * sx), g4 = __ldg(A + 4 * sx), g5 = __ldg(A + 5 * sx);
+                    if (mx ^ my) g1 = cscale(g1, -1.f);
+                    if (mx ^ mz) g2 = cscale(g2, -1.f);
+                    if (my ^ mz) g4 = cscale(g4, -1.f);
+                    if (a.conj) {
+                        g0 = cconj(g0); g1 = cconj(g1); g2 = cconj(g2);
+                        g3 = cconj(g3); g4 = cconj(g4); g5 = cconj(g5);
+                    }
+                    const float2 vx = Bat(0, h, k), vy = Bat(1, h, k), vz = Bat(2, h, k);
+                    Bat(0, h, k) = cadd(cadd(cmul(g0, vx), cmul(g1, vy)), cmul(g2, vz));
+                    Bat(1, h, k) = cadd(cadd(cmul(g1, vx), cmul(g3, vy)), cmul(g4, vz));
+                    Bat(2, h, k) = cadd(cadd(cmul(g2, vx), cmul(g4, vy)), cmul(g5, vz));
+                }
+            } else {
+#pragma unroll
+                for (int q = 0; q < R2; q++) {
+                    const int kx = 2 * (k1 + R1 * q) + h, mx = kx > NI, ox = mx ? 2 * NI - kx : kx;
+                    const float2 *A = Ayz + (size_t)ox * sy;
+                    float2 g0 = __ldg(A), g1 = __ldg(A + sx), g2 = __ldg(A + 2 * sx),
+                           g3 = __ldg(A + 3 * sx), g4 = __ldg(A + 4 * sx), g5 = __ldg(A + 5 * sx);
+                    if (mx ^ my) g1 = cscale(g1, -1.f);
+                    if (mx ^ mz) g2 = cscale(g2, -1.f);
+                    if (my ^ mz) g4 = cscale(g4, -1.f);
+                    if (a.conj) {
+                        g0 = cconj(g0); g1 = cconj(g1); g2 = cconj(g2);
+                        g3 = cconj(g3); g4 = cconj(g4); g5 = cconj(g5);
+                    }
+                    const float2 vx = X[0][q], vy = X[1][q], vz = X[2][q];
+                    X[0][q] = cadd(cadd(cmul(g0, vx), cmul(g1, vy)), cmul(g2, vz));
+                    X[1][q] = cadd(cadd(cmul(g1, vx), cmul(g3, vy)), cmul(g4, vz));
+                    X[2][q] = cadd(cadd(cmul(g2, vx), cmul(g4, vy)), cmul(g5, vz));
+                }
+                // inverse step A with the transposed split: lane k1 owns positions k1 + R1 q
+#pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    dft_reg<R2, true>(X[c]);
+#pragma unroll
+                    for (int u = 0; u < R2; u++) {
+                        const float2 y = u ? cmul(X[c][u], twid<true>(tw, k1 * u)) : X[c][u];
+                        Bat(c, h, k1 + R1 * u) = y;
+                    }
+                }
+            }
+        }
+        __syncthreads();
+    }
+
+    // ---- inverse step B (transposed split: R2 lanes of R1 elements), combine, store
+    if (R2 == 1) {
+        if (sub == 0) {
+#pragma unroll 1
+            for (int c = 0; c < 3; c++) {
+                float2 e[R1], o[R1];
+#pragma unroll
+                for (int k = 0; k < R1; k++) {
+                    e[k] = Bat(c, 0, k);
+                    o[k] = Bat(c, 1, k);
+                }
+                dft_reg<R1, true>(e);
+                dft_reg<R1, true>(o);
+#pragma unroll
+                for (int k = 0; k < R1; k++)
+                    base[c * cstr + k * plane] = cadd(e[k], cmulc(o[k], __ldg(&hw[k])));
+            }
+        }
+    } else if (sub < R2) {
+        const int k1p = sub;
+#pragma unroll 1
+        for (int c = 0; c < 3; c++) {
+            float2 e[R1], o[R1];
+#pragma unroll
+            for (int q = 0; q < R1; q++) {
+                e[q] = Bat(c, 0, R1 * k1p + q);
+                o[q] = Bat(c, 1, R1 * k1p + q);
+            }
+            dft_reg<R1, true>(e);
+            dft_reg<R1, true>(o);
+#pragma unroll
+            for (int k2 = 0; k2 < R1; k2++) {
+                const int i = k1p + R2 * k2;
+                base[c * cstr + i * plane] = cadd(e[k2], cmulc(o[k2], __ldg(&hw[i])));
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------ K3
+// Cluster pair (rank = z half hl) per (i, component): y-inverse of this half's NL
+// columns (both y halves), z-inverse of the NJ rows restricted to this half, then the two
+// halves are summed through distributed shared memory and the epilogue writes the rows of
+// this rank.
+template <int NJ, int NL, int NT>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(NT) k3f(MatvecArgs a)
+{
+    using SJ = Sp<NJ>;
+    using SL = Sp<NL>;
+    constexpr int PS = SL::PS;
+    __shared__ float2 Q[NJ * PS];
+    cg::cluster_group cl = cg::this_cluster();
+    const int hl = (int)cl.block_rank();
+    const int i = blockIdx.x >> 1, c = blockIdx.y, rhs = blockIdx.z;
+    if (a.rhs_active && !a.rhs_active[rhs]) return;   // uniform over the cluster
+    const int ni = a.L.ni;
+    const float2 *src = a.work + (size_t)rhs * a.wstride + ((size_t)c * ni + i) * (2 * NJ) * (2 * NL) + hl * NL;
+    const float2 *twl = a.L.tw_l, *hwl = a.L.tw_l + NL, *twj = a.L.tw_j, *hwj = a.L.tw_j + NJ;
+
+    // ---- y inverse on this half's columns: x[j] = IDFT(even)[j] + W^-j IDFT(odd)[j]
+    {
+        constexpr int R1 = SJ::R1, R2 = SJ::R2, RM = SJ::RM;
+        constexpr int CPP = NT / RM;
+        const int col0 = threadIdx.x % CPP, sub = threadIdx.x / CPP;
+#pragma unroll 1
+        for (int cbase = 0; cbase < NL; cbase += CPP) {
+            const int col = cbase + col0;
+            const bool ok = col < NL;
+            float2 y0[R2];
+#pragma unroll 1
+            for (int hy = 0; hy < 2; hy++) {
+                if (ok && sub < R2) {
+                    float2 v[R1];
+#pragma unroll
+                    for (int r = 0; r < R1; r++)
+                        v[r] = src[(size_t)(hy * NJ + sub + R2 * r) * (2 * NL) + col];
+                    dft_reg<R1, true>(v);
+#pragma unroll
+                    for (int k1 = 1; k1 < R1; k1++) v[k1] = cmul(v[k1], twid<true>(twj, sub * k1));
+#pragma unroll
+                    for (int k1 = 0; k1 < R1; k1++) Q[(sub + R2 * k1) * PS + spos(col)] = v[k1];
+                }
+                __syncthreads();
+                float2 u[R2];
+                if (ok && sub < R1) {
+#pragma unroll
+                    for (int t = 0; t < R2; t++) u[t] = Q[(R2 * sub + t) * PS + spos(col)];
+                    dft_reg<R2, true>(u);
+                    if (hy == 0) {
+#pragma unroll
+                        for (int k2 = 0; k2 < R2; k2++) y0[k2] = u[k2];
+                    } else {
+#pragma unroll
+                        for (int k2 = 0; k2 < R2; k2++) {
+                            const int j = sub + R1 * k2;
+                            y0[k2] = cadd(y0[k2], cmulc(u[k2], __ldg(&hwj[j])));
+                        }
+                    }
+                }
+                __syncthreads();
+            }
+            if (ok && sub < R1) {
+#pragma unroll
+                for (int k2 = 0; k2 < R2; k2++) Q[(sub + R1 * k2) * PS + spos(col)] = y0[k2];
+            }
+        }
+    }
+    __syncthreads();
+
+    // ---- z inverse of the rows (this half's spectral columns), row role
+    {
+        constexpr int RM = SL::RM, RPP = NT / RM;
+        const int sub = threadIdx.x % RM, rr = threadIdx.x / RM;
+#pragma unroll 1
+        for (int r0 = 0; r0 < NJ; r0 += RPP) {
+            const int row = r0 + rr;
+            float2 v[SL::R1];
+            if (row < NJ && sub < SL::R2) {
+#pragma unroll
+                for (int r = 0; r < SL::R1; r++) v[r] = Q[row * PS + spos(sub + SL::R2 * r)];
+            }
+            __syncwarp();
+            row_fft_from_regs<NL, true>(Q + (row < NJ ? row : 0) * PS, sub, row < NJ, v, twl);
+            if (hl == 1 && row < NJ) {
+                // odd half: times W_2NL^-l
+                for (int l = sub; l < NL; l += RM) Q[row * PS + spos(l)] = cmulc(Q[row * PS + spos(l)], __ldg(&hwl[l]));
+            }
+        }
+    }
+    cl.sync();
+
+    // ---- sum of the two halves, epilogue, rows of this rank
+    const float2 *R = cl.map_shared_rank(Q, hl ^ 1);
+    constexpr int HR = NJ / 2;
+    const size_t N = a.L.N;
+    const size_t obase = (size_t)rhs * a.fstride + (size_t)c * N + (size_t)i * NJ * NL;
+    const Epilogue &ep = a.ep;
+    for (int e = threadIdx.x; e < HR * NL; e += NT) {
+        const int jj = e / NL, l = e % NL, j = hl * HR + jj;
+        const int q = j * PS + spos(l);
+        const float2 conv = cadd(Q[q], R[q]);
+        const size_t o = obase + (size_t)j * NL + l;
+        float2 res = conv;
+        if (ep.mode == 1) {
+            const int m = ep.occ[(size_t)i * NJ * NL + (size_t)j * NL + l];
+            if (!ep.mv[m]) {
+                res = czero();
+            } else {
+                float2 al = ep.alpha[(size_t)rhs * ep.nmat1 + m];
+                if (ep.conj) al = cconj(al);
+                res = csub(ep.sv != 0.f ? cscale(ep.v[o], ep.sv) : czero(), cmul(al, conv));
+            }
+        }
+        a.out[o] = res;
+    }
+    cl.sync();
+}
+
+template <int NJ, int NL>
+constexpr int yz_threads()
+{
+    // enough threads for the column role on all NL columns and the row role on all rows
+    return (Sp<NJ>::RM * NL) > 256 ? 512 : 256;
+}
+
+template <int NJ, int NL>
+void launch_yz(const MatvecArgs &a, int fwd, cudaStream_t st)
+{
+    constexpr int NT = yz_threads<NJ, NL>();
+    if (fwd) k1f<NJ, NL, NT><<<dim3(2 * a.L.ni, 3, a.nrhs), NT, 0, st>>>(a);
+    else k3f<NJ, NL, NT><<<dim3(2 * a.L.ni, 3, a.nrhs), NT, 0, st>>>(a);
+}
+
+template <int NI>
+constexpr int x_tile()
+{
+    return NI <= 32 ? 32 : (NI == 64 ? 32 : 16);
+}
+
+template <int NI>
+void launch_x(const MatvecArgs &a, cudaStream_t st)
+{
+    constexpr int TL = x_tile<NI>();
+    const int ncol = 2 * a.L.nl;
+    const size_t smem = (size_t)6 * NI * TL * sizeof(float2);
+    k2f<NI, TL><<<dim3(2 * a.L.nj, ncol / TL, a.nrhs), Sp<NI>::RM * TL, smem, st>>>(a);
+}
+
+template <int NI>
+cudaError_t prep_x()
+{
+    constexpr int TL = x_tile<NI>();
+    return cudaFuncSetAttribute(k2f<NI, TL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)(6 * NI * TL * sizeof(float2)));
+}
+
+bool fast_edge(int n) { return n == 16 || n == 32 || n == 64; }
+
+}  // namespace
+
+bool matvec_fast_supported(const Lat &L)
+{
+    return fast_edge(L.ni) && fast_edge(L.nj) && fast_edge(L.nl) && 2 * L.nl >= 32;
+}
+
+cudaError_t matvec_fast_prepare(const Lat &L)
+{
+    switch (L.ni) {
+    case 16: return prep_x<16>();
+    case 32: return prep_x<32>();
+    case 64: return prep_x<64>();
+    }
+    return cudaErrorInvalidValue;
+}
+
+#define DISPATCH_YZ(NJv)                                                                     \
+    case NJv:                                                                                \
+        switch (a.L.nl) {                                                                    \
+        case 16: launch_yz<NJv, 16>(a, fwd, st); break;                                      \
+        case 32: launch_yz<NJv, 32>(a, fwd, st); break;                                      \
+        case 64: launch_yz<NJv, 64>(a, fwd, st); break;                                      \
+        }                                                                                    \
+        break;
+
+static void yz(const MatvecArgs &a, int fwd, cudaStream_t st)
+{
+    switch (a.L.nj) {
+        DISPATCH_YZ(16)
+        DISPATCH_YZ(32)
+        DISPATCH_YZ(64)
+    }
+}
+
+cudaError_t launch_matvec_fast(const MatvecArgs &a, cudaStream_t st)
+{
+    yz(a, 1, st);
+    switch (a.L.ni) {
+    case 16: launch_x<16>(a, st); break;
+    case 32: launch_x<32>(a, st); break;
+    case 64: launch_x<64>(a, st); break;
+    }
+    yz(a, 0, st);
+    return cudaGetLastError();
+}
+
+}  // namespace ddagpu

@@ -153,10 +153,15 @@ void *ddagpu_stream(ddagpu_ctx *ctx);
 /* Number of CUDA kernels this context has launched so far. */
 long long ddagpu_kernel_launches(ddagpu_ctx *ctx);
 /* Kernel launch parameters: columns per CTA of the x pass and rows per staging group of
- * the y/z passes; 0 keeps the current value.  ddagpu_autotune times the candidates on the
- * context's lattice and keeps the fastest. */
+ * the y/z passes of the generic kernels; 0 keeps the current value.  ddagpu_autotune
+ * times the generic tilings and the specialised passes on the context's lattice and keeps
+ * the fastest. */
 int ddagpu_set_tiling(ddagpu_ctx *ctx, int tile_x, int rows_g);
 int ddagpu_get_tiling(ddagpu_ctx *ctx, int *tile_x, int *rows_g);
+/* Kernel family of the matvec: 1 = passes specialised at compile time for lattice edges in
+ * {16, 32, 64} (the default where they apply), 0 = the generic passes (any edge 2..128). */
+int ddagpu_set_kernels(ddagpu_ctx *ctx, int fast);
+int ddagpu_get_kernels(ddagpu_ctx *ctx);
 int ddagpu_autotune(ddagpu_ctx *ctx, int nrhs);
 
 #ifdef __cplusplus

@@ -28,14 +28,22 @@ def D():
     return dda_fft_b200
 
 
+FAST = {16, 32, 64}
+
+
 @pytest.mark.parametrize("grid", [(2, 2, 2), (4, 4, 4), (8, 8, 8), (16, 16, 16), (32, 32, 32),
-                                  (8, 16, 8), (16, 4, 32), (64, 64, 64)])
+                                  (8, 16, 8), (16, 4, 32), (64, 64, 64), (16, 64, 32),
+                                  (64, 16, 16), (32, 16, 64)])
 @pytest.mark.parametrize("conj", [False, True])
-def test_convolution_vs_oracle(D, oracle, grid, conj):
+@pytest.mark.parametrize("fast", [False, True])
+def test_convolution_vs_oracle(D, oracle, grid, conj, fast):
+    if fast and not set(grid) <= FAST:
+        pytest.skip("specialised passes cover edges 16..64")
     rng = np.random.default_rng(sum(grid) + conj)
     kd = 2 * 3.0 / grid[0]
     p = crand(rng, grid + (3,))
     with D.Context(grid, kd) as ctx:
+        ctx.set_kernels(fast)
         out = ctx.convolution(p, conj=conj)
     ref = oracle.convolution(oracle.green_hat(*grid, kd), p.astype(np.complex128), conj=conj)
     assert rel(out, ref) < CONV_TOL
