@@ -94,6 +94,7 @@ def lib():
         L.ddagpu_get_tiling.argtypes = [_p, C.POINTER(_i), C.POINTER(_i)]
         L.ddagpu_autotune.argtypes = [_p, _i]
         L.ddagpu_set_kernels.argtypes = [_p, _i]
+        L.ddagpu_farfield_noalloc.argtypes = [_i, _i, _i, _i, _f, _p, _p, _p, _i, _p, _p, _p]
         L.ddagpu_get_kernels.argtypes = [_p]
         _lib = L
         return L

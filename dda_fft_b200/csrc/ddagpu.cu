@@ -895,6 +895,36 @@ int ddagpu_mueller(ddagpu_ctx *c, const float *kinc, const float *einc0, const f
     return DDAGPU_OK;
 }
 
+int ddagpu_farfield_noalloc(int device, int i_max, int j_max, int l_max, float d0,
+                            const signed char *occ_dev, const int *mv_dev, const void *p_dev,
+                            int ndir, const float *ksc_dev, float *esc_dev, void *stream)
+{
+    if (!pow2_in(i_max) || !pow2_in(j_max) || !pow2_in(l_max))
+        return fail(DDAGPU_EINVAL, "lattice edges must be powers of two in [2, 128]");
+    if (ndir < 0 || ndir > farfield_noalloc_max_dirs())
+        return fail(DDAGPU_EINVAL, "ndir exceeds the allocation-free maximum of " +
+                                       std::to_string(farfield_noalloc_max_dirs()) + " directions");
+    if (ndir == 0) return DDAGPU_OK;
+    if (!occ_dev || !mv_dev || !p_dev || !ksc_dev || !esc_dev)
+        return fail(DDAGPU_EINVAL, "null device pointer");
+    DevGuard dg(device);
+    double *scratch = nullptr;
+    CK(farfield_noalloc_scratch(device, &scratch));
+    PostArgs a{};
+    a.N = (size_t)i_max * j_max * l_max;
+    a.nrhs = 1;
+    a.ni = i_max;
+    a.nj = j_max;
+    a.nl = l_max;
+    a.occ = occ_dev;
+    a.mv = mv_dev;
+    a.p = (const float2 *)p_dev;
+    a.d0 = d0;
+    a.ndir = ndir;
+    CK(farfield_noalloc(a, ksc_dev, (float2 *)esc_dev, scratch, (cudaStream_t)stream));
+    return DDAGPU_OK;
+}
+
 int ddagpu_mc_rotations(unsigned long long base_seed, int worker, int count, double *rot)
 {
     if (!rot || count < 0 || worker < 0) return fail(DDAGPU_EINVAL, "bad argument");

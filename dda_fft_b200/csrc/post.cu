@@ -8,6 +8,8 @@
 // projection S - k (k.S), equal by linearity to the reference's per-dipole projection.
 // The phase is separable, exp(i kx x) exp(i ky y) exp(i kz z), so each CTA builds small
 // tables and the inner loop is three complex multiply-adds per dipole and direction.
+#include <mutex>
+
 #include "common.cuh"
 #include "internal.h"
 #include "post.h"
@@ -286,6 +288,68 @@ cudaError_t launch_mueller(const MuellerArgs &m, cudaStream_t st)
     const size_t n = (size_t)m.norient * m.nangles;
     if (n == 0) return cudaSuccess;
     mueller_avg<<<nblk(n, 128), 128, 0, st>>>(m);
+    return cudaGetLastError();
+}
+
+}  // namespace ddagpu
+
+// ---------------------------------------------------------------------------------------
+// Far field with no allocation, for callers that must not allocate device memory: code
+// running inside a CUDA graph capture, a real-time loop that forbids allocator calls, or
+// a host that hands this library only pre-allocated buffers.  The FP64 accumulators and
+// the double copy of the directions live in this file-scope device array instead of in a
+// context; every call on a device shares it.
+namespace ddagpu {
+
+namespace {
+
+constexpr int kNoAllocMaxDirs = 8192;   // 8192 x 9 doubles = 576 KiB per device
+__device__ __align__(256) double g_farfield_scratch[kNoAllocMaxDirs * 9];
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+double *g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+__global__ void ksc_to_double(const float *ksc, double *out, int n3)
+{
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q < n3) out[q] = (double)ksc[q];
+}
+
+}  // namespace
+
+int farfield_noalloc_max_dirs() { return kNoAllocMaxDirs; }
+
+// Device address of the scratch array on the current device, looked up once per device.
+cudaError_t farfield_noalloc_scratch(int device, double **ptr)
+{
+    if (device < 0 || device >= kNoAllocMaxDevices) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_ptr[device]) {
+        void *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_farfield_scratch);
+        if (e != cudaSuccess) return e;
+        g_noalloc_ptr[device] = (double *)p;
+    }
+    *ptr = g_noalloc_ptr[device];
+    return cudaSuccess;
+}
+
+cudaError_t farfield_noalloc(const PostArgs &in, const float *ksc_dev, float2 *esc_dev,
+                             double *scratch, cudaStream_t st)
+{
+    PostArgs a = in;
+    a.nrhs = 1;
+    a.esc_acc = scratch;                       // [ndir][6]
+    double *kscd = scratch + (size_t)kNoAllocMaxDirs * 6;   // [ndir][3]
+    a.ksc = kscd;
+    cudaError_t e;
+    if ((e = post_prepare(a.nj, a.nl)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(a.esc_acc, 0, (size_t)a.ndir * 6 * sizeof(double), st))) return e;
+    const int n3 = 3 * a.ndir;
+    ksc_to_double<<<nblk((size_t)n3, 256), 256, 0, st>>>(ksc_dev, kscd, n3);
+    farfield_sum<<<dim3(nblk(a.ndir, FF_DIRS), a.ni, 1), 256, farfield_smem(a.nj, a.nl), st>>>(a);
+    post_finalize<<<nblk((size_t)a.ndir, 256), 256, 0, st>>>(a, esc_dev, nullptr, nullptr);
     return cudaGetLastError();
 }
 

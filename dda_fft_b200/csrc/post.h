@@ -36,4 +36,10 @@ cudaError_t post_prepare(int nj, int nl);
 cudaError_t launch_post(const PostArgs &a, float2 *esc, float *cabs, float *cext, cudaStream_t st);
 cudaError_t launch_mueller(const MuellerArgs &m, cudaStream_t st);
 
+// allocation-free far field (scratch in a file-scope device array of post.cu)
+int farfield_noalloc_max_dirs();
+cudaError_t farfield_noalloc_scratch(int device, double **ptr);
+cudaError_t farfield_noalloc(const PostArgs &a, const float *ksc_dev, float2 *esc_dev,
+                             double *scratch, cudaStream_t st);
+
 }  // namespace ddagpu

@@ -144,6 +144,22 @@ int ddagpu_mc_rotations(unsigned long long base_seed, int worker, int count, dou
 /* Fixed orientation (degrees), main.cpp:516-541. */
 int ddagpu_fixed_rotation(double psi, double iota, double kappa, double *rot);
 
+/* Far field that allocates nothing, for callers that must not allocate device memory
+ * (code under CUDA graph capture, real-time loops that forbid allocator calls, hosts that
+ * hand the library only pre-allocated buffers).  No counterpart in the reference.  Needs no
+ * context: the caller passes device pointers to the occupancy occ_dev [i][j][l], the
+ * material activity flags mv_dev (one int per material index found in occ_dev), the
+ * dipoles p_dev ([3][i][j][l] complex float, structure of arrays), the directions
+ * ksc_dev [ndir][3] float, and receives esc_dev [ndir][6] float (cvector per direction),
+ * all on `stream` (cudaStream_t; NULL = legacy default stream).  At most 8192 directions
+ * per call; more returns DDAGPU_EINVAL.  The FP64 accumulators live in a fixed 576 KiB
+ * device array that every GPU loading the library holds until exit; the first call on a
+ * device looks up that array's address, so make it before any stream capture.  Calls
+ * that overlap on the GPU share the array and race: serialise them (one stream). */
+int ddagpu_farfield_noalloc(int device, int i_max, int j_max, int l_max, float d0,
+                            const signed char *occ_dev, const int *mv_dev, const void *p_dev,
+                            int ndir, const float *ksc_dev, float *esc_dev, void *stream);
+
 /* ---------------------------------------------------------------- device-resident form
  * G*p for nrhs fields already in device memory ([nrhs][3][i][j][l] complex float, SoA),
  * on the context's stream; nrhs <= max_rhs. */
