@@ -25,6 +25,17 @@ DDA_DEV float2 cconj(float2 a) { return make_float2(a.x, -a.y); }
 DDA_DEV float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
 DDA_DEV float2 czero() { return make_float2(0.f, 0.f); }
 
+// exp(i ph) for a phase given in FP64: the reduction to [-pi, pi] is done in FP64 (phases
+// reach tens of radians), the sine and cosine of the reduced angle in float.
+DDA_DEV float2 expi_reduced(double ph)
+{
+    const double two_pi = 6.283185307179586476925286766559;
+    const double r = fma(-two_pi, rint(ph * (1.0 / two_pi)), ph);
+    float s, c;
+    sincosf((float)r, &s, &c);
+    return make_float2(c, s);
+}
+
 // W_16^m = exp(-2 pi i m / 16) for m = 0..7 (the values of cos and sin at multiples of
 // pi/8: 1, cos(pi/8) = 0.9238795..., sqrt(1/2), sin(pi/8) = 0.3826834...).
 DDA_DEV float2 w16(int m)

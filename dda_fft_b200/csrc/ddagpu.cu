@@ -256,8 +256,8 @@ int run_solver(ddagpu_ctx *c, int nrhs, int solver, float tau, int max_step, flo
     CK(matvec(c->p, c->r, 0.f, nullptr, 0));   // r = -alpha (G * p_inc)
     res.matvec0 = 1;
     switch (solver) {
-    case 0:
-        CK(field(OP_STEP0_CG));
+    case 0:   // s = r is deferred to the first iteration (an RHS converged at step 0 never needs it)
+        CK(field(OP_ERR));
         CK(scal(SC_STEP0_ERR1, 0));
         break;
     case 1:
@@ -286,12 +286,7 @@ int run_solver(ddagpu_ctx *c, int nrhs, int solver, float tau, int max_step, flo
         break;
     }
     CK(scal(SC_START, 0));
-    // p_min = p at step 0
-    {
-        for (int k = 0; k < nrhs; k++)
-            CK(cudaMemcpyAsync(c->pmin + (size_t)k * 3 * c->N, c->p + (size_t)k * 3 * c->N,
-                               3 * c->N * sizeof(float2), cudaMemcpyDeviceToDevice, st));
-    }
+    // p_min = p (the step-0 iterate) is copied by the gated copy of the first iteration
     res.matvec_it = (solver == 1 || solver == 2) ? 2 : 1;
 
     // ---- iterations (dda_func.cpp:1301-1535)
@@ -307,6 +302,7 @@ int run_solver(ddagpu_ctx *c, int nrhs, int solver, float tau, int max_step, flo
         if (!any) break;
         switch (solver) {
         case 0:
+            if (o == 1) CK(field(OP_COPY_RS));
             CK(matvec(c->s, c->w, 1.f, c->s, 0));
             CK(field(OP_CG1));
             CK(scal(SC_CG1, o));

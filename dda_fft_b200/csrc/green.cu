@@ -9,7 +9,8 @@
 //   even axis:  sum_x f(x) e^{-i pi k x / n} = f(0) + 2 sum_{0<x<n} f(x) cos(pi k x / n)
 //   odd axis:                                  -2i sum_{0<x<n} f(x) sin(pi k x / n)
 // The three axis sums run in FP64 here; the octant is stored in float as
-// Ahat[comp][kx][ky][zmap(kz)], z in parity order (even kz first, then odd kz).
+// Ahat[kx][ky][zmap(kz)][comp], z in parity order (even kz first, then odd kz), so the six
+// components of one frequency form one 48-byte entry.
 #include "common.cuh"
 #include "internal.h"
 
@@ -92,13 +93,15 @@ __device__ inline int zmapd(int oz, int nl) { return (oz & 1) ? (nl / 2 + 1 + (o
 
 __global__ void to_octant(const double2 *in, float2 *ahat, int ni, int nj, int nl)
 {
+    // in[comp][kx][ky][kz] -> ahat[kx][ky][zmap(kz)][comp]
     const size_t per = (size_t)(ni + 1) * (nj + 1) * (nl + 1);
     const size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
     if (q >= 6 * per) return;
     const int oz = (int)(q % (nl + 1));
-    const size_t rest = q / (nl + 1);
+    const size_t xy = (q / (nl + 1)) % ((size_t)(ni + 1) * (nj + 1));
+    const int comp = (int)(q / per);
     const double2 v = in[q];
-    ahat[rest * (nl + 1) + zmapd(oz, nl)] = make_float2((float)v.x, (float)v.y);
+    ahat[((xy * (nl + 1)) + zmapd(oz, nl)) * 6 + comp] = make_float2((float)v.x, (float)v.y);
 }
 
 // Octant from a dense float Ahat [2ni][2nj][2nl][6] (the reference's cmA layout): the
@@ -127,7 +130,7 @@ __global__ void project_dense(const float2 *dense, float2 *ahat, int ni, int nj,
         sr += s * v.x;
         si += s * v.y;
     }
-    ahat[(((size_t)c * (ni + 1) + ox) * (nj + 1) + oy) * (nl + 1) + zmapd(oz, nl)] =
+    ahat[((((size_t)ox * (nj + 1) + oy) * (nl + 1)) + zmapd(oz, nl)) * 6 + c] =
         make_float2((float)(sr / 8.0), (float)(si / 8.0));
 }
 

@@ -59,7 +59,7 @@ struct MatvecArgs {
     size_t fstride;         // 3 N
     float2 *work;           // [nrhs][3][ni][2nj][2nl]
     size_t wstride;
-    const float2 *ahat;     // octant Green tensor [6][ni+1][nj+1][nl+1] (z in parity order)
+    const float2 *ahat;     // octant Green tensor [ni+1][nj+1][nl+1][6] (z in parity order)
     int conj;               // use conj(Ahat)
     float2 *out;            // [nrhs][3][N]
     Epilogue ep;

@@ -97,15 +97,16 @@ __global__ void __launch_bounds__(512) k2_x_product(MatvecArgs a)
     // Symmetric 3x3 product with the Green tensor at frequency (kx, j', l').
     const int hj = js >= nj, kj = js - hj * nj, jp = 2 * kj + hj;
     const int my = jp > nj, oy = my ? 2 * nj - jp : jp;
-    const size_t sz = (size_t)(nl + 1), sy = (size_t)(nj + 1) * sz, sx = (size_t)(ni + 1) * sy;
+    // Ahat[ox][oy][zmap(oz)][6]
+    const size_t sz = 6, sy = (size_t)(nl + 1) * 6, sxo = (size_t)(nj + 1) * sy;
     for (int e = threadIdx.x; e < 2 * ni * TW; e += blockDim.x) {
         const int t = e % TW, kh = e / TW, k = kh >> 1, hx = kh & 1;
         const int kx = 2 * k + hx, mx = kx > ni, ox = mx ? 2 * ni - kx : kx;
         const int ls = l0 + t, hl = ls >= nl, kl = ls - hl * nl, lp = 2 * kl + hl;
         const int mz = lp > nl, oz = mz ? 2 * nl - lp : lp;
-        const float2 *A = a.ahat + (size_t)ox * sy + (size_t)oy * sz + zmap(oz, nl);
-        float2 g0 = __ldg(A), g1 = __ldg(A + sx), g2 = __ldg(A + 2 * sx), g3 = __ldg(A + 3 * sx),
-               g4 = __ldg(A + 4 * sx), g5 = __ldg(A + 5 * sx);
+        const float2 *A = a.ahat + (size_t)ox * sxo + (size_t)oy * sy + (size_t)zmap(oz, nl) * sz;
+        float2 g0 = __ldg(A), g1 = __ldg(A + 1), g2 = __ldg(A + 2), g3 = __ldg(A + 3),
+               g4 = __ldg(A + 4), g5 = __ldg(A + 5);
         if (mx ^ my) g1 = cscale(g1, -1.f);
         if (mx ^ mz) g2 = cscale(g2, -1.f);
         if (my ^ mz) g4 = cscale(g4, -1.f);

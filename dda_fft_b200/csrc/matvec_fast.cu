@@ -10,8 +10,11 @@
 //   column role -- thread (sub, col) with consecutive lanes on consecutive lines; the
 //                  exchange needs the block (__syncthreads) but every access is a
 //                  contiguous run of the warp.
-// Shared planes use the swizzled row layout pos(p) = p + p/8 with a row stride PS = RM
-// (mod 16) float2, which keeps both roles free of bank conflicts.
+// Shared planes use the swizzled row layout pos(p) = p ^ ((p >> 3) & 7), a permutation
+// inside each aligned block of 8 elements, with a row stride PS = N + 8 or N + 4 float2
+// (PS = RM mod 16).  A warp reading 32 consecutive columns of one row, a row group reading
+// positions t2 + R2 r (step A) and a row group reading positions R2 k1 + t (step B) all
+// touch distinct banks.
 #include <cooperative_groups.h>
 
 #include "common.cuh"
@@ -27,12 +30,11 @@ template <int N>
 struct Sp {
     static constexpr int R1 = fft_split<N>::R1, R2 = fft_split<N>::R2;
     static constexpr int RM = R1 > R2 ? R1 : R2;
-    // swizzled row stride: N + N/8 rounded up to RM (mod 16)
-    static constexpr int base = N + N / 8;
-    static constexpr int PS = base + ((RM % 16) - (base % 16) + 16) % 16;
+    // row stride = RM (mod 16) float2: the rows of one half-warp land in disjoint banks
+    static constexpr int PS = N + ((RM % 16) - (N % 16) + 16) % 16;
 };
 
-DDA_DEV int spos(int p) { return p + (p >> 3); }
+DDA_DEV int spos(int p) { return p ^ ((p >> 3) & 7); }
 
 DDA_DEV int zmapf(int oz, int nl) { return (oz & 1) ? (nl / 2 + 1 + (oz >> 1)) : (oz >> 1); }
 
@@ -229,8 +231,9 @@ __global__ void __launch_bounds__(Sp<NI>::RM * TL) k2f(MatvecArgs a)
     const int my = jp > nj, oy = my ? 2 * nj - jp : jp;
     const int ls = l0 + t, hl = ls >= nl, kl = ls - hl * nl, lp = 2 * kl + hl;
     const int mz = lp > nl, oz = mz ? 2 * nl - lp : lp;
-    const size_t sz = (size_t)(nl + 1), sy = (size_t)(nj + 1) * sz, sx = (size_t)(NI + 1) * sy;
-    const float2 *Ayz = a.ahat + (size_t)oy * sz + zmapf(oz, nl);
+    // Ahat[ox][oy][zmap(oz)][6]: the 6 components of one frequency are one 48-byte entry
+    const size_t sz = 6, sy = (size_t)(nl + 1) * 6, sxo = (size_t)(nj + 1) * sy;
+    const float2 *Ayz = a.ahat + (size_t)oy * sy + (size_t)zmapf(oz, nl) * sz;
 #pragma unroll 1
     for (int h = 0; h < 2; h++) {
         float2 X[3][R2];
@@ -255,9 +258,11 @@ __global__ void __launch_bounds__(Sp<NI>::RM * TL) k2f(MatvecArgs a)
 #pragma unroll 1
                 for (int k = 0; k < R1; k++) {
                     const int kx = 2 * k + h, mx = kx > NI, ox = mx ? 2 * NI - kx : kx;
-                    const float2 *A = Ayz + (size_t)ox * sy;
-                    float2 g0 = __ldg(A), g1 = __ldg(A + sx), g2 = __ldg(A + 2 * sx),
-                           g3 = __ldg(A + 3 * sx), g4 = __ldg(A + 4 * sx), g5 = __ldg(A + 5 * sx);
+                    const float4 *A = reinterpret_cast<const float4 *>(Ayz + (size_t)ox * sxo);
+                    const float4 a01 = __ldg(A), a23 = __ldg(A + 1), a45 = __ldg(A + 2);
+                    float2 g0 = make_float2(a01.x, a01.y), g1 = make_float2(a01.z, a01.w),
+                           g2 = make_float2(a23.x, a23.y), g3 = make_float2(a23.z, a23.w),
+                           g4 = make_float2(a45.x, a45.y), g5 = make_float2(a45.z, a45.w);
                     if (mx ^ my) g1 = cscale(g1, -1.f);
                     if (mx ^ mz) g2 = cscale(g2, -1.f);
                     if (my ^ mz) g4 = cscale(g4, -1.f);
@@ -274,9 +279,11 @@ __global__ void __launch_bounds__(Sp<NI>::RM * TL) k2f(MatvecArgs a)
 #pragma unroll
                 for (int q = 0; q < R2; q++) {
                     const int kx = 2 * (k1 + R1 * q) + h, mx = kx > NI, ox = mx ? 2 * NI - kx : kx;
-                    const float2 *A = Ayz + (size_t)ox * sy;
-                    float2 g0 = __ldg(A), g1 = __ldg(A + sx), g2 = __ldg(A + 2 * sx),
-                           g3 = __ldg(A + 3 * sx), g4 = __ldg(A + 4 * sx), g5 = __ldg(A + 5 * sx);
+                    const float4 *A = reinterpret_cast<const float4 *>(Ayz + (size_t)ox * sxo);
+                    const float4 a01 = __ldg(A), a23 = __ldg(A + 1), a45 = __ldg(A + 2);
+                    float2 g0 = make_float2(a01.x, a01.y), g1 = make_float2(a01.z, a01.w),
+                           g2 = make_float2(a23.x, a23.y), g3 = make_float2(a23.z, a23.w),
+                           g4 = make_float2(a45.x, a45.y), g5 = make_float2(a45.z, a45.w);
                     if (mx ^ my) g1 = cscale(g1, -1.f);
                     if (mx ^ mz) g2 = cscale(g2, -1.f);
                     if (my ^ mz) g4 = cscale(g4, -1.f);

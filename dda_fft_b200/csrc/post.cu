@@ -43,9 +43,7 @@ __global__ void __launch_bounds__(256) farfield_sum(PostArgs a)
             if (pos < nl) ph = K[3 * d + 2] * (pos * a.d0 - cz);
             else if (pos < nl + nj) ph = K[3 * d + 1] * ((pos - nl) * a.d0 - cy);
             else ph = K[3 * d + 0] * (i * a.d0 - cx);
-            double s, c;
-            sincos(ph, &s, &c);
-            val = make_float2((float)c, (float)s);
+            val = expi_reduced(ph);
         }
         if (pos < nl) ez[pos * FF_DIRS + dl] = val;
         else if (pos < nl + nj) ey[(pos - nl) * FF_DIRS + dl] = val;
@@ -108,14 +106,10 @@ __global__ void __launch_bounds__(256) cabs_cext_sum(PostArgs a)
     const double cx = a.ni * a.d0 / 2, cy = nj * a.d0 / 2, cz = nl * a.d0 / 2;
     for (int e = threadIdx.x; e < nj + nl; e += blockDim.x) {
         const double ph = e < nj ? -k[1] * (e * a.d0 - cy) : -k[2] * ((e - nj) * a.d0 - cz);
-        double s, c;
-        sincos(ph, &s, &c);
-        tab[e] = make_float2((float)c, (float)s);
+        tab[e] = expi_reduced(ph);
     }
     __syncthreads();
-    double sx, cxx;
-    sincos(-k[0] * (i * a.d0 - cx), &sx, &cxx);
-    const float2 exv = make_float2((float)cxx, (float)sx);
+    const float2 exv = expi_reduced(-k[0] * (i * a.d0 - cx));
     const size_t N = a.N;
     const float2 *p = a.p + (size_t)rhs * 3 * N;
     const float2 *al = a.alpha + (size_t)rhs * a.nmat1;

@@ -212,6 +212,9 @@ __global__ void __launch_bounds__(256) field_op(FieldArgs a)
             st3(r, N, q, R);
         } else if (OP == OP_ERR) { // error only
             if (act) { ld3(r, N, q, R); v[0] += norm_cell(R); }
+        } else if (OP == OP_COPY_RS) { // s = r (CG step 0, deferred to the first iteration)
+            ld3(r, N, q, R);
+            st3(s, N, q, R);
         }
     }
     constexpr int NV = (OP == OP_CG1 || OP == OP_B_WW) ? 4
@@ -235,17 +238,17 @@ __global__ void __launch_bounds__(256) field_op(FieldArgs a)
 // phase is separable, so each block builds exp(i k_y y) and exp(i k_z z) tables.
 __global__ void __launch_bounds__(256) first_approx(FieldArgs a)
 {
-    extern __shared__ float2 tab[];   // [nj] y then [nl] z
+    extern __shared__ float2 tab[];   // [nj] y, [nl] z, then [ni] x
     const int rhs = blockIdx.y;
     if (a.rhs_active && !a.rhs_active[rhs]) return;
     const int ni = a.ni, nj = a.nj, nl = a.nl;
     const double *k = a.kinc + 3 * rhs, *E = a.einc + 6 * rhs;
     const double cx = (ni - 1) * a.d0 / 2, cy = (nj - 1) * a.d0 / 2, cz = (nl - 1) * a.d0 / 2;
-    for (int e = threadIdx.x; e < nj + nl; e += blockDim.x) {
-        double ph = e < nj ? k[1] * (e * a.d0 - cy) : k[2] * ((e - nj) * a.d0 - cz);
-        double sn, cs;
-        sincos(ph, &sn, &cs);
-        tab[e] = make_float2((float)cs, (float)sn);
+    for (int e = threadIdx.x; e < nj + nl + ni; e += blockDim.x) {
+        const double ph = e < nj        ? k[1] * (e * a.d0 - cy)
+                        : e < nj + nl   ? k[2] * ((e - nj) * a.d0 - cz)
+                                        : k[0] * ((e - nj - nl) * a.d0 - cx);
+        tab[e] = expi_reduced(ph);
     }
     __syncthreads();
     const size_t N = a.N, off = (size_t)rhs * 3 * N;
@@ -256,9 +259,7 @@ __global__ void __launch_bounds__(256) first_approx(FieldArgs a)
         const int m = a.occ[q];
         float2 out[3];
         if (a.mv[m]) {
-            double sx, cxx;
-            sincos(k[0] * (i * a.d0 - cx), &sx, &cxx);
-            const float2 ph = cmul(cmul(make_float2((float)cxx, (float)sx), tab[j]), tab[nj + l]);
+            const float2 ph = cmul(cmul(tab[nj + nl + i], tab[j]), tab[nj + l]);
             const float2 c1 = cmul(ph, al[m]);
 #pragma unroll
             for (int c = 0; c < 3; c++)
@@ -352,6 +353,10 @@ __global__ void scalar_stage(RhsState *st, const int *rhs_active_in, int *rhs_ac
         S.need_copy = 0;
         if (S.err <= S.err_max) {
             S.active = 0;
+        } else if (step == 1) {
+            // the step-0 iterate is the best one so far (dda_func.cpp:1286-1293); it is
+            // stored only now, when an iteration is about to overwrite it
+            S.need_copy = 1;
         } else if (S.err < S.err_min) {
             S.err_min = S.err;
             S.step_min = step - 1;
@@ -398,7 +403,7 @@ cudaError_t launch_field_op(int op, const FieldArgs &a, cudaStream_t st)
         CASE(OP_STEP0_CG) CASE(OP_STEP0_AA) CASE(OP_STEP0_BICG) CASE(OP_STEP0_SIMPLE)
         CASE(OP_CG1) CASE(OP_CG2) CASE(OP_CG3) CASE(OP_AA1) CASE(OP_AA2) CASE(OP_AA3)
         CASE(OP_B_RHO) CASE(OP_B_S) CASE(OP_B_GH) CASE(OP_B_R) CASE(OP_B_WW) CASE(OP_B_P)
-        CASE(OP_SIMPLE) CASE(OP_ERR)
+        CASE(OP_SIMPLE) CASE(OP_ERR) CASE(OP_COPY_RS)
 #undef CASE
     default: return cudaErrorInvalidValue;
     }
@@ -408,7 +413,7 @@ cudaError_t launch_field_op(int op, const FieldArgs &a, cudaStream_t st)
 cudaError_t launch_first_approx(const FieldArgs &a, cudaStream_t st)
 {
     const unsigned bx = (unsigned)((a.N + 1023) / 1024);
-    first_approx<<<dim3(bx < 1 ? 1 : bx, a.nrhs), 256, (a.nj + a.nl) * sizeof(float2), st>>>(a);
+    first_approx<<<dim3(bx < 1 ? 1 : bx, a.nrhs), 256, (a.ni + a.nj + a.nl) * sizeof(float2), st>>>(a);
     return cudaGetLastError();
 }
 

@@ -9,7 +9,7 @@ enum FieldOp {
     OP_CG1, OP_CG2, OP_CG3,
     OP_AA1, OP_AA2, OP_AA3,
     OP_B_RHO, OP_B_S, OP_B_GH, OP_B_R, OP_B_WW, OP_B_P,
-    OP_SIMPLE, OP_ERR
+    OP_SIMPLE, OP_ERR, OP_COPY_RS
 };
 
 enum ScalarStage {
