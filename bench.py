@@ -176,9 +176,12 @@ def main():
     ap.add_argument("--profile-matvec", type=int, default=0, metavar="NRHS",
                     help="only run the matvec on NRHS right-hand sides (for ncu captures)")
     ap.add_argument("--grid", type=int, default=GRID)
+    ap.add_argument("--workload", default="orientations", choices=["orientations", "precision"])
     args = ap.parse_args()
     if args.profile_matvec:
         return profile_matvec(args)
+    if args.workload == "precision":
+        return precision_run(args)
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
@@ -368,6 +371,43 @@ def profile_matvec(args):
     torch.cuda.synchronize()
     print(json.dumps({"profile_matvec": nrhs, "grid": n, "launches": ctx.kernel_launches}))
     ctx.close()
+
+
+def precision_run(args):
+    """The precision configuration: 128^3 sphere, x = 16, m = 1.6+0.0005i, BiCGStab,
+    theta 0..180 step 2.  Plain float BiCGStab (the reference's method, Error_max 1e-5,
+    100 steps) beside FP64-residual refinement to 1e-5; one JSON line."""
+    import torch
+    import dda_fft_b200 as D
+    n, x, m = 128, 16.0, complex(1.6, 0.0005)
+    kd = 2 * x / n
+    occ = ellipsoid_occ(n, 1.0, 1.0)
+    alpha = np.array([0, _cm_alpha(kd, m)], np.complex64)
+    th = np.deg2rad(np.arange(91) * 2.0)
+    ksc = np.stack([np.sin(th), np.zeros_like(th), np.cos(th)], 1)[None]
+    out = {"workload": "precision: 128^3 sphere x=16 m=1.6+0.0005i BiCGStab, 91 angles",
+           "kernels": None}
+    with D.Context(n, kd) as ctx:
+        out["kernels"] = "specialised" if ctx.fast_kernels else "generic"
+        for q, e in enumerate(((1, 0, 0), (0, 1, 0))):
+            t0 = time.perf_counter()
+            r = ctx.dda_fft(occ, alpha, [0, 1], kd, (0, 0, 1), e, ksc, solver=2, max_step=100,
+                            err_max=1e-5)
+            torch.cuda.synchronize()
+            t1 = time.perf_counter()
+            f = ctx.dda_fft_refined(occ, alpha, [0, 1], kd, (0, 0, 1), e, ksc, solver=2,
+                                    err_max=1e-5, max_outer=40, inner_rel=0.05,
+                                    inner_max_step=300)
+            t2 = time.perf_counter()
+            out[f"pol{q}"] = {
+                "plain": {"steps": r["steps"], "err_final": r["err"], "err_min": r["err_min"],
+                          "rolled_back": r["rolled_back"], "cext": r["cext"], "cabs": r["cabs"],
+                          "seconds": t1 - t0, "trace_min": float(np.min(r["trace"]))},
+                "refined": {"outer": f["outer"], "inner_steps": f["inner_steps"],
+                            "matvecs": f["matvecs"], "err": f["err"],
+                            "history": [float(v) for v in f["history"]], "cext": f["cext"],
+                            "cabs": f["cabs"], "seconds": t2 - t1}}
+    print(json.dumps(out), flush=True)
 
 
 def _cm_alpha(d0, m):

@@ -49,6 +49,11 @@ class SolveInfo(C.Structure):
                 ("err", _d), ("err_min", _d)]
 
 
+class RefineInfo(C.Structure):
+    _fields_ = [("outer", _i), ("inner_steps", _i), ("matvecs", _i), ("err", _d),
+                ("err_history", _d * 64)]
+
+
 class _BatchCfg(C.Structure):
     _fields_ = [("solver", _i), ("tau", _f), ("max_step", _i), ("err_max", _f),
                 ("polarizability", _i), ("n_mat", _i), ("m", _p), ("occ", _p), ("nplanes", _i),
@@ -78,6 +83,8 @@ def lib():
         L.ddagpu_dda_fft.argtypes = [_p, _i, _i, _f, _i, _i, _i, _p, _p, _i, _p, _i, _f, _f, _p,
                                      _p, _i, _i, _i, _p, _p, _p, _p, C.POINTER(SolveInfo), _p]
         L.ddagpu_farfield.argtypes = [_p, _p, _i, _p, _f, _p, _i, _p, _p]
+        L.ddagpu_dda_fft_refined.argtypes = [_p, _i, _f, _p, _p, _i, _p, _f, _p, _p, _d, _i, _d,
+                                             _i, _i, _i, _p, _p, _p, _p, C.POINTER(RefineInfo)]
         L.ddagpu_cabscext.argtypes = [_p, _f, _p, _p, _p, _i, _p, _p, _p, _p]
         L.ddagpu_mueller.argtypes = [_p, _p, _p, _p, _i, _i, _p, _p, _p, _p, _p]
         L.ddagpu_orientation_solves.argtypes = [_p, C.POINTER(_BatchCfg), _i, _p, _p, _p, _p,
@@ -225,6 +232,28 @@ class Context:
         if trace:
             out["trace"] = tr[: info.steps + 1]
         return out
+
+    def dda_fft_refined(self, occ, alpha, listmv, d0, kinc, einc, ksc, solver=2, tau=0.0,
+                        err_max=1e-5, max_outer=20, inner_rel=0.05, inner_max_step=200):
+        """FP64-residual iterative refinement around the chosen solver."""
+        o = np.ascontiguousarray(occ, np.int8)
+        a = _cvec(np.asarray(alpha, np.complex64).reshape(-1, 1)).ravel()
+        mv = np.ascontiguousarray(listmv, np.int32)
+        ks = _f32(ksc)
+        npl, nang = ks.shape[:2]
+        esc = np.zeros((npl, nang, 3), np.complex64)
+        k = _f32(kinc)
+        e = _cvec(np.asarray(einc, np.complex64))
+        ca, ce = C.c_float(), C.c_float()
+        info = RefineInfo()
+        _check(lib().ddagpu_dda_fft_refined(self._h, solver, tau, _ptr(a), _ptr(mv), len(mv) - 1,
+                                            _ptr(o), d0, _ptr(k), _ptr(e), err_max, max_outer,
+                                            inner_rel, inner_max_step, npl, nang, _ptr(ks),
+                                            _ptr(esc.view(np.float32)), C.byref(ca), C.byref(ce),
+                                            C.byref(info)))
+        hist = np.array(info.err_history[: min(info.outer + 1, 64)])
+        return dict(esc=esc, cabs=ca.value, cext=ce.value, outer=info.outer,
+                    inner_steps=info.inner_steps, matvecs=info.matvecs, err=info.err, history=hist)
 
     def farfield(self, occ, listmv, d0, p, ksc) -> np.ndarray:
         o = np.ascontiguousarray(occ, np.int8)

@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstddef>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -85,6 +86,8 @@ struct ddagpu_ctx {
     float2 *esc = nullptr;
     float *cabs = nullptr, *cext = nullptr;
     int nplane_cap = 0, nangle_cap = 0;
+    float2 *b32 = nullptr, *rb = nullptr;   // refinement: outer and inner right-hand sides
+    double2 *x64 = nullptr;                 // refinement: FP64 solution
     bool occ_valid = false;      // occupancy of the last batched call is resident
     int occ_nmat1 = 0, occ_nact = 0;
     long long launches = 0;      // kernels launched by this context
@@ -197,6 +200,10 @@ FieldArgs fa_args(ddagpu_ctx *c, int nrhs, int nmat1, double d0, float tau)
     f.einc = c->einc;
     f.d0 = d0;
     f.tau = tau;
+    f.b = c->b32;
+    f.rb = c->rb;
+    f.x64 = c->x64;
+    f.rhs_in = nullptr;
     return f;
 }
 
@@ -209,7 +216,8 @@ struct SolveResult {
 // The solver of DDA_FFT for nrhs right-hand sides whose occ, mv, alpha, kinc and einc are
 // already on the device.  Leaves the final (or rolled-back) dipoles in c->p.
 int run_solver(ddagpu_ctx *c, int nrhs, int solver, float tau, int max_step, float err_max,
-               int nmat1, double d0, int nact, SolveResult &res, bool want_trace)
+               int nmat1, double d0, int nact, SolveResult &res, bool want_trace,
+               const float2 *rhs_in = nullptr)
 {
     if (solver < 0 || solver > 3) return fail(DDAGPU_EINVAL, "solver must be 0..3");
     if (max_step < 0) return fail(DDAGPU_EINVAL, "Max_Step must be >= 0");
@@ -236,6 +244,7 @@ int run_solver(ddagpu_ctx *c, int nrhs, int solver, float tau, int max_step, flo
     CK(cudaMemcpyAsync(c->active, ones.data(), nrhs * sizeof(int), cudaMemcpyHostToDevice, st));
 
     FieldArgs F = fa_args(c, nrhs, nmat1, d0, tau);
+    F.rhs_in = rhs_in;
     auto field = [&](int op) {
         c->launches += 1;
         return launch_field_op(op, F, st);
@@ -250,8 +259,9 @@ int run_solver(ddagpu_ctx *c, int nrhs, int solver, float tau, int max_step, flo
         return launch_matvec(mv_args(c, nrhs, src, out, 1, sv, v, conj, nmat1, true), st);
     };
 
-    // ---- step 0 (dda_func.cpp:1102-1293)
-    CK(launch_first_approx(F, st));
+    // ---- step 0 (dda_func.cpp:1102-1293): p = p_inc, or the given right-hand side
+    if (rhs_in) CK(launch_refine(4, F, st));
+    else CK(launch_first_approx(F, st));
     c->launches += 1;
     CK(matvec(c->p, c->r, 0.f, nullptr, 0));   // r = -alpha (G * p_inc)
     res.matvec0 = 1;
@@ -519,6 +529,9 @@ int ddagpu_destroy(ddagpu_ctx *c)
     if (!c) return DDAGPU_OK;
     DevGuard dg(c->dev);
     if (c->st) cudaStreamSynchronize(c->st);
+    if (c->b32) cudaFree(c->b32);
+    if (c->rb) cudaFree(c->rb);
+    if (c->x64) cudaFree(c->x64);
     void *ptrs[] = {c->ahat, c->tw,     c->work,   c->p,       c->pmin,   c->r,     c->s,
                     c->w,    c->g,      c->h,      c->state,   c->active, c->trace, c->occ,
                     c->mv,   c->alpha,  c->kinc,   c->einc,    c->ksc,    c->esc_acc,
@@ -784,6 +797,111 @@ int ddagpu_dda_fft(ddagpu_ctx *c, int iNoIllumination, int solver, float rTau, i
     }
     if (trace)
         for (int k = 0; k <= Max_Step; k++) trace[k] = k <= S.steps ? res.trace[(size_t)k] : 0.0;
+    return DDAGPU_OK;
+}
+
+int ddagpu_dda_fft_refined(ddagpu_ctx *c, int solver, float rTau, const float *cListMaterials,
+                           const int *iListMV, int n_mat, const signed char *cAlpha, float d0,
+                           const float *kinc, const float *Einc, double Error_max, int max_outer,
+                           double inner_rel, int inner_max_step, int iNoScPl, int iNoA,
+                           const float *ksc, float *Esc, float *rCabs, float *rCext,
+                           ddagpu_refine_info *info)
+{
+    if (!c || !cListMaterials || !iListMV || !cAlpha || !kinc || !Einc || !rCabs || !rCext)
+        return fail(DDAGPU_EINVAL, "null argument");
+    if (max_outer < 0 || inner_max_step < 1 || !(inner_rel > 0.0 && inner_rel < 1.0) ||
+        !(Error_max > 0.0))
+        return fail(DDAGPU_EINVAL, "bad refinement parameters");
+    if (iNoScPl < 0 || iNoA < 0 || ((size_t)iNoScPl * iNoA > 0 && (!ksc || !Esc)))
+        return fail(DDAGPU_EINVAL, "bad scattering directions");
+    std::lock_guard<std::mutex> lk(c->mu);
+    DevGuard dg(c->dev);
+    const int nmat1 = n_mat + 1, ndir = iNoScPl * iNoA;
+    const size_t n3 = 3 * c->N;
+    if (!c->b32) {
+        CK(dalloc(&c->b32, n3));
+        CK(dalloc(&c->rb, n3));
+        CK(dalloc(&c->x64, n3));
+    }
+    RET(upload_materials(c, iListMV, nmat1, cAlpha));
+    RET(ensure_post(c, std::max(ndir, 1), std::max(iNoScPl, 1), std::max(iNoA, 1)));
+    std::vector<float2> al((size_t)nmat1);
+    for (int m = 0; m < nmat1; m++) al[(size_t)m] = make_float2(cListMaterials[2 * m], cListMaterials[2 * m + 1]);
+    double kd3[3] = {kinc[0], kinc[1], kinc[2]}, ed6[6];
+    for (int k = 0; k < 6; k++) ed6[k] = Einc[k];
+    std::vector<double> kdir((size_t)ndir * 3);
+    for (size_t k = 0; k < kdir.size(); k++) kdir[k] = ksc[k];
+    CK(cudaMemcpyAsync(c->alpha, al.data(), nmat1 * sizeof(float2), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->kinc, kd3, sizeof kd3, cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->einc, ed6, sizeof ed6, cudaMemcpyHostToDevice, c->st));
+    if (ndir) CK(cudaMemcpyAsync(c->ksc, kdir.data(), kdir.size() * sizeof(double), cudaMemcpyHostToDevice, c->st));
+    const int nact = count_active(cAlpha, c->N, iListMV, nmat1);
+    if (nact == 0) return fail(DDAGPU_EINVAL, "no active dipoles");
+    // outer right-hand side b = p_inc (FirstApproximation), x = b
+    {
+        RhsState S0;
+        std::memset(&S0, 0, sizeof S0);
+        S0.active = 1;
+        S0.nact = nact;
+        int one = 1;
+        CK(cudaMemcpyAsync(c->state, &S0, sizeof S0, cudaMemcpyHostToDevice, c->st));
+        CK(cudaMemcpyAsync(c->active, &one, sizeof one, cudaMemcpyHostToDevice, c->st));
+    }
+    FieldArgs F = fa_args(c, 1, nmat1, d0, rTau);
+    CK(launch_first_approx(F, c->st));
+    CK(cudaMemcpyAsync(c->b32, c->p, n3 * sizeof(float2), cudaMemcpyDeviceToDevice, c->st));
+    CK(launch_refine(0, F, c->st));
+    c->launches += 2;
+    ddagpu_refine_info ri;
+    std::memset(&ri, 0, sizeof ri);
+    double err = 0.0;
+    for (int k = 0;; k++) {
+        // true residual in FP64: r = b - (x - alpha G*x), G*x from the float matvec
+        CK(launch_refine(3, F, c->st));
+        CK(launch_matvec(mv_args(c, 1, c->p, c->w, 0, 0.f, nullptr, 0, nmat1, false), c->st));
+        const double zero8[kAcc] = {0, 0, 0, 0, 0, 0, 0, 0};
+        double *acc_dev = reinterpret_cast<double *>(reinterpret_cast<char *>(c->state) +
+                                                     offsetof(RhsState, acc));
+        CK(cudaMemcpyAsync(acc_dev, zero8, sizeof zero8, cudaMemcpyHostToDevice, c->st));
+        int one = 1;
+        CK(cudaMemcpyAsync(c->active, &one, sizeof one, cudaMemcpyHostToDevice, c->st));
+        CK(launch_refine(1, F, c->st));
+        c->launches += 5;
+        double acc = 0.0;
+        CK(cudaMemcpyAsync(&acc, acc_dev, sizeof acc, cudaMemcpyDeviceToHost, c->st));
+        CK(cudaStreamSynchronize(c->st));
+        err = acc / nact;
+        if (k < 64) ri.err_history[k] = err;
+        ri.outer = k;
+        if (err <= Error_max || k >= max_outer) break;
+        // inner FP32 solve of A d = r from d0 = r, to a fraction of the current error
+        SolveResult res;
+        const float inner_err = (float)std::max(inner_rel * err, 0.5 * Error_max);
+        RET(run_solver(c, 1, solver, rTau, inner_max_step, inner_err, nmat1, d0, nact, res, false, c->rb));
+        ri.inner_steps += res.st[0].steps;
+        ri.matvecs += res.matvec0 + res.matvec_it * res.st[0].steps;
+        int one2 = 1;
+        CK(cudaMemcpyAsync(c->active, &one2, sizeof one2, cudaMemcpyHostToDevice, c->st));
+        CK(launch_refine(2, F, c->st));
+        c->launches += 1;
+    }
+    ri.err = err;
+    ri.matvecs += ri.outer + 1;
+    CK(launch_refine(3, F, c->st));
+    RET(run_post(c, 1, nmat1, d0, ndir));
+    std::vector<float2> esc((size_t)ndir * 3);
+    float ca = 0, ce = 0;
+    if (ndir) CK(cudaMemcpyAsync(esc.data(), c->esc, esc.size() * sizeof(float2), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaMemcpyAsync(&ca, c->cabs, sizeof(float), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaMemcpyAsync(&ce, c->cext, sizeof(float), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    for (size_t k = 0; k < esc.size(); k++) {
+        Esc[2 * k] = esc[k].x;
+        Esc[2 * k + 1] = esc[k].y;
+    }
+    *rCabs = ca;
+    *rCext = ce;
+    if (info) *info = ri;
     return DDAGPU_OK;
 }
 

@@ -392,7 +392,82 @@ __global__ void __launch_bounds__(256) gated_copy(FieldArgs a, int dir)
         dst[q] = src[q];
 }
 
+// Iterative refinement passes over all 3 components of every cell.
+__global__ void __launch_bounds__(256) refine_op(FieldArgs a, int op)
+{
+    __shared__ double scratch[8];
+    const int rhs = blockIdx.y;
+    if (a.rhs_active && !a.rhs_active[rhs]) return;
+    const size_t N = a.N, off = (size_t)rhs * 3 * N;
+    double v[1] = {0.0};
+    for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < N;
+         q += (size_t)gridDim.x * blockDim.x) {
+        const int m = a.occ[q];
+        const bool act = a.mv[m] != 0;
+        if (op == 0) {
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                const float2 x = a.b[off + c * N + q];
+                a.x64[off + c * N + q] = make_double2(x.x, x.y);
+            }
+        } else if (op == 1) {
+            const float2 al = a.alpha[(size_t)rhs * a.nmat1 + m];
+            double nrm = 0.0;
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                const size_t o = off + c * N + q;
+                double rr = 0.0, ri = 0.0;
+                if (act) {
+                    const float2 cv = a.w[o], bb = a.b[o];
+                    const double2 x = a.x64[o];
+                    // A x = x - alpha conv, r = b - A x
+                    const double acr = (double)al.x * cv.x - (double)al.y * cv.y;
+                    const double aci = (double)al.x * cv.y + (double)al.y * cv.x;
+                    rr = (double)bb.x - (x.x - acr);
+                    ri = (double)bb.y - (x.y - aci);
+                }
+                nrm += rr * rr + ri * ri;
+                a.rb[o] = make_float2((float)rr, (float)ri);
+            }
+            if (act) v[0] += sqrt(nrm);
+        } else if (op == 2) {
+            if (act) {
+#pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    const size_t o = off + c * N + q;
+                    const float2 d = a.p[o];
+                    double2 x = a.x64[o];
+                    x.x += d.x;
+                    x.y += d.y;
+                    a.x64[o] = x;
+                }
+            }
+        } else if (op == 3) {
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                const size_t o = off + c * N + q;
+                const double2 x = a.x64[o];
+                a.p[o] = make_float2((float)x.x, (float)x.y);
+            }
+        } else {
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                const size_t o = off + c * N + q;
+                a.p[o] = act ? a.rhs_in[o] : czero();
+            }
+        }
+    }
+    if (op == 1) block_sum_atomic<1>(v, scratch, a.st[rhs].acc);
+}
+
 }  // namespace
+
+cudaError_t launch_refine(int op, const FieldArgs &a, cudaStream_t st)
+{
+    const unsigned bx = (unsigned)((a.N + 1023) / 1024);
+    refine_op<<<dim3(bx < 1 ? 1 : bx, a.nrhs), 256, 0, st>>>(a, op);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_field_op(int op, const FieldArgs &a, cudaStream_t st)
 {

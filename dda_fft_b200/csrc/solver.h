@@ -33,6 +33,11 @@ struct FieldArgs {
     const double *einc;       // [nrhs][6]
     double d0;
     float tau;
+    // iterative refinement (FP64 solution and residual)
+    const float2 *b;          // [nrhs][3][N] right-hand side of the outer system (p_inc)
+    float2 *rb;               // [nrhs][3][N] right-hand side of the inner solve (float r)
+    double2 *x64;             // [nrhs][3][N] FP64 solution
+    const float2 *rhs_in;     // step 0 starts from p = rhs_in instead of p_inc when set
 };
 
 cudaError_t launch_field_op(int op, const FieldArgs &a, cudaStream_t st);
@@ -40,5 +45,9 @@ cudaError_t launch_first_approx(const FieldArgs &a, cudaStream_t st);
 cudaError_t launch_scalar(RhsState *st_, const int *act_in, int *act_out, int nrhs, int stage,
                           int step, double *trace, int trace_len, cudaStream_t st);
 cudaError_t launch_gated_copy(const FieldArgs &a, int dir, cudaStream_t st);
+
+// refinement passes: 0 x64 = b; 1 r = b - (x64 - alpha conv) with conv in w, error into
+// acc[0], inner rhs rb = float(r); 2 x64 += p; 3 p = float(x64); 4 p = rhs_in
+cudaError_t launch_refine(int op, const FieldArgs &a, cudaStream_t st);
 
 }  // namespace ddagpu

@@ -85,6 +85,29 @@ int ddagpu_dda_fft(ddagpu_ctx *ctx, int iNoIllumination, int iMode_SolutionMetho
                    int iMode_FFT, int iNoScPl, int iNoA, const float *ksc, float *Esc,
                    float *rCabs, float *rCext, ddagpu_solve_info *info, double *trace);
 
+/* Iterative refinement around DDA_FFT's solvers: the solution and the true residual
+ * r = p_inc - (p - alpha G*p) are kept in FP64, each outer step solves A d = r in FP32
+ * with solver iMode_SolutionMethod (restarted from d = r, to inner_rel x the current
+ * residual, at most inner_max_step iterations, best iterate kept) and adds d to p.  Stops
+ * when the mean true residual norm (the reference's discrepancy, dda_func.cpp:784-811, of
+ * the true instead of the recursively updated residual) is <= Error_max, or after
+ * max_outer steps; info reports the residual of every outer step.  Outputs as
+ * ddagpu_dda_fft. */
+typedef struct {
+    int outer;               /* outer steps taken                                       */
+    int inner_steps;         /* inner solver iterations, all outer steps                */
+    int matvecs;             /* convolutions, inner and outer                           */
+    double err;              /* final mean true residual norm                           */
+    double err_history[64];  /* mean true residual norm before each outer step          */
+} ddagpu_refine_info;
+
+int ddagpu_dda_fft_refined(ddagpu_ctx *ctx, int iMode_SolutionMethod, float rTau,
+                           const float *cListMaterials, const int *iListMV, int n_mat,
+                           const signed char *cAlpha, float d0, const float *kinc,
+                           const float *Einc, double Error_max, int max_outer, double inner_rel,
+                           int inner_max_step, int iNoScPl, int iNoA, const float *ksc,
+                           float *Esc, float *rCabs, float *rCext, ddagpu_refine_info *info);
+
 /* FarField sub-seam (dda_func.cpp:1576-1625) for ndir directions at once. */
 int ddagpu_farfield(ddagpu_ctx *ctx, const int *iListMV, int n_mat, const signed char *cAlpha,
                     float d0, const float *p, int ndir, const float *ksc, float *Esc);
