@@ -176,12 +176,15 @@ def main():
     ap.add_argument("--profile-matvec", type=int, default=0, metavar="NRHS",
                     help="only run the matvec on NRHS right-hand sides (for ncu captures)")
     ap.add_argument("--grid", type=int, default=GRID)
-    ap.add_argument("--workload", default="orientations", choices=["orientations", "precision"])
+    ap.add_argument("--workload", default="orientations",
+                    choices=["orientations", "precision", "adjoint"])
     args = ap.parse_args()
     if args.profile_matvec:
         return profile_matvec(args)
     if args.workload == "precision":
         return precision_run(args)
+    if args.workload == "adjoint":
+        return adjoint_run(args)
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
@@ -408,6 +411,38 @@ def precision_run(args):
                             "history": [float(v) for v in f["history"]], "cext": f["cext"],
                             "cabs": f["cabs"], "seconds": t2 - t1}}
     print(json.dumps(out), flush=True)
+
+
+def adjoint_run(args):
+    """The differentiation configuration: two-material porous 64^3 cube (packing 0.3,
+    materials 1.5+0.01i / 1.7+0.1i at 0.7 / 0.3, seed 11), x = 5, CMRR, CG; forward pass
+    (both polarisations) and the adjoint gradient of Cabs + M11(180 deg) for every dipole;
+    one JSON line with the times and matvec counts of both passes."""
+    import torch
+    from dda_fft_b200.adjoint import GPUBackend, Problem, observables, porous_target
+    n = args.grid
+    filled, m = porous_target(n, seed=11)
+    P = Problem(filled, kd=2 * 5.0 / n, model="cmrr")
+    G = GPUBackend(P, err_max=1e-8)
+    m_re = torch.tensor(m.real, requires_grad=True)
+    m_im = torch.tensor(m.imag, requires_grad=True)
+    observables(m_re, m_im, P, G)                       # warm-up
+    mv0 = G.matvecs
+    t0 = time.perf_counter()
+    f = observables(m_re, m_im, P, G)
+    t1 = time.perf_counter()
+    mv1 = G.matvecs
+    (f[0] + f[1]).backward()
+    t2 = time.perf_counter()
+    mv2 = G.matvecs
+    print(json.dumps({"workload": f"adjoint: {n}^3 porous two-material cube, x=5, CMRR, CG",
+                      "dipoles": int(P.ndip), "cabs": float(f[0]), "m11_180": float(f[1]),
+                      "forward_s": t1 - t0, "backward_s": t2 - t1,
+                      "backward_over_forward": (t2 - t1) / (t1 - t0),
+                      "forward_matvecs": mv1 - mv0, "backward_matvecs": mv2 - mv1,
+                      "grad_norm_re": float(np.linalg.norm(m_re.grad.numpy())),
+                      "grad_norm_im": float(np.linalg.norm(m_im.grad.numpy()))}), flush=True)
+    G.close()
 
 
 def _cm_alpha(d0, m):

@@ -83,6 +83,8 @@ def lib():
         L.ddagpu_dda_fft.argtypes = [_p, _i, _i, _f, _i, _i, _i, _p, _p, _i, _p, _i, _f, _f, _p,
                                      _p, _i, _i, _i, _p, _p, _p, _p, C.POINTER(SolveInfo), _p]
         L.ddagpu_farfield.argtypes = [_p, _p, _i, _p, _f, _p, _i, _p, _p]
+        L.ddagpu_solve_linear.argtypes = [_p, _i, _f, _p, _p, _i, _p, _p, _d, _i, _i, _d, _i, _p,
+                                          C.POINTER(RefineInfo)]
         L.ddagpu_dda_fft_refined.argtypes = [_p, _i, _f, _p, _p, _i, _p, _f, _p, _p, _d, _i, _d,
                                              _i, _i, _i, _p, _p, _p, _p, C.POINTER(RefineInfo)]
         L.ddagpu_cabscext.argtypes = [_p, _f, _p, _p, _p, _i, _p, _p, _p, _p]
@@ -254,6 +256,23 @@ class Context:
         hist = np.array(info.err_history[: min(info.outer + 1, 64)])
         return dict(esc=esc, cabs=ca.value, cext=ce.value, outer=info.outer,
                     inner_steps=info.inner_steps, matvecs=info.matvecs, err=info.err, history=hist)
+
+    def solve_linear(self, occ, alpha, listmv, rhs, solver=0, tau=0.0, err_max=1e-8,
+                     max_step=40, refine=True, inner_rel=0.05, inner_max_step=300):
+        """x with (I - D_alpha G) x = rhs; rhs complex (ni, nj, nl, 3)."""
+        o = np.ascontiguousarray(occ, np.int8)
+        a = _cvec(np.asarray(alpha, np.complex64).reshape(-1, 1)).ravel()
+        mv = np.ascontiguousarray(listmv, np.int32)
+        b = _cvec(rhs)
+        x = np.zeros_like(b)
+        info = RefineInfo()
+        _check(lib().ddagpu_solve_linear(self._h, solver, tau, _ptr(a), _ptr(mv), len(mv) - 1,
+                                         _ptr(o), _ptr(b), err_max, max_step, int(refine),
+                                         inner_rel, inner_max_step, _ptr(x), C.byref(info)))
+        hist = np.array(info.err_history[: min(info.outer + 1, 64)])
+        return x.view(np.complex64).reshape(np.shape(rhs)), dict(
+            outer=info.outer, inner_steps=info.inner_steps, matvecs=info.matvecs, err=info.err,
+            history=hist)
 
     def farfield(self, occ, listmv, d0, p, ksc) -> np.ndarray:
         o = np.ascontiguousarray(occ, np.int8)

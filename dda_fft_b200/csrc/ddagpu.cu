@@ -800,6 +800,140 @@ int ddagpu_dda_fft(ddagpu_ctx *c, int iNoIllumination, int solver, float rTau, i
     return DDAGPU_OK;
 }
 
+}  // extern "C"
+namespace {
+
+// Outer refinement loop for one right-hand side already in c->b32 (see
+// ddagpu_dda_fft_refined); leaves p = float(x64).
+int refine_loop(ddagpu_ctx *c, int solver, float rTau, int nmat1, double d0, int nact,
+                double Error_max, int max_outer, double inner_rel, int inner_max_step,
+                ddagpu_refine_info &ri, double &err)
+{
+    FieldArgs F = fa_args(c, 1, nmat1, d0, rTau);
+    {
+        int one = 1;
+        CK(cudaMemcpyAsync(c->active, &one, sizeof one, cudaMemcpyHostToDevice, c->st));
+    }
+    CK(launch_refine(0, F, c->st));
+    c->launches += 1;
+    std::memset(&ri, 0, sizeof ri);
+    err = 0.0;
+    for (int k = 0;; k++) {
+        // true residual in FP64: r = b - (x - alpha G*x), G*x from the float matvec
+        CK(launch_refine(3, F, c->st));
+        CK(launch_matvec(mv_args(c, 1, c->p, c->w, 0, 0.f, nullptr, 0, nmat1, false), c->st));
+        const double zero8[kAcc] = {0, 0, 0, 0, 0, 0, 0, 0};
+        double *acc_dev = reinterpret_cast<double *>(reinterpret_cast<char *>(c->state) +
+                                                     offsetof(RhsState, acc));
+        CK(cudaMemcpyAsync(acc_dev, zero8, sizeof zero8, cudaMemcpyHostToDevice, c->st));
+        int one = 1;
+        CK(cudaMemcpyAsync(c->active, &one, sizeof one, cudaMemcpyHostToDevice, c->st));
+        CK(launch_refine(1, F, c->st));
+        c->launches += 5;
+        double acc = 0.0;
+        CK(cudaMemcpyAsync(&acc, acc_dev, sizeof acc, cudaMemcpyDeviceToHost, c->st));
+        CK(cudaStreamSynchronize(c->st));
+        err = acc / nact;
+        if (k < 64) ri.err_history[k] = err;
+        ri.outer = k;
+        if (err <= Error_max || k >= max_outer) break;
+        // inner FP32 solve of A d = r from d0 = r, to a fraction of the current error
+        SolveResult res;
+        const float inner_err = (float)std::max(inner_rel * err, 0.5 * Error_max);
+        RET(run_solver(c, 1, solver, rTau, inner_max_step, inner_err, nmat1, d0, nact, res, false, c->rb));
+        ri.inner_steps += res.st[0].steps;
+        ri.matvecs += res.matvec0 + res.matvec_it * res.st[0].steps;
+        CK(cudaMemcpyAsync(c->active, &one, sizeof one, cudaMemcpyHostToDevice, c->st));
+        CK(launch_refine(2, F, c->st));
+        c->launches += 1;
+    }
+    ri.err = err;
+    ri.matvecs += ri.outer + 1;
+    CK(launch_refine(3, F, c->st));
+    c->launches += 1;
+    return DDAGPU_OK;
+}
+
+void aos_to_soa(const float *in, float2 *out, size_t N)
+{
+    for (size_t q = 0; q < N; q++)
+        for (int k = 0; k < 3; k++) out[k * N + q] = make_float2(in[6 * q + 2 * k], in[6 * q + 2 * k + 1]);
+}
+
+void soa_to_aos(const float2 *in, float *out, size_t N)
+{
+    for (size_t q = 0; q < N; q++)
+        for (int k = 0; k < 3; k++) {
+            out[6 * q + 2 * k] = in[k * N + q].x;
+            out[6 * q + 2 * k + 1] = in[k * N + q].y;
+        }
+}
+
+}  // namespace
+
+extern "C" {
+
+int ddagpu_solve_linear(ddagpu_ctx *c, int solver, float rTau, const float *cListMaterials,
+                        const int *iListMV, int n_mat, const signed char *cAlpha, const float *rhs,
+                        double Error_max, int max_step, int refine, double inner_rel,
+                        int inner_max_step, float *x_out, ddagpu_refine_info *info)
+{
+    if (!c || !cListMaterials || !iListMV || !cAlpha || !rhs || !x_out)
+        return fail(DDAGPU_EINVAL, "null argument");
+    if (!(Error_max > 0.0) || max_step < 0 || (refine && (inner_max_step < 1 ||
+                                                          !(inner_rel > 0.0 && inner_rel < 1.0))))
+        return fail(DDAGPU_EINVAL, "bad solve parameters");
+    std::lock_guard<std::mutex> lk(c->mu);
+    DevGuard dg(c->dev);
+    const int nmat1 = n_mat + 1;
+    const size_t n3 = 3 * c->N;
+    if (!c->b32) {
+        CK(dalloc(&c->b32, n3));
+        CK(dalloc(&c->rb, n3));
+        CK(dalloc(&c->x64, n3));
+    }
+    RET(upload_materials(c, iListMV, nmat1, cAlpha));
+    std::vector<float2> al((size_t)nmat1);
+    for (int m = 0; m < nmat1; m++) al[(size_t)m] = make_float2(cListMaterials[2 * m], cListMaterials[2 * m + 1]);
+    CK(cudaMemcpyAsync(c->alpha, al.data(), nmat1 * sizeof(float2), cudaMemcpyHostToDevice, c->st));
+    const int nact = count_active(cAlpha, c->N, iListMV, nmat1);
+    if (nact == 0) return fail(DDAGPU_EINVAL, "no active dipoles");
+    std::vector<float2> soa(n3);
+    aos_to_soa(rhs, soa.data(), c->N);
+    CK(cudaMemcpyAsync(c->b32, soa.data(), n3 * sizeof(float2), cudaMemcpyHostToDevice, c->st));
+    ddagpu_refine_info ri;
+    std::memset(&ri, 0, sizeof ri);
+    if (refine) {
+        RhsState S0;
+        std::memset(&S0, 0, sizeof S0);
+        S0.active = 1;
+        S0.nact = nact;
+        CK(cudaMemcpyAsync(c->state, &S0, sizeof S0, cudaMemcpyHostToDevice, c->st));
+        double err = 0.0;
+        RET(refine_loop(c, solver, rTau, nmat1, c->kd, nact, Error_max, max_step, inner_rel,
+                        inner_max_step, ri, err));
+    } else {
+        SolveResult res;
+        RET(run_solver(c, 1, solver, rTau, max_step, (float)Error_max, nmat1, c->kd, nact, res,
+                       false, c->b32));
+        const RhsState &S = res.st[0];
+        ri.outer = 0;
+        ri.inner_steps = S.steps;
+        ri.matvecs = res.matvec0 + res.matvec_it * S.steps;
+        ri.err = S.restored ? S.err_min : S.err;
+        ri.err_history[0] = ri.err;
+    }
+    CK(cudaMemcpyAsync(soa.data(), c->p, n3 * sizeof(float2), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    soa_to_aos(soa.data(), x_out, c->N);
+    if (info) *info = ri;
+    return DDAGPU_OK;
+}
+
+}  // extern "C"
+
+extern "C" {
+
 int ddagpu_dda_fft_refined(ddagpu_ctx *c, int solver, float rTau, const float *cListMaterials,
                            const int *iListMV, int n_mat, const signed char *cAlpha, float d0,
                            const float *kinc, const float *Einc, double Error_max, int max_outer,
@@ -850,44 +984,11 @@ int ddagpu_dda_fft_refined(ddagpu_ctx *c, int solver, float rTau, const float *c
     FieldArgs F = fa_args(c, 1, nmat1, d0, rTau);
     CK(launch_first_approx(F, c->st));
     CK(cudaMemcpyAsync(c->b32, c->p, n3 * sizeof(float2), cudaMemcpyDeviceToDevice, c->st));
-    CK(launch_refine(0, F, c->st));
-    c->launches += 2;
+    c->launches += 1;
     ddagpu_refine_info ri;
-    std::memset(&ri, 0, sizeof ri);
     double err = 0.0;
-    for (int k = 0;; k++) {
-        // true residual in FP64: r = b - (x - alpha G*x), G*x from the float matvec
-        CK(launch_refine(3, F, c->st));
-        CK(launch_matvec(mv_args(c, 1, c->p, c->w, 0, 0.f, nullptr, 0, nmat1, false), c->st));
-        const double zero8[kAcc] = {0, 0, 0, 0, 0, 0, 0, 0};
-        double *acc_dev = reinterpret_cast<double *>(reinterpret_cast<char *>(c->state) +
-                                                     offsetof(RhsState, acc));
-        CK(cudaMemcpyAsync(acc_dev, zero8, sizeof zero8, cudaMemcpyHostToDevice, c->st));
-        int one = 1;
-        CK(cudaMemcpyAsync(c->active, &one, sizeof one, cudaMemcpyHostToDevice, c->st));
-        CK(launch_refine(1, F, c->st));
-        c->launches += 5;
-        double acc = 0.0;
-        CK(cudaMemcpyAsync(&acc, acc_dev, sizeof acc, cudaMemcpyDeviceToHost, c->st));
-        CK(cudaStreamSynchronize(c->st));
-        err = acc / nact;
-        if (k < 64) ri.err_history[k] = err;
-        ri.outer = k;
-        if (err <= Error_max || k >= max_outer) break;
-        // inner FP32 solve of A d = r from d0 = r, to a fraction of the current error
-        SolveResult res;
-        const float inner_err = (float)std::max(inner_rel * err, 0.5 * Error_max);
-        RET(run_solver(c, 1, solver, rTau, inner_max_step, inner_err, nmat1, d0, nact, res, false, c->rb));
-        ri.inner_steps += res.st[0].steps;
-        ri.matvecs += res.matvec0 + res.matvec_it * res.st[0].steps;
-        int one2 = 1;
-        CK(cudaMemcpyAsync(c->active, &one2, sizeof one2, cudaMemcpyHostToDevice, c->st));
-        CK(launch_refine(2, F, c->st));
-        c->launches += 1;
-    }
-    ri.err = err;
-    ri.matvecs += ri.outer + 1;
-    CK(launch_refine(3, F, c->st));
+    RET(refine_loop(c, solver, rTau, nmat1, d0, nact, Error_max, max_outer, inner_rel,
+                    inner_max_step, ri, err));
     RET(run_post(c, 1, nmat1, d0, ndir));
     std::vector<float2> esc((size_t)ndir * 3);
     float ca = 0, ce = 0;

@@ -108,6 +108,17 @@ int ddagpu_dda_fft_refined(ddagpu_ctx *ctx, int iMode_SolutionMethod, float rTau
                            int inner_max_step, int iNoScPl, int iNoA, const float *ksc,
                            float *Esc, float *rCabs, float *rCext, ddagpu_refine_info *info);
 
+/* A x = rhs for an arbitrary right-hand side (A = I - D_alpha G of the context's lattice):
+ * the solver of DDA_FFT started from x = rhs instead of p_inc (dda_func.cpp:1103-1104),
+ * to the discrepancy Error_max in max_step steps, or with refine != 0 by the FP64
+ * refinement above (max_step = outer steps).  rhs and x_out are host fields.  Used for
+ * adjoint solves: A^T = I - G D_alpha, so A^T l = g is A m = D_alpha g with l = m / alpha. */
+int ddagpu_solve_linear(ddagpu_ctx *ctx, int iMode_SolutionMethod, float rTau,
+                        const float *cListMaterials, const int *iListMV, int n_mat,
+                        const signed char *cAlpha, const float *rhs, double Error_max,
+                        int max_step, int refine, double inner_rel, int inner_max_step,
+                        float *x_out, ddagpu_refine_info *info);
+
 /* FarField sub-seam (dda_func.cpp:1576-1625) for ndir directions at once. */
 int ddagpu_farfield(ddagpu_ctx *ctx, const int *iListMV, int n_mat, const signed char *cAlpha,
                     float d0, const float *p, int ndir, const float *ksc, float *Esc);

@@ -552,9 +552,16 @@ int or_dda_fft(const or_solve_in *in, or_solve_out *out)
     if (!p || !pmin || !r || !s || !g || !h || !w || !tmp) return -1;
     int mv = 0;
 
-    /* step 0 (dda_func.cpp:1102-1278) */
-    or_first_approximation(L.ni, L.nj, L.nl, in->listmv, in->alpha, in->occ, in->d0, in->kinc,
-                           in->einc, (double *)p);
+    /* step 0 (dda_func.cpp:1102-1278); with a given right-hand side y the same recurrences
+       solve A p = y starting from p = y (y vanishes on inactive cells) */
+    if (in->rhs) {
+        const cd *y = (const cd *)in->rhs;
+        for (size_t q = 0; q < L.n; q++)
+            for (int c3 = 0; c3 < 3; c3++) p[3 * q + c3] = act(&L, q) ? y[3 * q + c3] : 0;
+    } else {
+        or_first_approximation(L.ni, L.nj, L.nl, in->listmv, in->alpha, in->occ, in->d0,
+                               in->kinc, in->einc, (double *)p);
+    }
     or_convolution(L.ni, L.nj, L.nl, in->ahat, (const double *)p, (double *)tmp, 0);
     mv++;
     for (size_t q = 0; q < L.n; q++)

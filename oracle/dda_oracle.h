@@ -55,6 +55,8 @@ typedef struct {
     int nplanes, nangles;
     const double *ksc;       /* [plane][angle][3]                                   */
     int cast_scalars_float;  /* 1: round solver scalars to float like the float build */
+    const double *rhs;       /* if not NULL: solve A p = rhs from p = rhs instead of the
+                                incident field (adjoint solves); field layout            */
 } or_solve_in;
 
 typedef struct {

@@ -161,7 +161,7 @@ class Oracle:
         return nrm, ksc
 
     def dda_fft(self, occ, alpha, listmv, d0, kinc, einc, ahat, ksc, solver=0, tau=0.0,
-                max_step=20, err_max=1e-3, cast_scalars_float=False):
+                max_step=20, err_max=1e-3, cast_scalars_float=False, rhs=None):
         """DDA_FFT for one polarisation; returns a dict with p, esc, cabs, cext, trace."""
         ni, nj, nl = occ.shape
         o = _c(occ, np.int8)
@@ -176,7 +176,7 @@ class Oracle:
                         ("nmat", _i), ("alpha", _p), ("listmv", _p), ("occ", _p),
                         ("max_step", _i), ("err_max", _d), ("d0", _d), ("kinc", _d * 3),
                         ("einc", _d * 6), ("ahat", _p), ("nplanes", _i), ("nangles", _i),
-                        ("ksc", _p), ("cast", _i)]
+                        ("ksc", _p), ("cast", _i), ("rhs", _p)]
 
         class Out(C.Structure):
             _fields_ = [("p", _p), ("esc", _p), ("cabs", _d), ("cext", _d), ("trace", _p),
@@ -185,8 +185,10 @@ class Oracle:
         e = np.asarray(einc, np.complex128)
         ein = (_d * 6)(*[v for z in e for v in (z.real, z.imag)])
         kin = (_d * 3)(*[float(v) for v in kinc])
+        y = None if rhs is None else _c(rhs, np.complex128)
         si = In(ni, nj, nl, solver, tau, len(a) - 1, _ptr(a), _ptr(mv), _ptr(o), max_step,
-                err_max, d0, kin, ein, _ptr(A), npl, nang, _ptr(ks), int(cast_scalars_float))
+                err_max, d0, kin, ein, _ptr(A), npl, nang, _ptr(ks), int(cast_scalars_float),
+                None if y is None else _ptr(y))
         p = np.zeros((ni, nj, nl, 3), np.complex128)
         esc = np.zeros((npl, nang, 3), np.complex128)
         trace = np.zeros(max_step + 1)
