@@ -436,7 +436,8 @@ def adjoint_run(args):
     t2 = time.perf_counter()
     mv2 = G.matvecs
     print(json.dumps({"workload": f"adjoint: {n}^3 porous two-material cube, x=5, CMRR, CG",
-                      "dipoles": int(P.ndip), "cabs": float(f[0]), "m11_180": float(f[1]),
+                      "dipoles": int(P.ndip), "cabs": float(f[0].detach()),
+                      "m11_180": float(f[1].detach()),
                       "forward_s": t1 - t0, "backward_s": t2 - t1,
                       "backward_over_forward": (t2 - t1) / (t1 - t0),
                       "forward_matvecs": mv1 - mv0, "backward_matvecs": mv2 - mv1,
