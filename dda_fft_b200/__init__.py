@@ -6,6 +6,7 @@ and benchmarks.  There is no CPU fallback: if the library cannot be loaded, ever
 raises.
 """
 from .api import (  # noqa: F401
+    Agglomerate,
     BatchConfig,
     Context,
     DDAGPUError,
@@ -17,5 +18,5 @@ from .api import (  # noqa: F401
     num_angles,
 )
 
-__all__ = ["Context", "BatchConfig", "DDAGPUError", "build", "lib", "library_path",
+__all__ = ["Agglomerate", "Context", "BatchConfig", "DDAGPUError", "build", "lib", "library_path",
            "mc_rotations", "fixed_rotation", "num_angles"]

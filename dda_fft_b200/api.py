@@ -105,6 +105,12 @@ def lib():
         L.ddagpu_set_kernels.argtypes = [_p, _i]
         L.ddagpu_farfield_noalloc.argtypes = [_i, _i, _i, _i, _f, _p, _p, _p, _i, _p, _p, _p]
         L.ddagpu_get_kernels.argtypes = [_p]
+        L.ddagpu_rng_seed.argtypes = [C.c_ulonglong, _i]
+        L.ddagpu_rng_seed.restype = C.c_ulonglong
+        L.ddagpu_anthrax_count.argtypes = [_i, _i, _i, _f, _f, _f]
+        L.ddagpu_anthrax_count.restype = C.c_longlong
+        L.ddagpu_anthrax_place.argtypes = [C.POINTER(C.c_ulonglong), _i, _f, _f, _i, _p]
+        L.ddagpu_anthrax_rasterize.argtypes = [_i, _i, _i, _i, _p, _i, _p, C.POINTER(_i)]
         _lib = L
         return L
 
@@ -142,6 +148,49 @@ def fixed_rotation(psi=0.0, iota=0.0, kappa=0.0) -> np.ndarray:
     out = np.zeros((3, 3))
     _check(lib().ddagpu_fixed_rotation(psi, iota, kappa, _ptr(out)))
     return out
+
+
+class Agglomerate:
+    """Anthrax-like agglomerates of capsule monomers (target 6, iGenerateAnthrax,
+    particle.cpp:21-85): monomers placed on the host from the reference's random stream,
+    rasterised into the lattice on the GPU.  `state` follows the stream across samples
+    like the worker's generator does (main.cpp:803-830)."""
+
+    def __init__(self, base_seed: int = 0, worker: int = 0, state: int | None = None):
+        self.state = int(lib().ddagpu_rng_seed(C.c_ulonglong(base_seed), worker)
+                         if state is None else state)
+
+    @staticmethod
+    def count(grid, packing: float, monomer_radius: float, length_ratio: float) -> int:
+        ni, nj, nl = grid
+        return int(lib().ddagpu_anthrax_count(ni, nj, nl, packing, monomer_radius, length_ratio))
+
+    def place(self, i_max: int, monomer_radius: float, monomer_length: float,
+              count: int) -> np.ndarray:
+        """monomers[count][13] float32: r, l, begin xyz, end xyz, axis xyz, 0, 0."""
+        out = np.zeros((count, 13), np.float32)
+        s = C.c_ulonglong(self.state)
+        _check(lib().ddagpu_anthrax_place(C.byref(s), i_max, monomer_radius, monomer_length,
+                                          count, _ptr(out)))
+        self.state = s.value
+        return out
+
+    @staticmethod
+    def rasterize(grid, monomers: np.ndarray, device: int = 0):
+        """(occ int8 [ni][nj][nl], 1 = filled; number of filled cells)."""
+        ni, nj, nl = grid
+        m = _f32(monomers)
+        occ = np.zeros((ni, nj, nl), np.int8)
+        nd = C.c_int(0)
+        _check(lib().ddagpu_anthrax_rasterize(device, ni, nj, nl, _ptr(m), len(m), _ptr(occ),
+                                              C.byref(nd)))
+        return occ, nd.value
+
+    def generate(self, grid, monomer_radius: float, monomer_length: float, count: int,
+                 device: int = 0):
+        mon = self.place(grid[0], monomer_radius, monomer_length, count)
+        occ, nd = self.rasterize(grid, mon, device)
+        return occ, nd, mon
 
 
 @dataclass

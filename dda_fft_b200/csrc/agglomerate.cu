@@ -1,0 +1,288 @@
+// Agglomerates of capsule monomers (the anthrax-like target, iGenerateAnthrax,
+// particle.cpp:21-85): monomer placement on the host, rasterisation into the lattice on the
+// GPU.
+//
+// Placement consumes the reference's random stream (xorshift64*, randomize.cpp:44-58) and
+// accepts or rejects monomers with the reference's float geometry (worm,
+// particle.cpp:302-344; CrossTwoWorms, 233-300; PointToWorm, 379-400), so it is written
+// with the same float operations in the same order: a realisation drawn here is the
+// reference's realisation.  Rasterisation -- every cell inside the sphere of radius n/2
+// tested against every monomer (SeedToWorm, particle.cpp:346-377) -- is the O(cells x
+// monomers) part (about a minute per sample at 128^3 on one core); it runs one thread per
+// cell with the monomers staged through shared memory, in explicitly rounded float
+// arithmetic (no fused multiply-add) so that boundary cells fall on the same side as in the
+// reference.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <vector>
+
+#include "agglomerate.h"
+
+namespace ddagpu {
+
+namespace {
+
+struct V3 {
+    float x, y, z;
+};
+
+// host float vector algebra of cvector.cpp (left-to-right evaluation, no contraction)
+inline V3 vsub(V3 a, V3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+inline V3 vadd(V3 a, V3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+inline V3 vscale(float r, V3 a) { return {r * a.x, r * a.y, r * a.z}; }
+inline float vdot(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+inline V3 vcross(V3 a, V3 b)
+{
+    return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+inline float vabs(V3 a) { return std::sqrt(a.x * a.x + a.y * a.y + a.z * a.z); }
+
+struct Worm {
+    float r, l;
+    V3 b, e, n;
+};
+
+int rng_draw(unsigned long long &s)
+{
+    s ^= s >> 12;
+    s ^= s << 25;
+    s ^= s >> 27;
+    return (int)((s * 2685821657736338717ULL) >> 33);
+}
+
+const double kPi = 3.1415926535897932384626433832795;   // PI of complex.hpp
+const float kRandMax = 2147483647.f;
+
+// worm(), particle.cpp:302-344
+Worm make_worm(float r1, float th1, float ph1, float r2, float th2, float ph2, float length,
+               float radius, float R2)
+{
+    const float ct1 = std::cos(th1), st1 = std::sin(th1), cp1 = std::cos(ph1), sp1 = std::sin(ph1);
+    V3 begin = {r1, ph1, th1}, end = {r2, ph2, th2};
+    const V3 dir0 = vsub(end, begin);
+    Worm w;
+    w.r = -1.f;
+    begin.x = r1 * st1 * cp1;
+    begin.y = r1 * st1 * sp1;
+    begin.z = r1 * ct1;
+    if (vdot(begin, begin) > R2) return w;
+    V3 v0;
+    v0.x = st1 * cp1 * dir0.x - sp1 * dir0.y + ct1 * cp1 * dir0.z;
+    v0.y = st1 * sp1 * dir0.x + cp1 * dir0.y + ct1 * sp1 * dir0.z;
+    v0.z = ct1 * dir0.x - st1 * dir0.z;
+    const float inv = (float)(1. / (double)vabs(v0));
+    const V3 dir = vscale(inv, v0);
+    end = vadd(begin, vscale(length, dir));
+    if (vdot(end, end) > R2) return w;
+    w.r = radius;
+    w.l = length;
+    w.b = begin;
+    w.e = end;
+    w.n = dir;
+    return w;
+}
+
+// PointToWorm, particle.cpp:379-400
+int point_to_worm(const Worm &w, V3 p, float radius)
+{
+    const float t = vdot(vsub(p, w.b), w.n), max_d = w.r + radius;
+    float d = vabs(vadd(vsub(w.b, p), vscale(t, w.n)));
+    if (d > max_d) return 0;
+    if (t >= 0.f && t <= w.l) return 1;
+    if (t < 0) {
+        d = vabs(vsub(w.b, p));
+        return d > max_d ? 0 : 1;
+    }
+    d = vabs(vsub(w.e, p));
+    return d > max_d ? 0 : 1;
+}
+
+// CrossTwoWorms, particle.cpp:233-300 (including its reuse of the nearest point)
+int cross_two_worms(const Worm &a, const Worm &b)
+{
+    const V3 v0 = vcross(a.n, b.n);
+    float r0 = vabs(v0);
+    if (r0 <= 1.e-20) return 1;
+    const V3 v1 = vsub(b.b, a.b);
+    const float d = std::fabs(vdot(v1, v0) / r0);
+    float r2 = a.r + b.r;
+    if (d > r2) return 0;
+    const float b1 = vdot(v1, a.n), b2 = vdot(v1, b.n);
+    const float a11 = 1.f, a12 = vdot(b.n, a.n), a21 = -a12, a22 = -a11;
+    r2 = a11 * a22 - a12 * a21;
+    r0 = (b1 * a22 - b2 * a12) / r2;
+    const float r1 = (b2 * a11 - b1 * a21) / r2;
+    if (r0 >= 0.f && r0 <= a.l && r1 >= 0.f && r1 <= b.l) return 1;
+    V3 near = {0.f, 0.f, 0.f};
+    int i0 = 0, i1 = 0;
+    if (r0 >= 0.f && r0 <= a.l) {
+        near = vadd(a.b, vscale(r0, a.n));
+        i0 = 1;
+    }
+    if (r1 >= 0.f && r1 <= b.l) {
+        near = vadd(b.b, vscale(r1, b.n));
+        i1 = 1;
+    }
+    if (point_to_worm(a, b.b, b.r) == 1) return 1;
+    if (point_to_worm(a, b.e, b.r) == 1) return 1;
+    if (point_to_worm(b, a.b, a.r) == 1) return 1;
+    if (point_to_worm(b, a.e, a.r) == 1) return 1;
+    if (i0 == 1 && point_to_worm(b, near, a.r) == 1) return 1;
+    if (i1 == 1 && point_to_worm(a, near, b.r) == 1) return 1;
+    return 0;
+}
+
+// ---- device rasterisation (SeedToWorm, particle.cpp:346-377)
+struct DW {
+    float r, l, bx, by, bz, ex, ey, ez, nx, ny, nz;
+};
+
+__device__ __forceinline__ float fm(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float fa(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float fs(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float dot3(float ax, float ay, float az, float bx, float by, float bz)
+{
+    return fa(fa(fm(ax, bx), fm(ay, by)), fm(az, bz));
+}
+
+__device__ bool seed_to_worm(const DW &w, float px, float py, float pz)
+{
+    const float t = dot3(fs(px, w.bx), fs(py, w.by), fs(pz, w.bz), w.nx, w.ny, w.nz);
+    const float rr = fm(w.r, w.r);
+    if (t >= 0.f && t <= w.l) {
+        const float vx = fa(fs(w.bx, px), fm(w.nx, t)), vy = fa(fs(w.by, py), fm(w.ny, t)),
+                    vz = fa(fs(w.bz, pz), fm(w.nz, t));
+        return dot3(vx, vy, vz, vx, vy, vz) <= rr;
+    }
+    if (t > -w.r && t < 0.f) {
+        const float vx = fs(w.bx, px), vy = fs(w.by, py), vz = fs(w.bz, pz);
+        return dot3(vx, vy, vz, vx, vy, vz) <= rr;
+    }
+    if (t > w.l && t < fa(w.l, w.r)) {
+        const float vx = fs(w.ex, px), vy = fs(w.ey, py), vz = fs(w.ez, pz);
+        return dot3(vx, vy, vz, vx, vy, vz) <= rr;
+    }
+    return false;
+}
+
+constexpr int kChunk = 256;
+
+__global__ void __launch_bounds__(256) rasterize(const DW *worms, int count, int ni, int nj, int nl,
+                                                 float cx, float cy, float cz, float R2,
+                                                 signed char *occ, int *ndip)
+{
+    __shared__ DW sw[kChunk];
+    __shared__ int block_hits;
+    const size_t N = (size_t)ni * nj * nl;
+    const size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (threadIdx.x == 0) block_hits = 0;
+    float px = 0.f, py = 0.f, pz = 0.f;
+    bool inside = false;
+    if (q < N) {
+        const int l = (int)(q % nl), j = (int)((q / nl) % nj), i = (int)(q / ((size_t)nl * nj));
+        px = fs((float)i, cx);
+        py = fs((float)j, cy);
+        pz = fs((float)l, cz);
+        inside = fa(fa(fm(px, px), fm(py, py)), fm(pz, pz)) <= R2;
+    }
+    bool hit = false;
+    for (int c0 = 0; c0 < count; c0 += kChunk) {
+        __syncthreads();
+        for (int k = threadIdx.x; k < kChunk && c0 + k < count; k += blockDim.x) sw[k] = worms[c0 + k];
+        __syncthreads();
+        const int m = count - c0 < kChunk ? count - c0 : kChunk;
+        if (inside && !hit)
+            for (int k = 0; k < m; k++)
+                if (seed_to_worm(sw[k], px, py, pz)) {
+                    hit = true;
+                    break;
+                }
+    }
+    if (q < N) occ[q] = hit ? 1 : 0;
+    if (hit) atomicAdd(&block_hits, 1);
+    __syncthreads();
+    if (threadIdx.x == 0 && block_hits) atomicAdd(ndip, block_hits);
+}
+
+}  // namespace
+
+long long anthrax_count(int ni, int nj, int nl, float packing, float radius, float ratio)
+{
+    // iWormsNumber, main.cpp:585
+    const double v = (double)(packing * (float)(ni * nj * nl)) /
+                     (8. * (double)(radius * radius * radius) * (0.75 * (double)ratio + 1));
+    return (long long)v + 1;
+}
+
+int anthrax_place(unsigned long long *state, int ni, float radius, float length, int count,
+                  float *cyl13, long long max_tries)
+{
+    // iGenerateAnthrax placement, particle.cpp:21-60
+    const float R = (float)((double)(float)ni / 2.), R2 = (R - radius) * (R - radius);
+    std::vector<Worm> w;
+    w.reserve((size_t)count);
+    unsigned long long s = *state;
+    long long tries = 0;
+    int l = 0;
+    while ((int)w.size() < count) {
+        Worm c;
+        c.r = -1.f;
+        while (c.r < 0.f) {
+            if (++tries > max_tries) return -1;
+            const float r1 = R * (float)rng_draw(s) / kRandMax;
+            const float r2 = r1;
+            const float ph1 = (float)(2. * kPi * (double)(float)rng_draw(s) / (double)kRandMax);
+            const float ph2 = (float)(2. * kPi * (double)(float)rng_draw(s) / (double)kRandMax);
+            float r0 = (float)(2. * (double)(float)rng_draw(s) / (double)kRandMax - 1.);
+            const float th1 = std::acos(r0);
+            r0 = (float)(2. * (double)(float)rng_draw(s) / (double)kRandMax - 1.);
+            const float th2 = std::acos(r0);
+            c = make_worm(r1, th1, ph1, r2, th2, ph2, length, radius, R2);
+        }
+        for (size_t j = 0; j < w.size(); j++) {
+            l = cross_two_worms(c, w[j]);
+            if (l == 1) break;
+        }
+        if (l == 0) w.push_back(c);
+    }
+    *state = s;
+    for (int k = 0; k < count; k++) {
+        float *o = cyl13 + 13 * (size_t)k;
+        const Worm &m = w[(size_t)k];
+        const float v[13] = {m.r, m.l, m.b.x, m.b.y, m.b.z, m.e.x, m.e.y, m.e.z, m.n.x, m.n.y, m.n.z, 0.f, 0.f};
+        for (int q = 0; q < 13; q++) o[q] = v[q];
+    }
+    return 0;
+}
+
+cudaError_t anthrax_rasterize(const float *cyl13, int count, int ni, int nj, int nl,
+                              signed char *occ_dev, int *ndip_dev, cudaStream_t st)
+{
+    // iGenerateAnthrax rasterisation, particle.cpp:62-83: centre n/2 - 0.5, radius n/2
+    std::vector<DW> h((size_t)count);
+    for (int k = 0; k < count; k++) {
+        const float *c = cyl13 + 13 * (size_t)k;
+        h[(size_t)k] = DW{c[0], c[1], c[2], c[3], c[4], c[5], c[6], c[7], c[8], c[9], c[10]};
+    }
+    DW *d = nullptr;
+    cudaError_t e = cudaMallocAsync(&d, (count ? count : 1) * sizeof(DW), st);
+    if (e) return e;
+    // pageable source: the copy has taken the host data when the call returns
+    if (count) e = cudaMemcpyAsync(d, h.data(), count * sizeof(DW), cudaMemcpyHostToDevice, st);
+    if (!e) e = cudaMemsetAsync(ndip_dev, 0, sizeof(int), st);
+    if (!e) {
+        const float R = (float)((double)(float)ni / 2.);
+        const float cx = (float)((double)(float)ni / 2. - .5),
+                    cy = (float)((double)(float)nj / 2. - .5),
+                    cz = (float)((double)(float)nl / 2. - .5);
+        const size_t N = (size_t)ni * nj * nl;
+        rasterize<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(d, count, ni, nj, nl, cx, cy, cz,
+                                                              R * R, occ_dev, ndip_dev);
+        e = cudaGetLastError();
+    }
+    cudaFreeAsync(d, st);
+    return e;
+}
+
+}  // namespace ddagpu

@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "../../include/ddagpu.h"
+#include "agglomerate.h"
 #include "internal.h"
 #include "post.h"
 #include "solver.h"
@@ -1169,6 +1170,56 @@ int ddagpu_mc_rotations(unsigned long long base_seed, int worker, int count, dou
         t[7] = -sps * cio;
         t[8] = cps;
     }
+    return DDAGPU_OK;
+}
+
+unsigned long long ddagpu_rng_seed(unsigned long long base_seed, int worker)
+{
+    const unsigned long long s = base_seed + 0x9E3779B97F4A7C15ULL * (unsigned long long)(worker + 1);
+    return s ? s : 0x9E3779B97F4A7C15ULL;   // dda_srand, randomize.cpp:44-48
+}
+
+long long ddagpu_anthrax_count(int i_max, int j_max, int l_max, float packing,
+                               float monomer_radius, float length_ratio)
+{
+    return anthrax_count(i_max, j_max, l_max, packing, monomer_radius, length_ratio);
+}
+
+int ddagpu_anthrax_place(unsigned long long *rng_state, int i_max, float monomer_radius,
+                         float monomer_length, int count, float *monomers)
+{
+    if (!rng_state || !monomers || count < 1 || i_max < 2 || !(monomer_radius > 0.f))
+        return fail(DDAGPU_EINVAL, "bad agglomerate arguments");
+    const long long max_tries = 2000000LL + 20000LL * count;
+    if (anthrax_place(rng_state, i_max, monomer_radius, monomer_length, count, monomers, max_tries))
+        return fail(DDAGPU_EINVAL, "monomer placement did not finish (packing too dense)");
+    return DDAGPU_OK;
+}
+
+int ddagpu_anthrax_rasterize(int device, int i_max, int j_max, int l_max, const float *monomers,
+                             int count, signed char *occ, int *ndip)
+{
+    if (!pow2_in(i_max) || !pow2_in(j_max) || !pow2_in(l_max))
+        return fail(DDAGPU_EINVAL, "lattice edges must be powers of two in [2, 128]");
+    if (!monomers || !occ || count < 0) return fail(DDAGPU_EINVAL, "null or bad argument");
+    DevGuard dg(device);
+    const size_t N = (size_t)i_max * j_max * l_max;
+    cudaStream_t st;
+    CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    signed char *d = nullptr;
+    int *nd = nullptr, h = 0;
+    cudaError_t e = cudaMallocAsync(&d, N, st);
+    if (e == cudaSuccess) e = cudaMallocAsync(&nd, sizeof(int), st);
+    if (e == cudaSuccess) e = anthrax_rasterize(monomers, count, i_max, j_max, l_max, d, nd, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(occ, d, N, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&h, nd, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (d) cudaFreeAsync(d, st);
+    if (nd) cudaFreeAsync(nd, st);
+    cudaError_t e2 = cudaStreamSynchronize(st);
+    cudaStreamDestroy(st);
+    CK(e);
+    CK(e2);
+    if (ndip) *ndip = h;
     return DDAGPU_OK;
 }
 

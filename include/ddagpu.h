@@ -175,6 +175,22 @@ int ddagpu_num_angles(float theta_min, float theta_max, float theta_step);
 /* Rotation matrices of the reference's Monte-Carlo orientation sampler: worker `worker` of
  * a run seeded base_seed (main.cpp:803-804, 876-898, randomize.cpp:44-58). */
 int ddagpu_mc_rotations(unsigned long long base_seed, int worker, int count, double *rot);
+/* Random stream of worker `worker` of a run seeded base_seed (main.cpp:803-804): the state
+ * to pass to ddagpu_anthrax_place; samples drawn one after another keep updating it. */
+unsigned long long ddagpu_rng_seed(unsigned long long base_seed, int worker);
+
+/* Agglomerates of capsule monomers (target 6, iGenerateAnthrax, particle.cpp:21-85).
+ * Monomer count as main.cpp:585-586; placement on the host with the reference's random
+ * stream and float geometry (monomers[count][13] = r, l, begin[3], end[3], axis[3], 0, 0;
+ * returns DDAGPU_EINVAL if the packing is too dense to place them); rasterisation of the
+ * monomers into the lattice on the GPU (occ host output, 1 = filled). */
+long long ddagpu_anthrax_count(int i_max, int j_max, int l_max, float packing,
+                               float monomer_radius, float length_ratio);
+int ddagpu_anthrax_place(unsigned long long *rng_state, int i_max, float monomer_radius,
+                         float monomer_length, int count, float *monomers);
+int ddagpu_anthrax_rasterize(int device, int i_max, int j_max, int l_max, const float *monomers,
+                             int count, signed char *occ, int *ndip);
+
 /* Fixed orientation (degrees), main.cpp:516-541. */
 int ddagpu_fixed_rotation(double psi, double iota, double kappa, double *rot);
 

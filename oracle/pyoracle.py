@@ -246,6 +246,7 @@ class RefLib:
         L.dref_fft_line.argtypes = [_i, _i, _p, _p]
         L.dref_gen_ellipsoid.argtypes = [_i, _i, _i, _d, _d, _p]
         L.dref_rng.argtypes = [C.c_ulonglong, _i, _p]
+        L.dref_gen_anthrax.argtypes = [C.c_ulonglong, _i, _i, _i, _d, _d, _i, _p, _p, _p]
         L.dref_run_samples.argtypes = [C.POINTER(RunCfg), _p, _i, _i, _i, _p, _p, _p, _p, _p]
 
     def green(self, ni, nj, nl, kd, fft_mode=0):
@@ -348,6 +349,15 @@ class RefLib:
         out = np.zeros(count, np.int32)
         self.lib.dref_rng(C.c_ulonglong(seed), count, _ptr(out))
         return out
+
+    def gen_anthrax(self, seed, n, radius, length, count):
+        """iGenerateAnthrax after dda_srand(seed): (occ, ndip, monomers[count][13], next draw)."""
+        occ = np.zeros((n, n, n), np.int8)
+        cyl = np.zeros((count, 13), self.rdt)
+        nxt = C.c_int(0)
+        nd = self.lib.dref_gen_anthrax(C.c_ulonglong(seed), n, n, n, radius, length, count,
+                                       _ptr(occ), _ptr(cyl), C.byref(nxt))
+        return occ, nd, cyl, nxt.value
 
     def run_samples(self, cfg: RunCfg, nsamples, nthreads=1, occ=None, verbose=0):
         """The reference's sample loop; returns (seconds, cabs_sum, cext_sum, mueller_sum)."""

@@ -414,6 +414,30 @@ int dref_gen_ellipsoid(int ni, int nj, int nl, double b_a, double c_a, signed ch
     return n;
 }
 
+/* iGenerateAnthrax (particle.cpp:21-85) after dda_srand(seed): occupancy, the monomers
+   (13 reals each: r, l, b[3], e[3], n[3]) and the next draw of the stream. */
+int dref_gen_anthrax(unsigned long long seed, int ni, int nj, int nl, double radius,
+                     double length, int count, signed char *occ, ioreal *cyl, int *next_draw)
+{
+    std::vector<char> occb((size_t)ni * nj * nl);
+    view3<char> vo(occb.data(), ni, nj, nl);
+    std::vector<cylinder> w((size_t)count);
+    dda_srand(seed);
+    int n = iGenerateAnthrax(ni, nj, nl, (real)radius, (real)length, count, w.data(), vo.get());
+    std::memcpy(occ, occb.data(), occb.size());
+    for (int k = 0; k < count; k++) {
+        ioreal *o = cyl + 13 * (size_t)k;
+        o[0] = w[(size_t)k].r;
+        o[1] = w[(size_t)k].l;
+        o[2] = w[(size_t)k].b.x; o[3] = w[(size_t)k].b.y; o[4] = w[(size_t)k].b.z;
+        o[5] = w[(size_t)k].e.x; o[6] = w[(size_t)k].e.y; o[7] = w[(size_t)k].e.z;
+        o[8] = w[(size_t)k].n.x; o[9] = w[(size_t)k].n.y; o[10] = w[(size_t)k].n.z;
+        o[11] = o[12] = 0;
+    }
+    if (next_draw) *next_draw = dda_rand();
+    return n;
+}
+
 /* count draws of the reference generator after dda_srand(seed) (randomize.cpp:44-58). */
 int dref_rng(unsigned long long seed, int count, int *out)
 {

@@ -6,6 +6,7 @@ oracle/ref_shim.cpp), its FP64 build (oracle/_ref/libddaref64.so) and its unmodi
 executable (oracle/_ref/dda_fft.out).  Run in a container that has the reference tree:
 
     make -f oracle/Makefile all && python tests/golden/make_golden.py
+    python tests/golden/make_golden.py agglomerates     # anthrax_v72.npz
 
 The fixtures are small (.npz, a few MB in all) and are committed; the tests read
 them without needing the reference.
@@ -170,7 +171,38 @@ def end_to_end(R, R64, out):
     out["ldr16_64"] = np.concatenate([[ca, ce], mm.ravel()])
 
 
+# (name, lattice edge, monomer radius, length ratio, packing, generator seed): the
+# agglomerate target of the realisation batch (radius 3, ratio 0, packing 0.25) and a
+# capsule case with a cylindrical part
+AGGLOMERATES = [("c3b32", 32, 3.0, 0.0, 0.25, 7), ("c3b64", 64, 3.0, 0.0, 0.25, 7),
+                ("caps64", 64, 2.0, 2.5, 0.3, 99), ("c3b128", 128, 3.0, 0.0, 0.25, 7)]
+
+
+def agglomerates(R, out):
+    """iGenerateAnthrax (particle.cpp:21-85) after dda_srand(seed), monomer count as
+    main.cpp:585-586: monomers, dipole count, the next draw of the stream, and the
+    occupancy (bit-packed; as a SHA-256 only for 128^3)."""
+    import hashlib
+    for name, n, r, lr, rho, seed in AGGLOMERATES:
+        count = int(rho * n ** 3 / (8.0 * r ** 3 * (0.75 * lr + 1))) + 1
+        occ, nd, cyl, nxt = R.gen_anthrax(seed, n, r, r * lr, count)
+        out[f"{name}_cfg"] = np.array([n, r, lr, rho, seed, count], np.float64)
+        out[f"{name}_monomers"] = cyl.astype(np.float32)
+        out[f"{name}_ndip_next"] = np.array([nd, nxt], np.int64)
+        if n <= 64:
+            out[f"{name}_occ_bits"] = np.packbits(occ.ravel() != 0)
+        out[f"{name}_occ_sha256"] = np.frombuffer(
+            hashlib.sha256((occ != 0).astype(np.uint8).tobytes()).digest(), np.uint8)
+
+
 def main():
+    if sys.argv[1:] == ["agglomerates"]:
+        out: dict = {}
+        agglomerates(RefLib(), out)
+        path = os.path.join(HERE, "anthrax_v72.npz")
+        np.savez_compressed(path, **out)
+        print(f"wrote {path}: {os.path.getsize(path) / 1e6:.2f} MB, {len(out)} arrays")
+        return
     R = RefLib()
     R64 = RefLib(REF64_SO)
     assert R.rdt == np.float32 and R64.rdt == np.float64
