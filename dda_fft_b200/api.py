@@ -91,6 +91,10 @@ def lib():
         L.ddagpu_mueller.argtypes = [_p, _p, _p, _p, _i, _i, _p, _p, _p, _p, _p]
         L.ddagpu_orientation_solves.argtypes = [_p, C.POINTER(_BatchCfg), _i, _p, _p, _p, _p,
                                                 C.POINTER(BatchInfo)]
+        L.ddagpu_realization_solves.argtypes = [_p, C.POINTER(_BatchCfg), _i, _p, _p, _p, _p, _p,
+                                                C.POINTER(BatchInfo)]
+        L.ddagpu_agglomerate_solves.argtypes = [_p, C.POINTER(_BatchCfg), _i, _p, _p, _p, _p, _p,
+                                                _p, _p, C.POINTER(BatchInfo)]
         L.ddagpu_num_angles.argtypes = [_f, _f, _f]
         L.ddagpu_mc_rotations.argtypes = [C.c_ulonglong, _i, _i, _p]
         L.ddagpu_fixed_rotation.argtypes = [_d, _d, _d, _p]
@@ -372,6 +376,49 @@ class Context:
                                                _ptr(cext), _ptr(mm), C.byref(info)))
         return dict(cabs=cabs, cext=cext, mueller=mm, n_rhs=info.n_rhs, max_steps=info.max_steps,
                     rolled_back=info.rolled_back, max_err=info.max_err)
+
+    def _cfg(self, cfg: BatchConfig, m):
+        return _BatchCfg(cfg.solver, cfg.tau, cfg.max_step, cfg.err_max, cfg.polarizability,
+                         len(cfg.materials), _ptr(m), None, cfg.nplanes, cfg.theta_min,
+                         cfg.theta_max, cfg.theta_step)
+
+    def realization_solves(self, cfg: BatchConfig, occ: np.ndarray, rot=None):
+        """Both polarisations of every realisation occ[k] (its own occupancy), batched on
+        the GPU; rot[k] (3x3) per realisation or None for the fixed orientation."""
+        occ = np.ascontiguousarray(occ, np.int8).reshape((-1,) + self.grid)
+        n = occ.shape[0]
+        r = None if rot is None else np.ascontiguousarray(rot, np.float64).reshape(n, 3, 3)
+        na = num_angles(cfg.theta_min, cfg.theta_max, cfg.theta_step)
+        m = np.ascontiguousarray(np.asarray(cfg.materials, np.float32).ravel())
+        c = self._cfg(cfg, m)
+        cabs, cext, mm = np.zeros(n), np.zeros(n), np.zeros((n, na, 4, 4))
+        info = BatchInfo()
+        _check(lib().ddagpu_realization_solves(self._h, C.byref(c), n, _ptr(occ),
+                                               None if r is None else _ptr(r), _ptr(cabs),
+                                               _ptr(cext), _ptr(mm), C.byref(info)))
+        return dict(cabs=cabs, cext=cext, mueller=mm, n_rhs=info.n_rhs, max_steps=info.max_steps,
+                    rolled_back=info.rolled_back, max_err=info.max_err)
+
+    def agglomerate_solves(self, cfg: BatchConfig, monomers, rot=None):
+        """Realisations given as monomer lists (Agglomerate.place), rasterised on the GPU
+        into the batch; cfg.materials must hold one material."""
+        counts = np.array([len(x) for x in monomers], np.int32)
+        n = len(counts)
+        flat = (np.ascontiguousarray(np.concatenate([np.asarray(x, np.float32).reshape(-1, 13)
+                                                     for x in monomers]), np.float32)
+                if counts.sum() else np.zeros((1, 13), np.float32))
+        r = None if rot is None else np.ascontiguousarray(rot, np.float64).reshape(n, 3, 3)
+        na = num_angles(cfg.theta_min, cfg.theta_max, cfg.theta_step)
+        m = np.ascontiguousarray(np.asarray(cfg.materials, np.float32).ravel())
+        c = self._cfg(cfg, m)
+        cabs, cext, mm = np.zeros(n), np.zeros(n), np.zeros((n, na, 4, 4))
+        ndip = np.zeros(n, np.int32)
+        info = BatchInfo()
+        _check(lib().ddagpu_agglomerate_solves(self._h, C.byref(c), n, _ptr(flat), _ptr(counts),
+                                               None if r is None else _ptr(r), _ptr(cabs),
+                                               _ptr(cext), _ptr(mm), _ptr(ndip), C.byref(info)))
+        return dict(cabs=cabs, cext=cext, mueller=mm, ndip=ndip, n_rhs=info.n_rhs,
+                    max_steps=info.max_steps, rolled_back=info.rolled_back, max_err=info.max_err)
 
     # ------------------------------------------------------------ device-resident
     def convolution_dev(self, p_dev, out_dev, nrhs: int = 1, conj: bool = False) -> None:

@@ -90,6 +90,9 @@ struct ddagpu_ctx {
     float2 *b32 = nullptr, *rb = nullptr;   // refinement: outer and inner right-hand sides
     double2 *x64 = nullptr;                 // refinement: FP64 solution
     bool occ_valid = false;      // occupancy of the last batched call is resident
+    signed char *occ_b = nullptr;   // [cap][N] per-right-hand-side occupancy (realisations)
+    int *ndip = nullptr;            // [cap] dipoles of each rasterised realisation
+    size_t occ_stride = 0;          // N while occ_b is in use, 0 otherwise
     int occ_nmat1 = 0, occ_nact = 0;
     long long launches = 0;      // kernels launched by this context
     std::mutex mu;
@@ -165,7 +168,8 @@ MatvecArgs mv_args(ddagpu_ctx *c, int nrhs, const float2 *src, float2 *out, int 
     a.ep.conj = conj;
     a.ep.sv = sv;
     a.ep.v = v;
-    a.ep.occ = c->occ;
+    a.ep.occ = c->occ_stride ? c->occ_b : c->occ;
+    a.ep.occ_stride = c->occ_stride;
     a.ep.alpha = c->alpha;
     a.ep.mv = c->mv;
     a.ep.nmat1 = nmat1;
@@ -184,7 +188,8 @@ FieldArgs fa_args(ddagpu_ctx *c, int nrhs, int nmat1, double d0, float tau)
     f.ni = c->ni;
     f.nj = c->nj;
     f.nl = c->nl;
-    f.occ = c->occ;
+    f.occ = c->occ_stride ? c->occ_b : c->occ;
+    f.occ_stride = c->occ_stride;
     f.mv = c->mv;
     f.alpha = c->alpha;
     f.nmat1 = nmat1;
@@ -218,7 +223,7 @@ struct SolveResult {
 // already on the device.  Leaves the final (or rolled-back) dipoles in c->p.
 int run_solver(ddagpu_ctx *c, int nrhs, int solver, float tau, int max_step, float err_max,
                int nmat1, double d0, int nact, SolveResult &res, bool want_trace,
-               const float2 *rhs_in = nullptr)
+               const float2 *rhs_in = nullptr, const int *nact_per = nullptr)
 {
     if (solver < 0 || solver > 3) return fail(DDAGPU_EINVAL, "solver must be 0..3");
     if (max_step < 0) return fail(DDAGPU_EINVAL, "Max_Step must be >= 0");
@@ -234,11 +239,12 @@ int run_solver(ddagpu_ctx *c, int nrhs, int solver, float tau, int max_step, flo
     double *trace = want_trace ? c->trace : nullptr;
     const int tlen = want_trace ? tl : 0;
     std::vector<RhsState> init((size_t)nrhs);
-    for (auto &S : init) {
+    for (int k = 0; k < nrhs; k++) {
+        RhsState &S = init[(size_t)k];
         std::memset(&S, 0, sizeof S);
         S.err_max = (double)err_max;
         S.active = 1;
-        S.nact = nact;
+        S.nact = nact_per ? nact_per[k] : nact;
     }
     CK(cudaMemcpyAsync(c->state, init.data(), nrhs * sizeof(RhsState), cudaMemcpyHostToDevice, st));
     std::vector<int> ones((size_t)nrhs, 1);
@@ -536,7 +542,8 @@ int ddagpu_destroy(ddagpu_ctx *c)
     void *ptrs[] = {c->ahat, c->tw,     c->work,   c->p,       c->pmin,   c->r,     c->s,
                     c->w,    c->g,      c->h,      c->state,   c->active, c->trace, c->occ,
                     c->mv,   c->alpha,  c->kinc,   c->einc,    c->ksc,    c->esc_acc,
-                    c->cc_acc, c->normals, c->mueller, c->esc, c->cabs,   c->cext};
+                    c->cc_acc, c->normals, c->mueller, c->esc, c->cabs,   c->cext,
+                    c->occ_b, c->ndip};
     for (void *q : ptrs)
         if (q) cudaFree(q);
     if (c->st) cudaStreamDestroy(c->st);
@@ -717,7 +724,8 @@ int run_post(ddagpu_ctx *c, int nrhs, int nmat1, double d0, int ndir)
     pa.ni = c->ni;
     pa.nj = c->nj;
     pa.nl = c->nl;
-    pa.occ = c->occ;
+    pa.occ = c->occ_stride ? c->occ_b : c->occ;
+    pa.occ_stride = c->occ_stride;
     pa.mv = c->mv;
     pa.alpha = c->alpha;
     pa.nmat1 = nmat1;
@@ -731,6 +739,154 @@ int run_post(ddagpu_ctx *c, int nrhs, int nmat1, double d0, int ndir)
     pa.cc_acc = c->cc_acc;
     CK(launch_post(pa, c->esc, c->cabs, c->cext, c->st));
     c->launches += ndir > 0 ? 3 : 2;
+    return DDAGPU_OK;
+}
+
+// ---- batched solves: shared set-up and one chunk of up to cap / 2 orientations
+struct BatchGeom {
+    int nA = 0, nP = 0, ndir = 0, nmat1 = 0;
+    std::vector<int> mv;
+    std::vector<double> ksc0, nrm0;   // scattering directions and plane normals before rotation
+};
+
+int batch_check(ddagpu_ctx *c, const ddagpu_batch_cfg *cfg)
+{
+    if (c->cap < 2) return fail(DDAGPU_EINVAL, "the context needs max_rhs >= 2");
+    if (cfg->n_mat < 1 || !cfg->m || cfg->nplanes < 1 || !(cfg->theta_step > 0.f))
+        return fail(DDAGPU_EINVAL, "bad batch configuration");
+    if (cfg->n_mat + 1 > c->nmat_cap) return fail(DDAGPU_EINVAL, "n_mat outside 0..254");
+    if (cfg->polarizability < 1 || cfg->polarizability > 5)
+        return fail(DDAGPU_EINVAL, "polarizability must be 1..5");
+    return DDAGPU_OK;
+}
+
+int batch_setup(ddagpu_ctx *c, const ddagpu_batch_cfg *cfg, BatchGeom &g)
+{
+    g.nA = ddagpu_num_angles(cfg->theta_min, cfg->theta_max, cfg->theta_step);
+    g.nP = cfg->nplanes;
+    g.ndir = g.nA * g.nP;
+    g.nmat1 = cfg->n_mat + 1;
+    if (g.nA < 1) return fail(DDAGPU_EINVAL, "no scattering angles");
+    RET(ensure_post(c, g.ndir, g.nP, g.nA));
+    // material activity (main.cpp:610-613)
+    g.mv.assign((size_t)g.nmat1, 0);
+    for (int k = 0; k < cfg->n_mat; k++)
+        g.mv[(size_t)k + 1] = (cfg->m[2 * k] == 1.f && cfg->m[2 * k + 1] == 0.f) ? 0 : 1;
+    // scattering geometry before rotation (main.cpp:336-387)
+    const double pi = 3.14159265358979323846264338327950288;
+    g.ksc0.assign((size_t)g.ndir * 3, 0.0);
+    g.nrm0.assign((size_t)g.nP * 3, 0.0);
+    for (int pl = 0; pl < g.nP; pl++) {
+        const double ang = pl * (180.0 / g.nP) * pi / 180.0, cs = std::cos(ang), sn = std::sin(ang);
+        g.nrm0[3 * pl + 0] = sn;
+        g.nrm0[3 * pl + 1] = cs;
+        g.nrm0[3 * pl + 2] = 0.0;
+        for (int a = 0; a < g.nA; a++) {
+            const double th = ((double)cfg->theta_min + (double)cfg->theta_step * a) * pi / 180.0;
+            const double k0[3] = {std::sin(th), 0.0, std::cos(th)};
+            double *k = g.ksc0.data() + 3 * ((size_t)pl * g.nA + a);
+            k[0] = cs * k0[0] + sn * k0[1];
+            k[1] = -sn * k0[0] + cs * k0[1];
+            k[2] = k0[2];
+        }
+    }
+    return DDAGPU_OK;
+}
+
+// rot[o0 .. o0 + no) or, without rotations, the fixed orientation psi = iota = kappa = 0
+void batch_rotations(const double *rot, int o0, int no, std::vector<double> &out)
+{
+    out.assign((size_t)9 * no, 0.0);
+    for (int o = 0; o < no; o++)
+        for (int q = 0; q < 9; q++)
+            out[(size_t)9 * o + q] = rot ? rot[9 * ((size_t)o0 + o) + q] : (q % 4 == 0 ? 1.0 : 0.0);
+}
+
+int ensure_occ_batch(ddagpu_ctx *c)
+{
+    if (!c->occ_b) CK(dalloc(&c->occ_b, (size_t)c->cap * c->N));
+    if (!c->ndip) CK(dalloc(&c->ndip, (size_t)c->cap));
+    return DDAGPU_OK;
+}
+
+// Per-right-hand-side occupancy (c->occ_b) for the lifetime of the guard.
+struct OccBatch {
+    ddagpu_ctx *c;
+    explicit OccBatch(ddagpu_ctx *cc) : c(cc) { c->occ_stride = c->N; }
+    ~OccBatch() { c->occ_stride = 0; }
+};
+
+// Solves no orientations (rotation matrices rot[no][9]) as 2 no right-hand sides -- both
+// incident polarisations, x and y before rotation (main.cpp:153-154) -- whose occupancy is
+// on the device, then far fields, cross sections and the Mueller matrices averaged over the
+// planes (main.cpp:870-949).  cabs / cext / mueller point at this chunk's first orientation.
+int batch_chunk(ddagpu_ctx *c, const ddagpu_batch_cfg *cfg, const BatchGeom &g, const double *rot,
+                int no, int nact, const int *nact_per, double *cabs, double *cext, double *mueller,
+                ddagpu_batch_info &bi)
+{
+    const int nr = 2 * no, ndir = g.ndir, nP = g.nP, nA = g.nA, nmat1 = g.nmat1;
+    const double d0 = c->kd;
+    std::vector<double> kin((size_t)nr * 3, 0.0), ein((size_t)nr * 6, 0.0),
+        ks((size_t)nr * ndir * 3, 0.0), nv((size_t)no * nP * 3, 0.0);
+    std::vector<float2> al((size_t)nr * nmat1, make_float2(0.f, 0.f));
+    for (int o = 0; o < no; o++) {
+        const double *T = rot + 9 * (size_t)o;
+        auto R = [&](const double *v, double *out) {
+            for (int i = 0; i < 3; i++) out[i] = T[3 * i] * v[0] + T[3 * i + 1] * v[1] + T[3 * i + 2] * v[2];
+        };
+        const double kz[3] = {0, 0, 1}, ex[3] = {1, 0, 0}, ey[3] = {0, 1, 0};
+        double k[3], e0[3], e1[3];
+        R(kz, k);
+        R(ex, e0);
+        R(ey, e1);
+        for (int q = 0; q < 2; q++) {
+            const int rr = 2 * o + q;
+            const double *e = q ? e1 : e0;
+            for (int i = 0; i < 3; i++) {
+                kin[3 * rr + i] = k[i];
+                ein[6 * rr + 2 * i] = e[i];
+                ein[6 * rr + 2 * i + 1] = 0.0;
+            }
+            for (int dd = 0; dd < ndir; dd++)
+                R(g.ksc0.data() + 3 * dd, ks.data() + ((size_t)rr * ndir + dd) * 3);
+            for (int mm = 0; mm < cfg->n_mat; mm++) {
+                const cd a = polarizability(cfg->polarizability, d0, {cfg->m[2 * mm], cfg->m[2 * mm + 1]},
+                                            kin.data() + 3 * rr, ein.data() + 6 * rr);
+                al[(size_t)rr * nmat1 + mm + 1] = make_float2((float)a.r, (float)a.i);
+            }
+        }
+        for (int pl = 0; pl < nP; pl++) R(g.nrm0.data() + 3 * pl, nv.data() + ((size_t)o * nP + pl) * 3);
+    }
+    CK(cudaMemcpyAsync(c->kinc, kin.data(), kin.size() * sizeof(double), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->einc, ein.data(), ein.size() * sizeof(double), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->ksc, ks.data(), ks.size() * sizeof(double), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->normals, nv.data(), nv.size() * sizeof(double), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->alpha, al.data(), al.size() * sizeof(float2), cudaMemcpyHostToDevice, c->st));
+    SolveResult res;
+    RET(run_solver(c, nr, cfg->solver, cfg->tau, cfg->max_step, cfg->err_max, nmat1, d0, nact, res,
+                   false, nullptr, nact_per));
+    RET(run_post(c, nr, nmat1, d0, ndir));
+    MuellerArgs m{no, nP, nA, ndir, c->kinc, c->einc, c->ksc, c->normals, c->esc, c->mueller};
+    CK(launch_mueller(m, c->st));
+    c->launches += 1;
+    std::vector<float> ca((size_t)nr), ce((size_t)nr);
+    std::vector<double> mo((size_t)no * nA * 16);
+    CK(cudaMemcpyAsync(ca.data(), c->cabs, nr * sizeof(float), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaMemcpyAsync(ce.data(), c->cext, nr * sizeof(float), cudaMemcpyDeviceToHost, c->st));
+    if (mueller)
+        CK(cudaMemcpyAsync(mo.data(), c->mueller, mo.size() * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    for (int o = 0; o < no; o++) {
+        if (cabs) cabs[o] = 0.5 * ca[(size_t)2 * o] + 0.5 * ca[(size_t)2 * o + 1];
+        if (cext) cext[o] = 0.5 * ce[(size_t)2 * o] + 0.5 * ce[(size_t)2 * o + 1];
+    }
+    if (mueller) std::memcpy(mueller, mo.data(), mo.size() * sizeof(double));
+    bi.n_rhs += nr;
+    for (const RhsState &S : res.st) {
+        bi.max_steps = std::max(bi.max_steps, S.steps);
+        bi.rolled_back += S.restored;
+        bi.max_err = std::max(bi.max_err, S.restored ? S.err_min : S.err);
+    }
     return DDAGPU_OK;
 }
 
@@ -1251,124 +1407,127 @@ int ddagpu_orientation_solves(ddagpu_ctx *c, const ddagpu_batch_cfg *cfg, int n_
                               ddagpu_batch_info *info)
 {
     if (!c || !cfg || !rot || n_orient < 0) return fail(DDAGPU_EINVAL, "null or bad argument");
-    if (c->cap < 2) return fail(DDAGPU_EINVAL, "the context needs max_rhs >= 2");
-    if (cfg->n_mat < 1 || !cfg->m || cfg->nplanes < 1 || !(cfg->theta_step > 0.f))
-        return fail(DDAGPU_EINVAL, "bad batch configuration");
-    if (cfg->polarizability < 1 || cfg->polarizability > 5)
-        return fail(DDAGPU_EINVAL, "polarizability must be 1..5");
+    RET(batch_check(c, cfg));
     std::lock_guard<std::mutex> lk(c->mu);
     DevGuard dg(c->dev);
-    const int nA = ddagpu_num_angles(cfg->theta_min, cfg->theta_max, cfg->theta_step);
-    const int nP = cfg->nplanes, ndir = nA * nP, nmat1 = cfg->n_mat + 1;
-    if (nA < 1) return fail(DDAGPU_EINVAL, "no scattering angles");
-    RET(ensure_post(c, ndir, nP, nA));
-    // material activity (main.cpp:610-613) and occupancy, shared by every orientation
-    std::vector<int> mv((size_t)nmat1, 0);
-    for (int k = 0; k < cfg->n_mat; k++)
-        mv[(size_t)k + 1] = (cfg->m[2 * k] == 1.f && cfg->m[2 * k + 1] == 0.f) ? 0 : 1;
+    BatchGeom g;
+    RET(batch_setup(c, cfg, g));
+    // occupancy shared by every orientation
     int nact = 0;
     if (cfg->occ) {
-        RET(upload_materials(c, mv.data(), nmat1, cfg->occ));
-        nact = count_active(cfg->occ, c->N, mv.data(), nmat1);
+        RET(upload_materials(c, g.mv.data(), g.nmat1, cfg->occ));
+        nact = count_active(cfg->occ, c->N, g.mv.data(), g.nmat1);
         c->occ_valid = true;
-        c->occ_nmat1 = nmat1;
+        c->occ_nmat1 = g.nmat1;
         c->occ_nact = nact;
     } else {
         // occupancy of the previous batched call, still on the device
-        if (!c->occ_valid || c->occ_nmat1 != nmat1)
+        if (!c->occ_valid || c->occ_nmat1 != g.nmat1)
             return fail(DDAGPU_EINVAL, "cfg->occ is null and no occupancy is resident");
-        CK(cudaMemcpyAsync(c->mv, mv.data(), nmat1 * sizeof(int), cudaMemcpyHostToDevice, c->st));
+        CK(cudaMemcpyAsync(c->mv, g.mv.data(), g.nmat1 * sizeof(int), cudaMemcpyHostToDevice, c->st));
         nact = c->occ_nact;
     }
     if (nact == 0) return fail(DDAGPU_EINVAL, "no active dipoles");
-    const double d0 = c->kd;
-    // scattering geometry before rotation (main.cpp:336-387)
-    const double pi = 3.14159265358979323846264338327950288;
-    std::vector<double> ksc0((size_t)ndir * 3), nrm0((size_t)nP * 3);
-    for (int pl = 0; pl < nP; pl++) {
-        const double ang = pl * (180.0 / nP) * pi / 180.0, cs = std::cos(ang), sn = std::sin(ang);
-        nrm0[3 * pl + 0] = sn;
-        nrm0[3 * pl + 1] = cs;
-        nrm0[3 * pl + 2] = 0.0;
-        for (int a = 0; a < nA; a++) {
-            const double th = ((double)cfg->theta_min + (double)cfg->theta_step * a) * pi / 180.0;
-            const double k0[3] = {std::sin(th), 0.0, std::cos(th)};
-            double *k = ksc0.data() + 3 * ((size_t)pl * nA + a);
-            k[0] = cs * k0[0] + sn * k0[1];
-            k[1] = -sn * k0[0] + cs * k0[1];
-            k[2] = k0[2];
-        }
-    }
     const int per = c->cap / 2;
     ddagpu_batch_info bi{0, 0, 0, 0.0};
-    std::vector<double> kin, ein, ks, nv;
-    std::vector<float2> al;
-    std::vector<float> ca, ce;
-    std::vector<double> mo;
     for (int o0 = 0; o0 < n_orient; o0 += per) {
-        const int no = std::min(per, n_orient - o0), nr = 2 * no;
-        kin.assign((size_t)nr * 3, 0.0);
-        ein.assign((size_t)nr * 6, 0.0);
-        ks.assign((size_t)nr * ndir * 3, 0.0);
-        nv.assign((size_t)no * nP * 3, 0.0);
-        al.assign((size_t)nr * nmat1, make_float2(0.f, 0.f));
-        for (int o = 0; o < no; o++) {
-            const double *T = rot + 9 * (size_t)(o0 + o);
-            auto R = [&](const double *v, double *out) {
-                for (int i = 0; i < 3; i++) out[i] = T[3 * i] * v[0] + T[3 * i + 1] * v[1] + T[3 * i + 2] * v[2];
-            };
-            const double kz[3] = {0, 0, 1}, ex[3] = {1, 0, 0}, ey[3] = {0, 1, 0};
-            double k[3], e0[3], e1[3];
-            R(kz, k);
-            R(ex, e0);
-            R(ey, e1);
-            for (int q = 0; q < 2; q++) {
-                const int rr = 2 * o + q;
-                const double *e = q ? e1 : e0;
-                for (int i = 0; i < 3; i++) {
-                    kin[3 * rr + i] = k[i];
-                    ein[6 * rr + 2 * i] = e[i];
-                    ein[6 * rr + 2 * i + 1] = 0.0;
-                }
-                for (int d = 0; d < ndir; d++) R(ksc0.data() + 3 * d, ks.data() + ((size_t)rr * ndir + d) * 3);
-                for (int mm = 0; mm < cfg->n_mat; mm++) {
-                    const cd a = polarizability(cfg->polarizability, d0, {cfg->m[2 * mm], cfg->m[2 * mm + 1]},
-                                                kin.data() + 3 * rr, ein.data() + 6 * rr);
-                    al[(size_t)rr * nmat1 + mm + 1] = make_float2((float)a.r, (float)a.i);
-                }
-            }
-            for (int pl = 0; pl < nP; pl++) R(nrm0.data() + 3 * pl, nv.data() + ((size_t)o * nP + pl) * 3);
+        const int no = std::min(per, n_orient - o0);
+        RET(batch_chunk(c, cfg, g, rot + 9 * (size_t)o0, no, nact, nullptr, cabs ? cabs + o0 : nullptr,
+                        cext ? cext + o0 : nullptr,
+                        mueller ? mueller + (size_t)o0 * g.nA * 16 : nullptr, bi));
+    }
+    if (info) *info = bi;
+    return DDAGPU_OK;
+}
+
+int ddagpu_realization_solves(ddagpu_ctx *c, const ddagpu_batch_cfg *cfg, int n_real,
+                              const signed char *occ, const double *rot, double *cabs,
+                              double *cext, double *mueller, ddagpu_batch_info *info)
+{
+    if (!c || !cfg || !occ || n_real < 0) return fail(DDAGPU_EINVAL, "null or bad argument");
+    RET(batch_check(c, cfg));
+    std::lock_guard<std::mutex> lk(c->mu);
+    DevGuard dg(c->dev);
+    BatchGeom g;
+    RET(batch_setup(c, cfg, g));
+    RET(ensure_occ_batch(c));
+    const size_t N = c->N;
+    for (int k = 0; k < n_real; k++) RET(check_occ(occ + (size_t)k * N, N, g.nmat1));
+    CK(cudaMemcpyAsync(c->mv, g.mv.data(), g.nmat1 * sizeof(int), cudaMemcpyHostToDevice, c->st));
+    const int per = c->cap / 2;
+    ddagpu_batch_info bi{0, 0, 0, 0.0};
+    std::vector<int> nact;
+    std::vector<double> rots;
+    for (int o0 = 0; o0 < n_real; o0 += per) {
+        const int no = std::min(per, n_real - o0);
+        nact.assign((size_t)2 * no, 0);
+        for (int k = 0; k < no; k++) {
+            const signed char *src = occ + (size_t)(o0 + k) * N;
+            nact[2 * k] = nact[2 * k + 1] = count_active(src, N, g.mv.data(), g.nmat1);
+            if (nact[2 * k] == 0) return fail(DDAGPU_EINVAL, "a realisation has no active dipoles");
+            CK(cudaMemcpyAsync(c->occ_b + 2 * k * N, src, N, cudaMemcpyHostToDevice, c->st));
+            CK(cudaMemcpyAsync(c->occ_b + (2 * k + 1) * N, c->occ_b + 2 * k * N, N,
+                               cudaMemcpyDeviceToDevice, c->st));
         }
-        CK(cudaMemcpyAsync(c->kinc, kin.data(), kin.size() * sizeof(double), cudaMemcpyHostToDevice, c->st));
-        CK(cudaMemcpyAsync(c->einc, ein.data(), ein.size() * sizeof(double), cudaMemcpyHostToDevice, c->st));
-        CK(cudaMemcpyAsync(c->ksc, ks.data(), ks.size() * sizeof(double), cudaMemcpyHostToDevice, c->st));
-        CK(cudaMemcpyAsync(c->normals, nv.data(), nv.size() * sizeof(double), cudaMemcpyHostToDevice, c->st));
-        CK(cudaMemcpyAsync(c->alpha, al.data(), al.size() * sizeof(float2), cudaMemcpyHostToDevice, c->st));
-        SolveResult res;
-        RET(run_solver(c, nr, cfg->solver, cfg->tau, cfg->max_step, cfg->err_max, nmat1, d0, nact, res, false));
-        RET(run_post(c, nr, nmat1, d0, ndir));
-        MuellerArgs m{no, nP, nA, ndir, c->kinc, c->einc, c->ksc, c->normals, c->esc, c->mueller};
-        CK(launch_mueller(m, c->st));
-        c->launches += 1;
-        ca.resize((size_t)nr);
-        ce.resize((size_t)nr);
-        mo.resize((size_t)no * nA * 16);
-        CK(cudaMemcpyAsync(ca.data(), c->cabs, nr * sizeof(float), cudaMemcpyDeviceToHost, c->st));
-        CK(cudaMemcpyAsync(ce.data(), c->cext, nr * sizeof(float), cudaMemcpyDeviceToHost, c->st));
-        if (mueller)
-            CK(cudaMemcpyAsync(mo.data(), c->mueller, mo.size() * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+        batch_rotations(rot, o0, no, rots);
+        OccBatch ob(c);
+        RET(batch_chunk(c, cfg, g, rots.data(), no, 0, nact.data(), cabs ? cabs + o0 : nullptr,
+                        cext ? cext + o0 : nullptr,
+                        mueller ? mueller + (size_t)o0 * g.nA * 16 : nullptr, bi));
+    }
+    if (info) *info = bi;
+    return DDAGPU_OK;
+}
+
+int ddagpu_agglomerate_solves(ddagpu_ctx *c, const ddagpu_batch_cfg *cfg, int n_real,
+                              const float *monomers, const int *counts, const double *rot,
+                              double *cabs, double *cext, double *mueller, int *ndip,
+                              ddagpu_batch_info *info)
+{
+    if (!c || !cfg || !counts || n_real < 0) return fail(DDAGPU_EINVAL, "null or bad argument");
+    RET(batch_check(c, cfg));
+    if (cfg->n_mat != 1) return fail(DDAGPU_EINVAL, "agglomerates are one material (n_mat = 1)");
+    std::vector<size_t> first((size_t)n_real + 1, 0);
+    for (int k = 0; k < n_real; k++) {
+        if (counts[k] < 0) return fail(DDAGPU_EINVAL, "negative monomer count");
+        first[(size_t)k + 1] = first[(size_t)k] + (size_t)counts[k];
+    }
+    if (first[(size_t)n_real] && !monomers) return fail(DDAGPU_EINVAL, "null monomers");
+    std::lock_guard<std::mutex> lk(c->mu);
+    DevGuard dg(c->dev);
+    BatchGeom g;
+    RET(batch_setup(c, cfg, g));
+    RET(ensure_occ_batch(c));
+    const size_t N = c->N;
+    CK(cudaMemcpyAsync(c->mv, g.mv.data(), g.nmat1 * sizeof(int), cudaMemcpyHostToDevice, c->st));
+    const int per = c->cap / 2;
+    ddagpu_batch_info bi{0, 0, 0, 0.0};
+    std::vector<int> nact, nd;
+    std::vector<double> rots;
+    for (int o0 = 0; o0 < n_real; o0 += per) {
+        const int no = std::min(per, n_real - o0);
+        for (int k = 0; k < no; k++) {
+            const int r = o0 + k;
+            CK(anthrax_rasterize(monomers + 13 * first[(size_t)r], counts[r], c->ni, c->nj, c->nl,
+                                 c->occ_b + 2 * k * N, c->ndip + k, c->st));
+            CK(cudaMemcpyAsync(c->occ_b + (2 * k + 1) * N, c->occ_b + 2 * k * N, N,
+                               cudaMemcpyDeviceToDevice, c->st));
+            c->launches += 1;
+        }
+        nd.assign((size_t)no, 0);
+        CK(cudaMemcpyAsync(nd.data(), c->ndip, no * sizeof(int), cudaMemcpyDeviceToHost, c->st));
         CK(cudaStreamSynchronize(c->st));
-        for (int o = 0; o < no; o++) {
-            if (cabs) cabs[o0 + o] = 0.5 * ca[2 * o] + 0.5 * ca[2 * o + 1];
-            if (cext) cext[o0 + o] = 0.5 * ce[2 * o] + 0.5 * ce[2 * o + 1];
+        nact.assign((size_t)2 * no, 0);
+        for (int k = 0; k < no; k++) {
+            if (ndip) ndip[o0 + k] = nd[(size_t)k];
+            nact[2 * k] = nact[2 * k + 1] = g.mv[1] ? nd[(size_t)k] : 0;
+            if (nact[2 * k] == 0) return fail(DDAGPU_EINVAL, "a realisation has no active dipoles");
         }
-        if (mueller) std::memcpy(mueller + (size_t)o0 * nA * 16, mo.data(), mo.size() * sizeof(double));
-        bi.n_rhs += nr;
-        for (const RhsState &S : res.st) {
-            bi.max_steps = std::max(bi.max_steps, S.steps);
-            bi.rolled_back += S.restored;
-            bi.max_err = std::max(bi.max_err, S.restored ? S.err_min : S.err);
-        }
+        batch_rotations(rot, o0, no, rots);
+        OccBatch ob(c);
+        RET(batch_chunk(c, cfg, g, rots.data(), no, 0, nact.data(), cabs ? cabs + o0 : nullptr,
+                        cext ? cext + o0 : nullptr,
+                        mueller ? mueller + (size_t)o0 * g.nA * 16 : nullptr, bi));
     }
     if (info) *info = bi;
     return DDAGPU_OK;

@@ -46,7 +46,8 @@ struct Epilogue {
     int conj;               // use conj(alpha)
     float sv;               // scale of v
     const float2 *v;        // field v, same layout as out (may be null if sv == 0)
-    const signed char *occ; // [N] material per cell
+    const signed char *occ; // [N] material per cell (per right-hand side if occ_stride)
+    size_t occ_stride;      // bytes between the occupancies of consecutive right-hand sides
     const float2 *alpha;    // [nrhs][nmat1] polarisability per material
     const int *mv;          // [nmat1] active material flags
     int nmat1;              // materials including index 0

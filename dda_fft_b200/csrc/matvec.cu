@@ -182,7 +182,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(512) k3_inverse_zy(M
         const size_t o = obase + (size_t)j * nl + l;
         float2 res = conv;
         if (ep.mode == 1) {
-            const int m = ep.occ[(size_t)i * nj * nl + (size_t)j * nl + l];
+            const int m = ep.occ[(size_t)rhs * ep.occ_stride + (size_t)i * nj * nl + (size_t)j * nl + l];
             if (!ep.mv[m]) {
                 res = czero();
             } else {

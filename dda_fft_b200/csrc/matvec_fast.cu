@@ -455,7 +455,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(NT) k3f(MatvecArgs a
         const size_t o = obase + (size_t)j * NL + l;
         float2 res = conv;
         if (ep.mode == 1) {
-            const int m = ep.occ[(size_t)i * NJ * NL + (size_t)j * NL + l];
+            const int m = ep.occ[(size_t)rhs * ep.occ_stride + (size_t)i * NJ * NL + (size_t)j * NL + l];
             if (!ep.mv[m]) {
                 res = czero();
             } else {

@@ -51,7 +51,7 @@ __global__ void __launch_bounds__(256) farfield_sum(PostArgs a)
     }
     const size_t N = a.N;
     const float2 *p = a.p + (size_t)rhs * 3 * N + (size_t)i * nj * nl;
-    const signed char *occ = a.occ + (size_t)i * nj * nl;
+    const signed char *occ = a.occ + (size_t)rhs * a.occ_stride + (size_t)i * nj * nl;
     float2 acc0 = czero(), acc1 = czero(), acc2 = czero();
     for (int j0 = 0; j0 < nj; j0 += FF_ROWS) {
         const int rows = nj - j0 < FF_ROWS ? nj - j0 : FF_ROWS;
@@ -113,10 +113,11 @@ __global__ void __launch_bounds__(256) cabs_cext_sum(PostArgs a)
     const size_t N = a.N;
     const float2 *p = a.p + (size_t)rhs * 3 * N;
     const float2 *al = a.alpha + (size_t)rhs * a.nmat1;
+    const signed char *occ = a.occ + (size_t)rhs * a.occ_stride;
     double v[2] = {0.0, 0.0};
     for (int e = threadIdx.x; e < nj * nl; e += blockDim.x) {
         const size_t q = (size_t)i * nj * nl + e;
-        const int m = a.occ[q];
+        const int m = occ[q];
         const float2 alpha = al[m];
         if (alpha.x == 0.f && alpha.y == 0.f) continue;
         const int j = e / nl, l = e - j * nl;

@@ -7,7 +7,8 @@ namespace ddagpu {
 struct PostArgs {
     size_t N;
     int nrhs, ni, nj, nl;
-    const signed char *occ;   // [N]
+    const signed char *occ;   // [N], or [nrhs][N] with occ_stride = N
+    size_t occ_stride;        // 0: one occupancy shared by every right-hand side
     const int *mv;            // [nmat1]
     const float2 *alpha;      // [nrhs][nmat1]
     int nmat1;

@@ -82,10 +82,11 @@ __global__ void __launch_bounds__(256) field_op(FieldArgs a)
     float2 *h = a.h ? a.h + off : nullptr, *w = a.w ? a.w + off : nullptr;
     const float2 cA = S.cA, cB = S.cB, cW = S.cW, c2 = S.c2;
     const float rA = S.rA, rB = S.rB, tau = a.tau;
+    const signed char *occ = a.occ + (size_t)rhs * a.occ_stride;
     double v[4] = {0.0, 0.0, 0.0, 0.0};
     for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < N;
          q += (size_t)gridDim.x * blockDim.x) {
-        const bool act = a.mv[(int)a.occ[q]] != 0;
+        const bool act = a.mv[(int)occ[q]] != 0;
         float2 P[3], R[3], Sv[3], X[3], Y[3];
         if (OP == OP_STEP0_CG) { // s = r; error
             ld3(r, N, q, R);
@@ -253,10 +254,11 @@ __global__ void __launch_bounds__(256) first_approx(FieldArgs a)
     __syncthreads();
     const size_t N = a.N, off = (size_t)rhs * 3 * N;
     const float2 *al = a.alpha + (size_t)rhs * a.nmat1;
+    const signed char *occ = a.occ + (size_t)rhs * a.occ_stride;
     for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < N;
          q += (size_t)gridDim.x * blockDim.x) {
         const int l = (int)(q % nl), j = (int)((q / nl) % nj), i = (int)(q / ((size_t)nl * nj));
-        const int m = a.occ[q];
+        const int m = occ[q];
         float2 out[3];
         if (a.mv[m]) {
             const float2 ph = cmul(cmul(tab[nj + nl + i], tab[j]), tab[nj + l]);
@@ -400,9 +402,10 @@ __global__ void __launch_bounds__(256) refine_op(FieldArgs a, int op)
     if (a.rhs_active && !a.rhs_active[rhs]) return;
     const size_t N = a.N, off = (size_t)rhs * 3 * N;
     double v[1] = {0.0};
+    const signed char *occ = a.occ + (size_t)rhs * a.occ_stride;
     for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < N;
          q += (size_t)gridDim.x * blockDim.x) {
-        const int m = a.occ[q];
+        const int m = occ[q];
         const bool act = a.mv[m] != 0;
         if (op == 0) {
 #pragma unroll

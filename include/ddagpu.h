@@ -169,6 +169,24 @@ int ddagpu_orientation_solves(ddagpu_ctx *ctx, const ddagpu_batch_cfg *cfg, int 
                               const double *rot, double *cabs, double *cext, double *mueller,
                               ddagpu_batch_info *info);
 
+/* Realisation batch: n_real targets on this context's lattice, each with its own occupancy
+ * occ[n_real][i][j][l] (host; cfg->occ is not used) -- the sample loop of main.cpp:806-985
+ * for targets that change between samples (random and agglomerate targets, or shape files).
+ * Right-hand sides of one batched solve carry different occupancies.  rot[n_real][9] as for
+ * ddagpu_orientation_solves, or NULL for the fixed orientation psi = iota = kappa = 0. */
+int ddagpu_realization_solves(ddagpu_ctx *ctx, const ddagpu_batch_cfg *cfg, int n_real,
+                              const signed char *occ, const double *rot, double *cabs,
+                              double *cext, double *mueller, ddagpu_batch_info *info);
+
+/* Agglomerate realisations (target 6, particle.cpp:21-85): realisation k is the monomer
+ * list monomers[first_k .. first_k + counts[k])[13] of ddagpu_anthrax_place, rasterised on
+ * the GPU straight into the batch (no occupancy crosses the host).  One material
+ * (cfg->n_mat = 1); ndip[n_real] (may be NULL) receives each realisation's dipole count. */
+int ddagpu_agglomerate_solves(ddagpu_ctx *ctx, const ddagpu_batch_cfg *cfg, int n_real,
+                              const float *monomers, const int *counts, const double *rot,
+                              double *cabs, double *cext, double *mueller, int *ndip,
+                              ddagpu_batch_info *info);
+
 /* Number of scattering angles for a configuration (rounding of main.cpp:201). */
 int ddagpu_num_angles(float theta_min, float theta_max, float theta_step);
 
