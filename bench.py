@@ -152,6 +152,13 @@ def run_reference_arm(args):
 
 
 # ------------------------------------------------------------------------- our arm
+def matvec_bytes(n: int, nrhs: int) -> float:
+    """Algorithmic HBM bytes of one matvec launch on an n^3 lattice: the Green-tensor
+    octant read once (384 B per cell) and, per right-hand side, the field read and written
+    plus the three passes over the half-padded spectrum (624 B per cell)."""
+    return 384.0 * n ** 3 + 624.0 * n ** 3 * nrhs
+
+
 def load_traffic(nrhs: int):
     """DRAM bytes per matvec from the committed ncu summary, scaled to nrhs."""
     path = os.path.join(ROOT, "profiles", "matvec_traffic.json")
@@ -177,7 +184,7 @@ def main():
                     help="only run the matvec on NRHS right-hand sides (for ncu captures)")
     ap.add_argument("--grid", type=int, default=GRID)
     ap.add_argument("--workload", default="orientations",
-                    choices=["orientations", "precision", "adjoint"])
+                    choices=["orientations", "precision", "adjoint", "realizations"])
     args = ap.parse_args()
     if args.profile_matvec:
         return profile_matvec(args)
@@ -187,6 +194,8 @@ def main():
         return adjoint_run(args)
     if args.warmup < 3:
         args.warmup = 3
+    if args.workload == "realizations":
+        return realizations_run(args)
     if args.impl == "reference":
         return run_reference_arm(args)
 
@@ -310,7 +319,7 @@ def main():
     g1.record(stream)
     torch.cuda.synchronize(dev)
     mv_ms = g0.elapsed_time(g1) / reps
-    alg_bytes = 384.0 * n3 + 624.0 * n3 * nrhs     # B RHS sharing Ahat
+    alg_bytes = matvec_bytes(GRID, nrhs)
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
         peak, peak_src = float(peaks["hbm_gbs"]), "measured"
@@ -444,6 +453,183 @@ def adjoint_run(args):
                       "grad_norm_re": float(np.linalg.norm(m_re.grad.numpy())),
                       "grad_norm_im": float(np.linalg.norm(m_im.grad.numpy()))}), flush=True)
     G.close()
+
+
+AGG_SIZES, AGG_N, AGG_R, AGG_LR, AGG_RHO = (32, 64, 128), 64, 3.0, 0.0, 0.25
+AGG_METRIC = "realization-solves/s, agglomerates on lattices drawn from {32,64,128}^3"
+AGG_WORKLOAD = ("64 agglomerate realisations (monomer radius 3 cells, length ratio 0, packing "
+                "0.25; realisation k placed from the random stream of worker k of seed 7) on "
+                "lattice edges drawn from {32, 64, 128} by the reference's generator seeded 7; "
+                "x=6, m=1.55+0.005i, CM, CG, Error_max 1e-3, Max_Step 20, fixed orientation, "
+                "1 plane, 19 angles, both polarisations")
+
+
+def xorshift_draws(seed: int, count: int):
+    """dda_srand / dda_rand (randomize.cpp:44-58): count draws after seeding."""
+    m = (1 << 64) - 1
+    s = seed or 0x9E3779B97F4A7C15
+    out = []
+    for _ in range(count):
+        s ^= s >> 12
+        s = (s ^ (s << 25)) & m
+        s ^= s >> 27
+        out.append(((s * 2685821657736338717) & m) >> 33)
+    return out
+
+
+def agglomerate_sizes():
+    return [AGG_SIZES[v % len(AGG_SIZES)] for v in xorshift_draws(SEED, AGG_N)]
+
+
+def realizations_reference(args, sizes):
+    """The reference's own sample loop (oracle/_ref) on agglomerates of each lattice size,
+    a bounded sample of realisations per size on all host threads; the job time is
+    estimated as the sum over sizes of (realisations of that size) / (measured rate)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as P
+    threads = os.cpu_count() or 1
+    R = P.RefLib()
+    per = {}
+    for n in AGG_SIZES:
+        ns = args.cpu_samples or threads
+        cfg = P.make_run_cfg(grid=n, target=6, x=X, materials=(MAT,), seed=SEED,
+                             monomer_radius=AGG_R, monomer_ratio=AGG_LR, packing=AGG_RHO)
+        secs, *_ = R.run_samples(cfg, ns, threads)
+        per[n] = (ns, secs)
+    total = sum(sizes.count(n) * per[n][1] / per[n][0] for n in AGG_SIZES)
+    value = len(sizes) / total
+    sample = ", ".join(f"{per[n][0]} realisations at {n}^3 in {per[n][1]:.1f} s"
+                       for n in AGG_SIZES) + f" on {threads} threads (Green tensor set-up excluded)"
+    return value, threads, sample, total
+
+
+def realizations_run(args):
+    """The realisation half of the batching configuration: every realisation is placed on
+    the host (the reference's float geometry, one thread per realisation), rasterised on
+    the GPU into the batch of its lattice size and solved for both polarisations; the three
+    lattice sizes run concurrently, one context and stream each.  value: the GPU part
+    (monomer lists to Mueller matrices); e2e: placement included."""
+    from concurrent.futures import ThreadPoolExecutor
+    sizes = agglomerate_sizes()
+    if args.impl == "reference":
+        if int(os.environ.get("RANK", "0")) != 0:
+            return
+        value, cores, sample, total = realizations_reference(args, sizes)
+        print(json.dumps({
+            "impl": "reference", "metric": AGG_METRIC, "value": value,
+            "unit": "realization-solves/s", "n_gpus": args.gpus, "steps": 1, "warmup": 0,
+            "ms_per_step": 1000 * total, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": AGG_WORKLOAD, "sizes": {str(n): sizes.count(n) for n in AGG_SIZES}},
+            "cpu_baseline": {"value": value, "unit": "realization-solves/s", "cores": cores,
+                             "kind": "reference", "sample": sample},
+            "e2e": {"value": value, "unit": "realization-solves/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}), flush=True)
+        return
+    import torch
+    import dda_fft_b200 as D
+    K, W = args.steps, args.warmup
+    groups = {n: [k for k, s in enumerate(sizes) if s == n] for n in AGG_SIZES}
+    counts = {n: D.Agglomerate.count((n, n, n), AGG_RHO, AGG_R, AGG_LR) for n in AGG_SIZES}
+    ctxs = {n: D.Context(n, 2 * X / n, max_rhs=2 * max(len(g), 1)) for n, g in groups.items() if g}
+    cfg = D.BatchConfig(occ=None, materials=[MAT])
+    pool = ThreadPoolExecutor(max_workers=os.cpu_count() or 4)
+
+    def place(step, k):
+        n = sizes[k]
+        return D.Agglomerate(SEED, step * AGG_N + k).place(n, AGG_R, AGG_R * AGG_LR, counts[n])
+
+    def solve_group(n, mons):
+        return ctxs[n].agglomerate_solves(cfg, mons)
+
+    def step_device(mons):
+        """the three lattice sizes concurrently, monomers already placed"""
+        futs = {n: pool.submit(solve_group, n, [mons[k] for k in g]) for n, g in groups.items() if g}
+        return {n: f.result() for n, f in futs.items()}
+
+    def step_e2e(step):
+        def group(n, g):
+            mons = list(pool.map(lambda k: place(step, k), g))
+            return solve_group(n, mons)
+        # the largest lattices first: their placement is the longest
+        with ThreadPoolExecutor(max_workers=len(groups)) as gp:
+            futs = {n: gp.submit(group, n, g) for n, g in sorted(groups.items(), reverse=True) if g}
+            return {n: f.result() for n, f in futs.items()}
+
+    placed = [list(pool.map(lambda k: place(s, k), range(AGG_N))) for s in range(W + K)]
+    for s in range(W):
+        step_device(placed[s])
+    clk = ClockSampler(0)
+    launches0 = sum(c.kernel_launches for c in ctxs.values())
+    torch.cuda.synchronize()
+    clk.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    res = None
+    for s in range(W, W + K):
+        res = step_device(placed[s])
+    torch.cuda.synchronize()
+    e1.record()
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    launches = sum(c.kernel_launches for c in ctxs.values()) - launches0
+    ms = e0.elapsed_time(e1)
+    value = K * AGG_N / (ms / 1000.0)
+    t0 = time.perf_counter()
+    for s in range(W, W + K):
+        step_e2e(s)
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    e2e = K * AGG_N / e2e_s
+    nA = D.num_angles(0, 180, 10)
+    h2d = sum(counts[s] * 13 * 4 for s in sizes) + AGG_N * 200
+    d2h = AGG_N * (16 + nA * 16 * 8 + 4)
+    # roofline: the matvec on the largest lattice's batch
+    nbig = max(n for n, g in groups.items() if g)
+    nrhs = 2 * len(groups[nbig])
+    ctx = ctxs[nbig]
+    x = torch.randn(nrhs, 3, nbig, nbig, nbig, dtype=torch.complex64, device="cuda")
+    y = torch.empty_like(x)
+    stream = torch.cuda.ExternalStream(ctx.stream_ptr, device=0)
+    for _ in range(3):
+        ctx.convolution_dev(x, y, nrhs)
+    g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    g0.record(stream)
+    for _ in range(5):
+        ctx.convolution_dev(x, y, nrhs)
+    g1.record(stream)
+    torch.cuda.synchronize()
+    mv_ms = g0.elapsed_time(g1) / 5
+    del x, y
+    try:
+        peak, src = float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]), "measured"
+    except Exception:
+        peak, src = 6650.0, "fallback"
+    achieved = matvec_bytes(nbig, nrhs) / (mv_ms / 1000.0) / 1e9
+    cpu = None
+    if not args.no_cpu:
+        v, cores, sample, _ = realizations_reference(args, sizes)
+        cpu = {"value": v, "unit": "realization-solves/s", "cores": cores, "kind": "reference",
+               "sample": sample}
+    info = {n: {"realizations": len(groups[n]), "max_steps": r["max_steps"],
+                "mean_dipoles": float(np.mean(r["ndip"])), "rolled_back": r["rolled_back"]}
+            for n, r in res.items()}
+    print(json.dumps({
+        "metric": AGG_METRIC, "value": value, "unit": "realization-solves/s", "n_gpus": 1,
+        "steps": K, "warmup": W, "ms_per_step": ms / K, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": AGG_WORKLOAD, "groups": info,
+                   "l2": "working set per step >> L2 (126 MB): no flush needed"},
+        "e2e": {"value": e2e, "unit": "realization-solves/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h, "includes": "host placement of every realisation"},
+        "roofline": {"kernel": f"matvec K1+K2+K3 at {nbig}^3", "bound": "hbm",
+                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_source": src, "traffic": None, "ms_per_launch": mv_ms,
+                     "rhs_per_launch": nrhs, "kernels": "specialised" if ctx.fast_kernels else "generic"},
+        "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches}), flush=True)
+    for c in ctxs.values():
+        c.close()
+    pool.shutdown()
 
 
 def _cm_alpha(d0, m):

@@ -207,20 +207,23 @@ class RunCfg(C.Structure):
                 ("tau", _d), ("err_max", _d), ("max_step", _i), ("fft_mode", _i),
                 ("orientation", _i), ("psi", _d), ("iota", _d), ("kappa", _d), ("nplanes", _i),
                 ("theta_min", _d), ("theta_max", _d), ("theta_step", _d),
-                ("seed", C.c_ulonglong)]
+                ("seed", C.c_ulonglong), ("monomer_radius", _d), ("monomer_ratio", _d),
+                ("packing", _d)]
 
 
 def make_run_cfg(grid=32, target=1, b_a=1.0, c_a=1.0, x=2.0, materials=((1.5, 0.01),),
                  polarizability=1, solver=0, tau=0.0, err_max=1e-3, max_step=20, fft_mode=0,
                  orientation=0, psi=0.0, iota=0.0, kappa=0.0, nplanes=1, theta_min=0.0,
-                 theta_max=180.0, theta_step=10.0, seed=1):
+                 theta_max=180.0, theta_step=10.0, seed=1, monomer_radius=0.0, monomer_ratio=0.0,
+                 packing=0.0):
     g = grid if isinstance(grid, (tuple, list)) else (grid, grid, grid)
     m = (_d * 32)()
     for k, (re, im) in enumerate(materials):
         m[2 * k], m[2 * k + 1] = re, im
     return RunCfg(g[0], g[1], g[2], target, b_a, c_a, x, len(materials), m, polarizability,
                   solver, tau, err_max, max_step, fft_mode, orientation, psi, iota, kappa,
-                  nplanes, theta_min, theta_max, theta_step, seed)
+                  nplanes, theta_min, theta_max, theta_step, seed, monomer_radius, monomer_ratio,
+                  packing)
 
 
 class RefLib:

@@ -455,7 +455,7 @@ int dref_rng(unsigned long long seed, int count, int *out)
  * ------------------------------------------------------------------------------- */
 struct dref_run_cfg {
     int ni, nj, nl;
-    int target;             /* 1 sphere, 2 ellipsoid, 11 occupancy from occ_in       */
+    int target;             /* 1 sphere, 2 ellipsoid, 6 agglomerate, 11 occ_in       */
     double b_a, c_a;
     double x;               /* size parameter                                        */
     int nmat;               /* materials                                             */
@@ -471,6 +471,7 @@ struct dref_run_cfg {
     int nplanes;
     double theta_min, theta_max, theta_step;
     unsigned long long seed;
+    double monomer_radius, monomer_ratio, packing;   /* target 6 (main.cpp:300, 585-586) */
 };
 
 int dref_run_samples(const dref_run_cfg *c, const signed char *occ_in, int nthreads, int nsamples,
@@ -588,6 +589,10 @@ int dref_run_samples(const dref_run_cfg *c, const signed char *occ_in, int nthre
         vector kinc = kincF;
         cvector einc[2] = {eincF[0], eincF[1]};
         std::vector<mmuller> mm((size_t)nA);
+        const real rw = (real)c->monomer_radius, lrw = (real)c->monomer_ratio, rho = (real)c->packing;
+        const int nworms = c->target == 6
+            ? (int)(rho * (real)(ni * nj * nl) / (8. * (rw * rw * rw) * (0.75 * lrw + 1))) + 1 : 0;
+        std::vector<cylinder> worms((size_t)(nworms > 0 ? nworms : 1));
         dda_workspace ws;
         dda_workspace_create(&ws, ni, nj, nl, c->solver);
         ws.iVerbose = verbose;
@@ -597,6 +602,8 @@ int dref_run_samples(const dref_run_cfg *c, const signed char *occ_in, int nthre
             if (task >= nsamples) break;
             if (c->target == 1) iGenerateEllipsoid(ni, nj, nl, 1., 1., vo.get());
             if (c->target == 2) iGenerateEllipsoid(ni, nj, nl, (real)c->b_a, (real)c->c_a, vo.get());
+            if (c->target == 6)
+                iGenerateAnthrax(ni, nj, nl, rw, rw * lrw, nworms, worms.data(), vo.get());
             if (c->orientation == 1) {
                 /* Euler-angle draw and rotation matrix of main.cpp:875-917 */
                 real cps = (real)dda_rand() * 2. / (real)DDA_RAND_MAX - 1.;

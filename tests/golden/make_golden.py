@@ -193,6 +193,12 @@ def agglomerates(R, out):
             out[f"{name}_occ_bits"] = np.packbits(occ.ravel() != 0)
         out[f"{name}_occ_sha256"] = np.frombuffer(
             hashlib.sha256((occ != 0).astype(np.uint8).tobytes()).digest(), np.uint8)
+    # the reference's sample loop on agglomerates (one worker: realisations drawn one after
+    # another from its stream), 32^3, x = 6, m = 1.55 + 0.005i, CM, CG, 3 samples
+    cfg = make_run_cfg(grid=32, target=6, x=6.0, materials=((1.55, 0.005),), seed=7,
+                       monomer_radius=3.0, monomer_ratio=0.0, packing=0.25)
+    _, ca, ce, mm = R.run_samples(cfg, 3, 1)
+    out["agg32_loop3"] = np.concatenate([[ca, ce], mm.ravel()])
 
 
 def main():
