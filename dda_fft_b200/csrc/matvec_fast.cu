@@ -1,5 +1,5 @@
-// Fast matvec passes for lattice edges in {16, 32, 64}: the same three passes and the same
-// split-order spectral layout as matvec.cu, with every size a compile-time constant.
+// Fast matvec passes for lattice edges in {16, 32, 64, 128}: the same three passes and the
+// same split-order spectral layout as matvec.cu, with every size a compile-time constant.
 //
 // Every n-point FFT uses the factorisation n = R1 R2 (fft_split): a thread holds R1
 // elements of a line for step A and R2 elements for step B, and the steps exchange data
@@ -90,7 +90,7 @@ __global__ void __launch_bounds__(NT) k1f(MatvecArgs a)
     using SJ = Sp<NJ>;
     using SL = Sp<NL>;
     constexpr int PS = SL::PS;
-    __shared__ float2 Z[NJ * PS];
+    extern __shared__ float2 Z[];   // [NJ][PS]
     const int hl = blockIdx.x & 1, i = blockIdx.x >> 1, c = blockIdx.y, rhs = blockIdx.z;
     if (a.rhs_active && !a.rhs_active[rhs]) return;
     const int ni = a.L.ni;
@@ -169,7 +169,7 @@ __global__ void __launch_bounds__(NT) k1f(MatvecArgs a)
 // CTA (spectral row js, TL spectral columns): forward x (both halves), 3x3 product,
 // inverse x, in place.  Shared B[c][h][pos][t].
 template <int NI, int TL>
-__global__ void __launch_bounds__(Sp<NI>::RM * TL) k2f(MatvecArgs a)
+__global__ void __launch_bounds__(Sp<NI>::RM * TL, NI == 128 ? 2 : 1) k2f(MatvecArgs a)
 {
     using S = Sp<NI>;
     constexpr int R1 = S::R1, R2 = S::R2, RM = S::RM;
@@ -361,7 +361,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(NT) k3f(MatvecArgs a
     using SJ = Sp<NJ>;
     using SL = Sp<NL>;
     constexpr int PS = SL::PS;
-    __shared__ float2 Q[NJ * PS];
+    extern __shared__ float2 Q[];   // [NJ][PS]
     cg::cluster_group cl = cg::this_cluster();
     const int hl = (int)cl.block_rank();
     const int i = blockIdx.x >> 1, c = blockIdx.y, rhs = blockIdx.z;
@@ -477,11 +477,29 @@ constexpr int yz_threads()
 }
 
 template <int NJ, int NL>
+constexpr size_t yz_smem()
+{
+    return (size_t)NJ * Sp<NL>::PS * sizeof(float2);   // one plane, 128 KB at 128 x 128
+}
+
+template <int NJ, int NL>
 void launch_yz(const MatvecArgs &a, int fwd, cudaStream_t st)
 {
     constexpr int NT = yz_threads<NJ, NL>();
-    if (fwd) k1f<NJ, NL, NT><<<dim3(2 * a.L.ni, 3, a.nrhs), NT, 0, st>>>(a);
-    else k3f<NJ, NL, NT><<<dim3(2 * a.L.ni, 3, a.nrhs), NT, 0, st>>>(a);
+    constexpr size_t S = yz_smem<NJ, NL>();
+    if (fwd) k1f<NJ, NL, NT><<<dim3(2 * a.L.ni, 3, a.nrhs), NT, S, st>>>(a);
+    else k3f<NJ, NL, NT><<<dim3(2 * a.L.ni, 3, a.nrhs), NT, S, st>>>(a);
+}
+
+template <int NJ, int NL>
+cudaError_t prep_yz()
+{
+    constexpr int NT = yz_threads<NJ, NL>();
+    constexpr int S = (int)yz_smem<NJ, NL>();
+    cudaError_t e = cudaFuncSetAttribute(k1f<NJ, NL, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, S);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k3f<NJ, NL, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, S);
+    return e;
 }
 
 template <int NI>
@@ -507,7 +525,7 @@ cudaError_t prep_x()
                                 (int)(6 * NI * TL * sizeof(float2)));
 }
 
-bool fast_edge(int n) { return n == 16 || n == 32 || n == 64; }
+bool fast_edge(int n) { return n == 16 || n == 32 || n == 64 || n == 128; }
 
 }  // namespace
 
@@ -516,32 +534,46 @@ bool matvec_fast_supported(const Lat &L)
     return fast_edge(L.ni) && fast_edge(L.nj) && fast_edge(L.nl) && 2 * L.nl >= 32;
 }
 
+#define DISPATCH_YZ(NJv, CALL)                                                               \
+    case NJv:                                                                                \
+        switch (nl) {                                                                        \
+        case 16: CALL(NJv, 16); break;                                                       \
+        case 32: CALL(NJv, 32); break;                                                       \
+        case 64: CALL(NJv, 64); break;                                                       \
+        case 128: CALL(NJv, 128); break;                                                     \
+        }                                                                                    \
+        break;
+#define YZ_SWITCH(CALL)                                                                      \
+    switch (nj) {                                                                            \
+        DISPATCH_YZ(16, CALL)                                                                \
+        DISPATCH_YZ(32, CALL)                                                                \
+        DISPATCH_YZ(64, CALL)                                                                \
+        DISPATCH_YZ(128, CALL)                                                               \
+    }
+
 cudaError_t matvec_fast_prepare(const Lat &L)
 {
+    cudaError_t e = cudaErrorInvalidValue;
+    const int nj = L.nj, nl = L.nl;
+#define PREP(J, K) e = prep_yz<J, K>()
+    YZ_SWITCH(PREP)
+#undef PREP
+    if (e != cudaSuccess) return e;
     switch (L.ni) {
     case 16: return prep_x<16>();
     case 32: return prep_x<32>();
     case 64: return prep_x<64>();
+    case 128: return prep_x<128>();
     }
     return cudaErrorInvalidValue;
 }
 
-#define DISPATCH_YZ(NJv)                                                                     \
-    case NJv:                                                                                \
-        switch (a.L.nl) {                                                                    \
-        case 16: launch_yz<NJv, 16>(a, fwd, st); break;                                      \
-        case 32: launch_yz<NJv, 32>(a, fwd, st); break;                                      \
-        case 64: launch_yz<NJv, 64>(a, fwd, st); break;                                      \
-        }                                                                                    \
-        break;
-
 static void yz(const MatvecArgs &a, int fwd, cudaStream_t st)
 {
-    switch (a.L.nj) {
-        DISPATCH_YZ(16)
-        DISPATCH_YZ(32)
-        DISPATCH_YZ(64)
-    }
+    const int nj = a.L.nj, nl = a.L.nl;
+#define LAUNCH(J, K) launch_yz<J, K>(a, fwd, st)
+    YZ_SWITCH(LAUNCH)
+#undef LAUNCH
 }
 
 cudaError_t launch_matvec_fast(const MatvecArgs &a, cudaStream_t st)
@@ -551,6 +583,7 @@ cudaError_t launch_matvec_fast(const MatvecArgs &a, cudaStream_t st)
     case 16: launch_x<16>(a, st); break;
     case 32: launch_x<32>(a, st); break;
     case 64: launch_x<64>(a, st); break;
+    case 128: launch_x<128>(a, st); break;
     }
     yz(a, 0, st);
     return cudaGetLastError();

@@ -28,17 +28,18 @@ def D():
     return dda_fft_b200
 
 
-FAST = {16, 32, 64}
+FAST = {16, 32, 64, 128}
 
 
 @pytest.mark.parametrize("grid", [(2, 2, 2), (4, 4, 4), (8, 8, 8), (16, 16, 16), (32, 32, 32),
                                   (8, 16, 8), (16, 4, 32), (64, 64, 64), (16, 64, 32),
-                                  (64, 16, 16), (32, 16, 64)])
+                                  (64, 16, 16), (32, 16, 64), (128, 16, 16), (16, 128, 32),
+                                  (32, 16, 128)])
 @pytest.mark.parametrize("conj", [False, True])
 @pytest.mark.parametrize("fast", [False, True])
 def test_convolution_vs_oracle(D, oracle, grid, conj, fast):
     if fast and not set(grid) <= FAST:
-        pytest.skip("specialised passes cover edges 16..64")
+        pytest.skip("specialised passes cover edges 16..128")
     rng = np.random.default_rng(sum(grid) + conj)
     kd = 2 * 3.0 / grid[0]
     p = crand(rng, grid + (3,))
@@ -107,6 +108,28 @@ def test_convolution_128_impulse(D):
         scale = max(scale, np.abs(g).max())
     assert worst < 1e-4 * scale + 1e-7
     assert np.abs(out[r0]).max() < 1e-4 * scale + 1e-7     # G(0) = 0
+
+
+@pytest.mark.parametrize("grid", [(128, 128, 128), (128, 64, 128), (64, 128, 32)])
+def test_fast_and_generic_agree_128(D, grid):
+    """The specialised 128-edge passes against the generic passes on the same random
+    fields (both float32; two right-hand sides, plain and conjugate)."""
+    import torch
+    rng = np.random.default_rng(5)
+    p = crand(rng, (2, 3) + grid)
+    with D.Context(grid, 0.2, max_rhs=2) as ctx:
+        assert ctx.fast_kernels
+        x = torch.from_numpy(p).cuda()
+        outs = {}
+        for fast in (True, False):
+            for conj in (False, True):
+                ctx.set_kernels(fast)
+                y = torch.empty_like(x)
+                ctx.convolution_dev(x, y, 2, conj=conj)
+                torch.cuda.synchronize()
+                outs[fast, conj] = y.cpu().numpy()
+    for conj in (False, True):
+        assert rel(outs[True, conj], outs[False, conj]) < 2e-6
 
 
 def test_convolution_linearity_128(D):
