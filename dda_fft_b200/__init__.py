@@ -10,6 +10,7 @@ from .api import (  # noqa: F401
     BatchConfig,
     Context,
     DDAGPUError,
+    RandomEllipsoid,
     build,
     fixed_rotation,
     lib,
@@ -18,5 +19,5 @@ from .api import (  # noqa: F401
     num_angles,
 )
 
-__all__ = ["Agglomerate", "Context", "BatchConfig", "DDAGPUError", "build", "lib", "library_path",
+__all__ = ["Agglomerate", "Context", "BatchConfig", "DDAGPUError", "RandomEllipsoid", "build", "lib", "library_path",
            "mc_rotations", "fixed_rotation", "num_angles"]

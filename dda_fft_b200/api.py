@@ -115,6 +115,10 @@ def lib():
         L.ddagpu_anthrax_count.restype = C.c_longlong
         L.ddagpu_anthrax_place.argtypes = [C.POINTER(C.c_ulonglong), _i, _f, _f, _i, _p]
         L.ddagpu_anthrax_rasterize.argtypes = [_i, _i, _i, _i, _p, _i, _p, C.POINTER(_i)]
+        L.ddagpu_random_ellipsoid_seeds.argtypes = [C.POINTER(C.c_ulonglong), _i, _i, _i, _f, _f,
+                                                    _i, _p]
+        L.ddagpu_random_ellipsoid_fill.argtypes = [_i, _i, _i, _i, _f, _f, _p, _p, _i, _p,
+                                                   C.POINTER(_i)]
         _lib = L
         return L
 
@@ -195,6 +199,44 @@ class Agglomerate:
         mon = self.place(grid[0], monomer_radius, monomer_length, count)
         occ, nd = self.rasterize(grid, mon, device)
         return occ, nd, mon
+
+
+class RandomEllipsoid:
+    """Random (Voronoi) ellipsoids (targets 4 and 5, iGenerateRandomEllipsoid,
+    particle.cpp:531-614): seeds drawn on the host from the reference's random stream,
+    nearest-seed fill on the GPU; seeds_per_material[m] seeds give material m + 1."""
+
+    def __init__(self, base_seed: int = 0, worker: int = 0, state: int | None = None):
+        self.state = int(lib().ddagpu_rng_seed(C.c_ulonglong(base_seed), worker)
+                         if state is None else state)
+
+    def seeds(self, grid, b_a: float, c_a: float, n_seeds: int) -> np.ndarray:
+        ni, nj, nl = grid
+        out = np.zeros((n_seeds, 3), np.float32)
+        s = C.c_ulonglong(self.state)
+        _check(lib().ddagpu_random_ellipsoid_seeds(C.byref(s), ni, nj, nl, b_a, c_a, n_seeds,
+                                                   _ptr(out)))
+        self.state = s.value
+        return out
+
+    @staticmethod
+    def fill(grid, b_a: float, c_a: float, seeds: np.ndarray, seeds_per_material,
+             device: int = 0):
+        """(occ int8 [ni][nj][nl] of materials 0..n_mat, the reference's count of
+        material-1 cells)."""
+        ni, nj, nl = grid
+        sd = _f32(seeds)
+        spm = np.ascontiguousarray(seeds_per_material, np.int32)
+        occ = np.zeros((ni, nj, nl), np.int8)
+        nd = C.c_int(0)
+        _check(lib().ddagpu_random_ellipsoid_fill(device, ni, nj, nl, b_a, c_a, _ptr(sd),
+                                                  _ptr(spm), len(spm), _ptr(occ), C.byref(nd)))
+        return occ, nd.value
+
+    def generate(self, grid, b_a: float, c_a: float, seeds_per_material, device: int = 0):
+        sd = self.seeds(grid, b_a, c_a, int(np.sum(seeds_per_material)))
+        occ, nd = self.fill(grid, b_a, c_a, sd, seeds_per_material, device)
+        return occ, nd, sd
 
 
 @dataclass

@@ -17,7 +17,7 @@
 #include <vector>
 
 #include "../../include/ddagpu.h"
-#include "agglomerate.h"
+#include "targets.h"
 #include "internal.h"
 #include "post.h"
 #include "solver.h"
@@ -1370,6 +1370,54 @@ int ddagpu_anthrax_rasterize(int device, int i_max, int j_max, int l_max, const 
     if (e == cudaSuccess) e = cudaMemcpyAsync(occ, d, N, cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(&h, nd, sizeof(int), cudaMemcpyDeviceToHost, st);
     if (d) cudaFreeAsync(d, st);
+    if (nd) cudaFreeAsync(nd, st);
+    cudaError_t e2 = cudaStreamSynchronize(st);
+    cudaStreamDestroy(st);
+    CK(e);
+    CK(e2);
+    if (ndip) *ndip = h;
+    return DDAGPU_OK;
+}
+
+int ddagpu_random_ellipsoid_seeds(unsigned long long *rng_state, int i_max, int j_max, int l_max,
+                                  float b_a, float c_a, int n_seeds, float *seeds)
+{
+    if (!rng_state || !seeds || n_seeds < 1 || i_max < 1 || j_max < 1 || l_max < 1)
+        return fail(DDAGPU_EINVAL, "bad random-ellipsoid arguments");
+    if (random_ellipsoid_seeds(rng_state, i_max, j_max, l_max, b_a, c_a, n_seeds, seeds))
+        return fail(DDAGPU_EINVAL, "the ellipsoid does not fit in the lattice");
+    return DDAGPU_OK;
+}
+
+int ddagpu_random_ellipsoid_fill(int device, int i_max, int j_max, int l_max, float b_a, float c_a,
+                                 const float *seeds, const int *seeds_per_material, int n_mat,
+                                 signed char *occ, int *ndip)
+{
+    if (!seeds || !seeds_per_material || !occ || n_mat < 1 || n_mat > kMaxMaterials - 1 ||
+        i_max < 1 || j_max < 1 || l_max < 1)
+        return fail(DDAGPU_EINVAL, "bad random-ellipsoid arguments");
+    long long total = 0;
+    for (int m = 0; m < n_mat; m++) {
+        if (seeds_per_material[m] < 0) return fail(DDAGPU_EINVAL, "negative seed count");
+        total += seeds_per_material[m];
+    }
+    if (total < 1 || total > (1 << 24)) return fail(DDAGPU_EINVAL, "bad total seed count");
+    if ((float)i_max * b_a > (float)j_max || (float)i_max * c_a > (float)l_max)
+        return fail(DDAGPU_EINVAL, "the ellipsoid does not fit in the lattice");
+    DevGuard dg(device);
+    const size_t N = (size_t)i_max * j_max * l_max;
+    cudaStream_t st;
+    CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    signed char *dv = nullptr;
+    int *nd = nullptr, h = 0;
+    cudaError_t e = cudaMallocAsync(&dv, N, st);
+    if (e == cudaSuccess) e = cudaMallocAsync(&nd, sizeof(int), st);
+    if (e == cudaSuccess)
+        e = random_ellipsoid_fill(seeds, seeds_per_material, n_mat, i_max, j_max, l_max, b_a, c_a, dv,
+                                  nd, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(occ, dv, N, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&h, nd, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (dv) cudaFreeAsync(dv, st);
     if (nd) cudaFreeAsync(nd, st);
     cudaError_t e2 = cudaStreamSynchronize(st);
     cudaStreamDestroy(st);

@@ -1,7 +1,8 @@
-// Agglomerates of capsule monomers (the anthrax-like target, iGenerateAnthrax,
-// particle.cpp:21-85): monomer placement on the host, rasterisation into the lattice on the
-// GPU.
+// Random targets of libddagpu: placement on the host from the reference's random stream,
+// rasterisation into the lattice on the GPU.
 //
+// Agglomerates of capsule monomers (the anthrax-like target, iGenerateAnthrax,
+// particle.cpp:21-85).
 // Placement consumes the reference's random stream (xorshift64*, randomize.cpp:44-58) and
 // accepts or rejects monomers with the reference's float geometry (worm,
 // particle.cpp:302-344; CrossTwoWorms, 233-300; PointToWorm, 379-400), so it is written
@@ -17,7 +18,7 @@
 #include <cmath>
 #include <vector>
 
-#include "agglomerate.h"
+#include "targets.h"
 
 namespace ddagpu {
 
@@ -205,7 +206,154 @@ __global__ void __launch_bounds__(256) rasterize(const DW *worms, int count, int
     if (threadIdx.x == 0 && block_hits) atomicAdd(ndip, block_hits);
 }
 
+// ---- random (Voronoi) ellipsoid, iGenerateRandomEllipsoid, particle.cpp:531-614
+struct EllGeom {
+    float cx, cy, cz;      // centre n / 2 - 0.5 per axis
+    float a2, b2, c2;      // squared semi-axes
+};
+
+EllGeom ellipsoid_geom(int ni, int nj, int nl, float b_a, float c_a)
+{
+    EllGeom g;
+    g.cx = (float)((double)(float)ni / 2. - .5);
+    g.cy = (float)((double)(float)nj / 2. - .5);
+    g.cz = (float)((double)(float)nl / 2. - .5);
+    float a = (float)ni, b = a * b_a, c = a * c_a;
+    a = (float)((double)a / 2.);
+    b = (float)((double)b / 2.);
+    c = (float)((double)c / 2.);
+    g.a2 = a * a;
+    g.b2 = b * b;
+    g.c2 = c * c;
+    return g;
+}
+
+// rounding(), complex.cpp:213-223, for the non-negative arguments used here
+int rounding_pos(float r0)
+{
+    double ip;
+    const double fr = std::modf((double)r0, &ip);
+    return fr > 0.5 ? (int)ip + 1 : (int)ip;
+}
+
+__device__ __forceinline__ float fd(float a, float b) { return __fdiv_rn(a, b); }
+
+constexpr int kSeedChunk = 512;
+
+__global__ void __launch_bounds__(256) voronoi_fill(const float *seeds, int nseeds, const int *sort_end,
+                                                    int nsorts, int ni, int nj, int nl, EllGeom g,
+                                                    float dist0, signed char *occ, int *ndip)
+{
+    __shared__ float s[3 * kSeedChunk];
+    __shared__ int block_hits;
+    const size_t N = (size_t)ni * nj * nl;
+    const size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (threadIdx.x == 0) block_hits = 0;
+    float px = 0.f, py = 0.f, pz = 0.f;
+    bool inside = false;
+    if (q < N) {
+        const int l = (int)(q % nl), j = (int)((q / nl) % nj), i = (int)(q / ((size_t)nl * nj));
+        px = (float)i;
+        py = (float)j;
+        pz = (float)l;
+        const float vx = fs(px, g.cx), vy = fs(py, g.cy), vz = fs(pz, g.cz);
+        inside = fa(fa(fd(fm(vx, vx), g.a2), fd(fm(vy, vy), g.b2)), fd(fm(vz, vz), g.c2)) <= 1.f;
+    }
+    int best = 0;
+    float dmin = dist0;
+    for (int c0 = 0; c0 < nseeds; c0 += kSeedChunk) {
+        __syncthreads();
+        const int m = nseeds - c0 < kSeedChunk ? nseeds - c0 : kSeedChunk;
+        for (int k = threadIdx.x; k < 3 * m; k += blockDim.x) s[k] = seeds[3 * (size_t)c0 + k];
+        __syncthreads();
+        if (inside)
+            for (int k = 0; k < m; k++) {
+                const float dx = fs(px, s[3 * k]), dy = fs(py, s[3 * k + 1]), dz = fs(pz, s[3 * k + 2]);
+                const float dist = __fsqrt_rn(dot3(dx, dy, dz, dx, dy, dz));
+                if (dist < dmin) {
+                    best = c0 + k;
+                    dmin = dist;
+                }
+            }
+    }
+    int mat = 0;
+    if (inside) {
+        // material m + 1 for seeds [sort_end[m-1], sort_end[m]) (first seed range: material 1)
+        for (int m = 0; m < nsorts; m++)
+            if (best < sort_end[m]) {
+                mat = m + 1;
+                break;
+            }
+    }
+    if (q < N) occ[q] = (signed char)mat;
+    if (mat == 1) atomicAdd(&block_hits, 1);   // the reference counts material-1 cells only
+    __syncthreads();
+    if (threadIdx.x == 0 && block_hits) atomicAdd(ndip, block_hits);
+}
+
 }  // namespace
+
+int random_ellipsoid_seeds(unsigned long long *state, int ni, int nj, int nl, float b_a, float c_a,
+                           int nseeds, float *seeds3)
+{
+    // iGenerateRandomEllipsoid, particle.cpp:538-573 (fits check, then seed draws)
+    const float a = (float)ni, b = a * b_a, c = a * c_a;
+    if (b > (float)nj || c > (float)nl) return -1;
+    const EllGeom g = ellipsoid_geom(ni, nj, nl, b_a, c_a);
+    unsigned long long s = *state;
+    for (int m = 0; m < nseeds; m++) {
+        V3 v0, v1;
+        int dup;
+        do {
+            dup = 0;
+            // (real)rand / (real)RAND_MAX in float, times ((real)n - 1.) in double, to float
+            v0.x = (float)rounding_pos((float)((double)((float)rng_draw(s) / kRandMax) * ((double)(float)ni - 1.)));
+            v0.y = (float)rounding_pos((float)((double)((float)rng_draw(s) / kRandMax) * ((double)(float)nj - 1.)));
+            v0.z = (float)rounding_pos((float)((double)((float)rng_draw(s) / kRandMax) * ((double)(float)nl - 1.)));
+            for (int i = 0; i < m; i++) {
+                const V3 d = vsub({seeds3[3 * i], seeds3[3 * i + 1], seeds3[3 * i + 2]}, v0);
+                if ((double)vabs(d) < 0.0000000001) {
+                    dup = 1;
+                    break;
+                }
+            }
+            v1 = vsub(v0, {g.cx, g.cy, g.cz});
+        } while (((v1.x * v1.x) / g.a2 + (v1.y * v1.y) / g.b2 + (v1.z * v1.z) / g.c2 > 1.f) && dup == 1);
+        seeds3[3 * m] = v0.x;
+        seeds3[3 * m + 1] = v0.y;
+        seeds3[3 * m + 2] = v0.z;
+    }
+    *state = s;
+    return 0;
+}
+
+cudaError_t random_ellipsoid_fill(const float *seeds3, const int *counts, int nsorts, int ni, int nj,
+                                  int nl, float b_a, float c_a, signed char *occ_dev, int *ndip_dev,
+                                  cudaStream_t st)
+{
+    // iGenerateRandomEllipsoid, particle.cpp:575-610: nearest seed (first on ties) inside
+    int nseeds = 0;
+    std::vector<int> ends((size_t)nsorts);
+    for (int m = 0; m < nsorts; m++) ends[(size_t)m] = (nseeds += counts[m]);
+    const EllGeom g = ellipsoid_geom(ni, nj, nl, b_a, c_a);
+    const float dist0 = std::sqrt((float)(ni * ni + nj * nj + nl * nl));
+    float *ds = nullptr;
+    int *de = nullptr;
+    cudaError_t e = cudaMallocAsync(&ds, (size_t)3 * (nseeds ? nseeds : 1) * sizeof(float), st);
+    if (!e) e = cudaMallocAsync(&de, (size_t)(nsorts ? nsorts : 1) * sizeof(int), st);
+    if (!e && nseeds) e = cudaMemcpyAsync(ds, seeds3, (size_t)3 * nseeds * sizeof(float), cudaMemcpyHostToDevice, st);
+    if (!e && nsorts) e = cudaMemcpyAsync(de, ends.data(), nsorts * sizeof(int), cudaMemcpyHostToDevice, st);
+    if (!e) e = cudaMemsetAsync(ndip_dev, 0, sizeof(int), st);
+    if (!e) {
+        const size_t N = (size_t)ni * nj * nl;
+        voronoi_fill<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(ds, nseeds, de, nsorts, ni, nj, nl, g,
+                                                                 dist0, occ_dev, ndip_dev);
+        e = cudaGetLastError();
+    }
+    if (ds) cudaFreeAsync(ds, st);
+    if (de) cudaFreeAsync(de, st);
+    return e;
+}
 
 long long anthrax_count(int ni, int nj, int nl, float packing, float radius, float ratio)
 {

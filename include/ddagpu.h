@@ -209,6 +209,18 @@ int ddagpu_anthrax_place(unsigned long long *rng_state, int i_max, float monomer
 int ddagpu_anthrax_rasterize(int device, int i_max, int j_max, int l_max, const float *monomers,
                              int count, signed char *occ, int *ndip);
 
+/* Random (Voronoi) ellipsoids (targets 4 and 5, iGenerateRandomEllipsoid,
+ * particle.cpp:531-614): seeds[n_seeds][3] drawn on the host from the reference's random
+ * stream (returns DDAGPU_EINVAL if the ellipsoid b/a, c/a does not fit the lattice); then
+ * every cell inside the ellipsoid takes the material of its nearest seed (the first on
+ * ties), seeds_per_material[m] seeds for material m + 1 in order, on the GPU.  ndip
+ * receives the reference's count: cells of material 1. */
+int ddagpu_random_ellipsoid_seeds(unsigned long long *rng_state, int i_max, int j_max, int l_max,
+                                  float b_a, float c_a, int n_seeds, float *seeds);
+int ddagpu_random_ellipsoid_fill(int device, int i_max, int j_max, int l_max, float b_a, float c_a,
+                                 const float *seeds, const int *seeds_per_material, int n_mat,
+                                 signed char *occ, int *ndip);
+
 /* Fixed orientation (degrees), main.cpp:516-541. */
 int ddagpu_fixed_rotation(double psi, double iota, double kappa, double *rot);
 

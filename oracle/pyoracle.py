@@ -250,6 +250,7 @@ class RefLib:
         L.dref_gen_ellipsoid.argtypes = [_i, _i, _i, _d, _d, _p]
         L.dref_rng.argtypes = [C.c_ulonglong, _i, _p]
         L.dref_gen_anthrax.argtypes = [C.c_ulonglong, _i, _i, _i, _d, _d, _i, _p, _p, _p]
+        L.dref_gen_random_ellipsoid.argtypes = [C.c_ulonglong, _i, _i, _i, _d, _d, _i, _p, _p, _p]
         L.dref_run_samples.argtypes = [C.POINTER(RunCfg), _p, _i, _i, _i, _p, _p, _p, _p, _p]
 
     def green(self, ni, nj, nl, kd, fft_mode=0):
@@ -361,6 +362,16 @@ class RefLib:
         nd = self.lib.dref_gen_anthrax(C.c_ulonglong(seed), n, n, n, radius, length, count,
                                        _ptr(occ), _ptr(cyl), C.byref(nxt))
         return occ, nd, cyl, nxt.value
+
+    def gen_random_ellipsoid(self, seed, grid, b_a, c_a, seeds_per_sort):
+        """iGenerateRandomEllipsoid after dda_srand(seed): (occ, count, next draw)."""
+        ni, nj, nl = grid
+        occ = np.zeros((ni, nj, nl), np.int8)
+        sps = np.ascontiguousarray(seeds_per_sort, np.int32)
+        nxt = C.c_int(0)
+        n = self.lib.dref_gen_random_ellipsoid(C.c_ulonglong(seed), ni, nj, nl, b_a, c_a, len(sps),
+                                               _ptr(sps), _ptr(occ), C.byref(nxt))
+        return occ, n, nxt.value
 
     def run_samples(self, cfg: RunCfg, nsamples, nthreads=1, occ=None, verbose=0):
         """The reference's sample loop; returns (seconds, cabs_sum, cext_sum, mueller_sum)."""

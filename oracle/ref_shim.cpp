@@ -438,6 +438,21 @@ int dref_gen_anthrax(unsigned long long seed, int ni, int nj, int nl, double rad
     return n;
 }
 
+/* iGenerateRandomEllipsoid (particle.cpp:531-614) after dda_srand(seed): occupancy, the
+   count the reference returns (material-1 cells) and the next draw of the stream. */
+int dref_gen_random_ellipsoid(unsigned long long seed, int ni, int nj, int nl, double b_a,
+                              double c_a, int nsorts, int *seeds_per_sort, signed char *occ,
+                              int *next_draw)
+{
+    std::vector<char> occb((size_t)ni * nj * nl);
+    view3<char> vo(occb.data(), ni, nj, nl);
+    dda_srand(seed);
+    int n = iGenerateRandomEllipsoid(ni, nj, nl, (real)b_a, (real)c_a, nsorts, seeds_per_sort, vo.get());
+    std::memcpy(occ, occb.data(), occb.size());
+    if (next_draw) *next_draw = dda_rand();
+    return n;
+}
+
 /* count draws of the reference generator after dda_srand(seed) (randomize.cpp:44-58). */
 int dref_rng(unsigned long long seed, int count, int *out)
 {

@@ -6,7 +6,7 @@ oracle/ref_shim.cpp), its FP64 build (oracle/_ref/libddaref64.so) and its unmodi
 executable (oracle/_ref/dda_fft.out).  Run in a container that has the reference tree:
 
     make -f oracle/Makefile all && python tests/golden/make_golden.py
-    python tests/golden/make_golden.py agglomerates     # anthrax_v72.npz
+    python tests/golden/make_golden.py targets          # targets_v72.npz
 
 The fixtures are small (.npz, a few MB in all) and are committed; the tests read
 them without needing the reference.
@@ -178,6 +178,12 @@ AGGLOMERATES = [("c3b32", 32, 3.0, 0.0, 0.25, 7), ("c3b64", 64, 3.0, 0.0, 0.25, 
                 ("caps64", 64, 2.0, 2.5, 0.3, 99), ("c3b128", 128, 3.0, 0.0, 0.25, 7)]
 
 
+# (name, lattice, b/a, c/a, seeds per material, generator seed)
+RANDOM_ELLIPSOIDS = [("rell32", (32, 32, 32), 1.0, 1.0, [40], 5),
+                     ("rell64", (64, 48, 32), 0.7, 0.5, [30, 20, 10], 9),
+                     ("rell16", (16, 16, 16), 1.0, 1.0, [3, 0, 2], 1)]
+
+
 def agglomerates(R, out):
     """iGenerateAnthrax (particle.cpp:21-85) after dda_srand(seed), monomer count as
     main.cpp:585-586: monomers, dipole count, the next draw of the stream, and the
@@ -199,13 +205,20 @@ def agglomerates(R, out):
                        monomer_radius=3.0, monomer_ratio=0.0, packing=0.25)
     _, ca, ce, mm = R.run_samples(cfg, 3, 1)
     out["agg32_loop3"] = np.concatenate([[ca, ce], mm.ravel()])
+    # random (Voronoi) ellipsoids, iGenerateRandomEllipsoid (particle.cpp:531-614)
+    for name, grid, ba, ca_, sps, seed in RANDOM_ELLIPSOIDS:
+        occ, n, nxt = R.gen_random_ellipsoid(seed, grid, ba, ca_, sps)
+        out[f"{name}_cfg"] = np.array(list(grid) + [ba, ca_, seed], np.float64)
+        out[f"{name}_seeds_per_material"] = np.array(sps, np.int32)
+        out[f"{name}_occ"] = occ
+        out[f"{name}_count_next"] = np.array([n, nxt], np.int64)
 
 
 def main():
-    if sys.argv[1:] == ["agglomerates"]:
+    if sys.argv[1:] == ["targets"]:
         out: dict = {}
         agglomerates(RefLib(), out)
-        path = os.path.join(HERE, "anthrax_v72.npz")
+        path = os.path.join(HERE, "targets_v72.npz")
         np.savez_compressed(path, **out)
         print(f"wrote {path}: {os.path.getsize(path) / 1e6:.2f} MB, {len(out)} arrays")
         return

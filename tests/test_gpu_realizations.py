@@ -22,7 +22,7 @@ def D():
 
 @pytest.fixture(scope="module")
 def fx():
-    return np.load(os.path.join(ROOT, "tests", "golden", "anthrax_v72.npz"))
+    return np.load(os.path.join(ROOT, "tests", "golden", "targets_v72.npz"))
 
 
 def targets(oracle, n):

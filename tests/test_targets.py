@@ -1,7 +1,7 @@
 """Agglomerate targets (iGenerateAnthrax, particle.cpp:21-85) against the reference's own
 generator: the host placement and its random stream must reproduce the reference's
 monomers and next draw bit for bit (CPU tests), and the GPU rasterisation the reference's
-occupancy cell for cell (GPU tests).  Fixtures: tests/golden/anthrax_v72.npz, written by
+occupancy cell for cell (GPU tests).  Fixtures: tests/golden/targets_v72.npz, written by
 tests/golden/make_golden.py from the reference's compiled sources."""
 import hashlib
 import os
@@ -15,7 +15,7 @@ CASES = ["c3b32", "c3b64", "caps64", "c3b128"]
 
 @pytest.fixture(scope="module")
 def fx():
-    return np.load(os.path.join(ROOT, "tests", "golden", "anthrax_v72.npz"))
+    return np.load(os.path.join(ROOT, "tests", "golden", "targets_v72.npz"))
 
 
 def cfg(fx, name):
@@ -119,3 +119,43 @@ def test_rasterization_edge_cases():
     np.testing.assert_array_equal(occ.ravel() != 0, ref)
     with pytest.raises(DDAGPUError):
         Agglomerate.rasterize((12, 16, 16), m)
+
+
+# ---------------------------------------------------------------- random (Voronoi) ellipsoids
+RELL = ["rell32", "rell64", "rell16"]
+
+
+def rell_cfg(fx, name):
+    ni, nj, nl, ba, ca, seed = fx[f"{name}_cfg"]
+    return (int(ni), int(nj), int(nl)), float(ba), float(ca), int(seed)
+
+
+@pytest.mark.parametrize("name", RELL)
+def test_random_ellipsoid_seed_stream(fx, name):
+    """The seed draws consume the reference's stream exactly (the next draw after them
+    matches) and every seed lies on the lattice."""
+    from dda_fft_b200 import RandomEllipsoid
+    grid, ba, ca, seed = rell_cfg(fx, name)
+    sps = fx[f"{name}_seeds_per_material"]
+    r = RandomEllipsoid(state=seed)
+    sd = r.seeds(grid, ba, ca, int(sps.sum()))
+    assert next_draw(r.state) == int(fx[f"{name}_count_next"][1])
+    assert (sd >= 0).all() and (sd <= np.array(grid) - 1).all()
+    assert np.array_equal(sd, np.round(sd))
+
+
+def test_random_ellipsoid_rejects_misfit():
+    from dda_fft_b200 import DDAGPUError, RandomEllipsoid
+    with pytest.raises(DDAGPUError):
+        RandomEllipsoid(state=3).seeds((32, 16, 32), 1.0, 1.0, 4)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", RELL)
+def test_random_ellipsoid_matches_reference(fx, name):
+    from dda_fft_b200 import RandomEllipsoid
+    grid, ba, ca, seed = rell_cfg(fx, name)
+    sps = fx[f"{name}_seeds_per_material"]
+    occ, count, _ = RandomEllipsoid(state=seed).generate(grid, ba, ca, sps)
+    np.testing.assert_array_equal(occ, fx[f"{name}_occ"])
+    assert count == int(fx[f"{name}_count_next"][0])
