@@ -11,13 +11,16 @@ from .api import (  # noqa: F401
     Context,
     DDAGPUError,
     RandomEllipsoid,
+    StateFile,
     build,
     fixed_rotation,
     lib,
     library_path,
     mc_rotations,
     num_angles,
+    sample_loop,
 )
 
-__all__ = ["Agglomerate", "Context", "BatchConfig", "DDAGPUError", "RandomEllipsoid", "build", "lib", "library_path",
-           "mc_rotations", "fixed_rotation", "num_angles"]
+__all__ = ["Agglomerate", "BatchConfig", "Context", "DDAGPUError", "RandomEllipsoid", "StateFile",
+           "build", "fixed_rotation", "lib", "library_path", "mc_rotations", "num_angles",
+           "sample_loop"]

@@ -95,6 +95,12 @@ def lib():
                                                 C.POINTER(BatchInfo)]
         L.ddagpu_agglomerate_solves.argtypes = [_p, C.POINTER(_BatchCfg), _i, _p, _p, _p, _p, _p,
                                                 _p, _p, C.POINTER(BatchInfo)]
+        L.ddagpu_state_read.argtypes = [C.c_char_p, _i, _i, C.POINTER(_i), C.POINTER(_f),
+                                        C.POINTER(_f), _p]
+        L.ddagpu_state_write.argtypes = [C.c_char_p, _i, _f, _f, _i, _p]
+        L.ddagpu_state_accumulate.argtypes = [_i, _p, _p, _i, _p, C.POINTER(_i), C.POINTER(_f),
+                                              C.POINTER(_f), _p]
+        L.ddagpu_write_dat.argtypes = [C.c_char_p, _i, _f, _f, _i, _f, _f, _p]
         L.ddagpu_num_angles.argtypes = [_f, _f, _f]
         L.ddagpu_mc_rotations.argtypes = [C.c_ulonglong, _i, _i, _p]
         L.ddagpu_fixed_rotation.argtypes = [_d, _d, _d, _p]
@@ -237,6 +243,70 @@ class RandomEllipsoid:
         sd = self.seeds(grid, b_a, c_a, int(np.sum(seeds_per_material)))
         occ, nd = self.fill(grid, b_a, c_a, sd, seeds_per_material, device)
         return occ, nd, sd
+
+
+class StateFile:
+    """The sample loop's .dst state in the reference's float layout (main.cpp:214-274,
+    961-981): sample counter, float sums of Cabs, Cext and the Mueller matrices."""
+
+    def __init__(self, path: str, n_angles: int, restart: bool = False):
+        self.path, self.n_angles = os.fspath(path), int(n_angles)
+        self.mueller = np.zeros((self.n_angles, 4, 4), np.float32)
+        c, a, e = _i(0), _f(0), _f(0)
+        _check(lib().ddagpu_state_read(self.path.encode(), self.n_angles, int(restart), C.byref(c),
+                                       C.byref(a), C.byref(e), _ptr(self.mueller)))
+        self.counter, self.cabs, self.cext = c.value, a.value, e.value
+
+    def add(self, result: dict) -> None:
+        """Accumulate the samples of one batched call (orientation_solves,
+        realization_solves, agglomerate_solves), in order."""
+        ca = np.ascontiguousarray(result["cabs"], np.float64)
+        ce = np.ascontiguousarray(result["cext"], np.float64)
+        mm = np.ascontiguousarray(result["mueller"], np.float64)
+        c, a, e = _i(self.counter), _f(self.cabs), _f(self.cext)
+        _check(lib().ddagpu_state_accumulate(len(ca), _ptr(ca), _ptr(ce), self.n_angles, _ptr(mm),
+                                             C.byref(c), C.byref(a), C.byref(e),
+                                             _ptr(self.mueller)))
+        self.counter, self.cabs, self.cext = c.value, a.value, e.value
+
+    def save(self) -> None:
+        _check(lib().ddagpu_state_write(self.path.encode(), self.counter, self.cabs, self.cext,
+                                        self.n_angles, _ptr(self.mueller)))
+
+    def write_dat(self, path: str, theta_min: float = 0.0, theta_step: float = 10.0) -> None:
+        """The .dat of main.cpp:1085-1118 (averages over the counter)."""
+        _check(lib().ddagpu_write_dat(os.fspath(path).encode(), self.counter, self.cabs, self.cext,
+                                      self.n_angles, theta_min, theta_step, _ptr(self.mueller)))
+
+
+def sample_loop(ctx, cfg, samples: int, state_path: str, dat_path: str | None = None,
+                orientation: str = "fixed", seed: int = 1, psi: float = 0.0, iota: float = 0.0,
+                kappa: float = 0.0, restart: bool = False, batch: int | None = None):
+    """The reference's sample loop for one worker (main.cpp:214-320, 689-986, 1085-1118)
+    over the batched GPU solves: open or create the state, solve the samples still missing
+    (samples - counter) in batches, refresh the state after every batch and write the .dat.
+    Like the reference, a resumed run numbers its samples after the stored ones but
+    restarts the worker's random stream (main.cpp:803-804), so its Monte-Carlo draws
+    repeat those of the first run."""
+    na = num_angles(cfg.theta_min, cfg.theta_max, cfg.theta_step)
+    st = StateFile(state_path, na, restart)
+    tasks = max(samples - st.counter, 0)
+    if orientation == "mc":
+        rot = mc_rotations(seed, tasks) if tasks else np.zeros((0, 3, 3))
+    elif orientation == "fixed":
+        rot = np.repeat(fixed_rotation(psi, iota, kappa)[None], tasks, axis=0)
+    else:
+        raise ValueError("orientation must be 'fixed' or 'mc'")
+    per = batch or max(ctx.max_rhs // 2, 1)
+    first = True
+    for s0 in range(0, tasks, per):
+        c = cfg if first else BatchConfig(**{**cfg.__dict__, "occ": None})
+        st.add(ctx.orientation_solves(c, rot[s0:s0 + per]))
+        st.save()
+        first = False
+    if dat_path is not None and st.counter > 0:
+        st.write_dat(dat_path, cfg.theta_min, cfg.theta_step)
+    return st
 
 
 @dataclass

@@ -25,14 +25,21 @@
 using namespace ddagpu;
 
 namespace {
-
 thread_local std::string g_err;
+}
 
-int fail(int code, const std::string &msg)
+namespace ddagpu {
+// the message behind ddagpu_last_error for the calling thread (also used by state.cpp)
+int set_error(int code, const std::string &msg)
 {
     g_err = msg;
     return code;
 }
+}  // namespace ddagpu
+
+namespace {
+
+int fail(int code, const std::string &msg) { return set_error(code, msg); }
 
 #define CK(expr)                                                                            \
     do {                                                                                    \

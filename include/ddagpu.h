@@ -221,6 +221,28 @@ int ddagpu_random_ellipsoid_fill(int device, int i_max, int j_max, int l_max, fl
                                  const float *seeds, const int *seeds_per_material, int n_mat,
                                  signed char *occ, int *ndip);
 
+/* ---------------------------------------------------------------- state and result files
+ * The sample loop's files in the float build's layout.  .dst: int counter, float Cabs and
+ * Cext sums, n_angles x 16 float Mueller sums (main.cpp:214-274, 961-981); .dat: the sums
+ * divided by the counter in the reference's text format (main.cpp:1085-1118).  I/O
+ * failures return DDAGPU_EINVAL with the reason (the reference exits with codes 2 and 4). */
+
+/* Open the state like main.cpp:214-274: restart != 0 removes it first; a missing file is
+ * created with a zero state; the state is then read back into the outputs. */
+int ddagpu_state_read(const char *path, int n_angles, int restart, int *counter, float *cabs,
+                      float *cext, float *mueller);
+/* Rewrite the state from its first byte and flush (main.cpp:966-981). */
+int ddagpu_state_write(const char *path, int counter, float cabs, float cext, int n_angles,
+                       const float *mueller);
+/* Add n finished samples, in order, to the float sums and the counter (main.cpp:961-966):
+ * cabs[n], cext[n], mueller[n][n_angles][16] as returned by the batched solves. */
+int ddagpu_state_accumulate(int n, const double *cabs, const double *cext, int n_angles,
+                            const double *mueller, int *counter, float *cabs_sum,
+                            float *cext_sum, float *mueller_sum);
+/* Write the .dat (main.cpp:1085-1118); theta_min / theta_step in degrees. */
+int ddagpu_write_dat(const char *path, int counter, float cabs, float cext, int n_angles,
+                     float theta_min, float theta_step, const float *mueller);
+
 /* Fixed orientation (degrees), main.cpp:516-541. */
 int ddagpu_fixed_rotation(double psi, double iota, double kappa, double *rot);
 
