@@ -254,6 +254,11 @@ def main():
         sums["cext"] += float(r["cext"].sum())
         m = r["mueller"].sum(axis=0)
         sums["mueller"] = m if sums["mueller"] is None else sums["mueller"] + m
+    # the job's one exchange: the sums over every rank's samples (dda_fft_b200.shard)
+    from dda_fft_b200.shard import reduce_sums
+    job = reduce_sums({"count": K * B, "cabs": sums["cabs"], "cext": sums["cext"],
+                       "mueller": sums["mueller"]}, sums["mueller"].shape[0],
+                      device=f"cuda:{dev}")
     e1.record(stream)
     barrier()
     clocks = clk.stop()
@@ -361,7 +366,8 @@ def main():
             "cpu_baseline": cpu,
             "clocks": clocks,
             "gpu_launches": launches,
-            "check": {"cext_mean": sums["cext"] / (K * B), "cabs_mean": sums["cabs"] / (K * B)},
+            "check": {"cext_mean": job["cext"] / job["count"], "cabs_mean": job["cabs"] / job["count"],
+                      "samples": job["count"]},
         }
         print(json.dumps(line), flush=True)
     ctx.close()
