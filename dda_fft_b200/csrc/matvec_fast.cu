@@ -169,7 +169,7 @@ __global__ void __launch_bounds__(NT) k1f(MatvecArgs a)
 // CTA (spectral row js, TL spectral columns): forward x (both halves), 3x3 product,
 // inverse x, in place.  Shared B[c][h][pos][t].
 template <int NI, int TL>
-__global__ void __launch_bounds__(Sp<NI>::RM * TL, NI == 128 ? 2 : 1) k2f(MatvecArgs a)
+__global__ void __launch_bounds__(Sp<NI>::RM * TL, NI == 16 ? 6 : 2) k2f(MatvecArgs a)
 {
     using S = Sp<NI>;
     constexpr int R1 = S::R1, R2 = S::R2, RM = S::RM;
@@ -205,15 +205,11 @@ __global__ void __launch_bounds__(Sp<NI>::RM * TL, NI == 128 ? 2 : 1) k2f(Matvec
             }
         }
     } else if (sub < R2) {
-#pragma unroll 1
-        for (int c = 0; c < 3; c++) {
-            float2 v[R1], w[R1];
+        // step A of one component from its R1 loaded values
+        auto step_a = [&](int c, float2 (&v)[R1]) {
+            float2 w[R1];
 #pragma unroll
-            for (int r = 0; r < R1; r++) {
-                const int i = sub + R2 * r;
-                v[r] = base[c * cstr + i * plane];
-                w[r] = cmul(v[r], __ldg(&hw[i]));
-            }
+            for (int r = 0; r < R1; r++) w[r] = cmul(v[r], __ldg(&hw[sub + R2 * r]));
             dft_reg<R1, false>(v);
             dft_reg<R1, false>(w);
 #pragma unroll
@@ -221,6 +217,28 @@ __global__ void __launch_bounds__(Sp<NI>::RM * TL, NI == 128 ? 2 : 1) k2f(Matvec
                 const float2 tk = k1 ? twid<false>(tw, sub * k1) : make_float2(1.f, 0.f);
                 Bat(c, 0, sub + R2 * k1) = k1 ? cmul(v[k1], tk) : v[k1];
                 Bat(c, 1, sub + R2 * k1) = k1 ? cmul(w[k1], tk) : w[k1];
+            }
+        };
+        if constexpr (3 * R1 <= 24) {
+            // all three components' loads in flight before any arithmetic
+            float2 v0[R1], v1[R1], v2[R1];
+#pragma unroll
+            for (int r = 0; r < R1; r++) {
+                const size_t o = (size_t)(sub + R2 * r) * plane;
+                v0[r] = base[o];
+                v1[r] = base[cstr + o];
+                v2[r] = base[2 * cstr + o];
+            }
+            step_a(0, v0);
+            step_a(1, v1);
+            step_a(2, v2);
+        } else {
+#pragma unroll 1
+            for (int c = 0; c < 3; c++) {
+                float2 v[R1];
+#pragma unroll
+                for (int r = 0; r < R1; r++) v[r] = base[c * cstr + (size_t)(sub + R2 * r) * plane];
+                step_a(c, v);
             }
         }
     }
