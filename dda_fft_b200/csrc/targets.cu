@@ -370,6 +370,9 @@ int anthrax_place(unsigned long long *state, int ni, float radius, float length,
     const float R = (float)((double)(float)ni / 2.), R2 = (R - radius) * (R - radius);
     std::vector<Worm> w;
     w.reserve((size_t)count);
+    // placed monomers' axes, starts and radii, structure of arrays
+    std::vector<float> nx_, ny_, nz_, bx_, by_, bz_, r_;
+    std::vector<unsigned char> cand_;
     unsigned long long s = *state;
     long long tries = 0;
     int l = 0;
@@ -388,11 +391,39 @@ int anthrax_place(unsigned long long *state, int ni, float radius, float length,
             const float th2 = std::acos(r0);
             c = make_worm(r1, th1, ph1, r2, th2, ph2, length, radius, R2);
         }
-        for (size_t j = 0; j < w.size(); j++) {
-            l = cross_two_worms(c, w[j]);
-            if (l == 1) break;
+        // The reference tests the candidate against every placed monomer with
+        // CrossTwoWorms and rejects it on the first crossing.  The first steps of that test
+        // -- the axis cross product, the parallel-axes rule and the line-distance exit
+        // (d > r_a + r_b returns 0) -- are evaluated here for all placed monomers at once,
+        // with the same float operations in the same order (a loop the compiler
+        // vectorises); the full test then runs only on the pairs that pass them, in order.
+        if (!w.empty()) {
+            const size_t nw = w.size();
+            const float cnx = c.n.x, cny = c.n.y, cnz = c.n.z, cbx = c.b.x, cby = c.b.y, cbz = c.b.z;
+            for (size_t j = 0; j < nw; j++) {
+                const float vx = cny * nz_[j] - cnz * ny_[j], vy = cnz * nx_[j] - cnx * nz_[j],
+                            vz = cnx * ny_[j] - cny * nx_[j];
+                const float r0 = std::sqrt(vx * vx + vy * vy + vz * vz);
+                const float ux = bx_[j] - cbx, uy = by_[j] - cby, uz = bz_[j] - cbz;
+                const float dd = std::fabs((ux * vx + uy * vy + uz * vz) / r0);
+                const float r2 = c.r + r_[j];
+                cand_[j] = ((double)r0 <= 1.e-20) | !(dd > r2);
+            }
+            l = 0;
+            for (size_t j = 0; j < nw && !l; j++)
+                if (cand_[j]) l = cross_two_worms(c, w[j]);
         }
-        if (l == 0) w.push_back(c);
+        if (l == 0) {
+            w.push_back(c);
+            nx_.push_back(c.n.x);
+            ny_.push_back(c.n.y);
+            nz_.push_back(c.n.z);
+            bx_.push_back(c.b.x);
+            by_.push_back(c.b.y);
+            bz_.push_back(c.b.z);
+            r_.push_back(c.r);
+            cand_.push_back(0);
+        }
     }
     *state = s;
     for (int k = 0; k < count; k++) {
