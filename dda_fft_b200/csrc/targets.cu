@@ -168,40 +168,78 @@ __device__ bool seed_to_worm(const DW &w, float px, float py, float pz)
 }
 
 constexpr int kChunk = 256;
+constexpr int kTile = 8;   // rasterisation tile: 8 x 8 x 8 cells per CTA, two cells per thread
 
+// One CTA per lattice tile.  The monomers pass through shared memory in chunks; a monomer
+// is tested against the tile's cells only if its box, widened by its radius and one cell,
+// meets the tile's box (SeedToWorm can only accept points within the radius of the axis
+// segment, so the skipped tests are all rejections).  A cell is filled if any monomer
+// accepts it, as in the reference's loop (particle.cpp:65-80), so the test order is free.
 __global__ void __launch_bounds__(256) rasterize(const DW *worms, int count, int ni, int nj, int nl,
                                                  float cx, float cy, float cz, float R2,
                                                  signed char *occ, int *ndip)
 {
     __shared__ DW sw[kChunk];
-    __shared__ int block_hits;
-    const size_t N = (size_t)ni * nj * nl;
-    const size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    __shared__ short surv[kChunk];
+    __shared__ int nsurv, block_hits;
+    const int tiles_l = (nl + kTile - 1) / kTile, tiles_j = (nj + kTile - 1) / kTile;
+    const int t = blockIdx.x;
+    const int i0 = (t / (tiles_l * tiles_j)) * kTile, j0 = ((t / tiles_l) % tiles_j) * kTile,
+              l0 = (t % tiles_l) * kTile;
     if (threadIdx.x == 0) block_hits = 0;
-    float px = 0.f, py = 0.f, pz = 0.f;
-    bool inside = false;
-    if (q < N) {
-        const int l = (int)(q % nl), j = (int)((q / nl) % nj), i = (int)(q / ((size_t)nl * nj));
-        px = fs((float)i, cx);
-        py = fs((float)j, cy);
-        pz = fs((float)l, cz);
-        inside = fa(fa(fm(px, px), fm(py, py)), fm(pz, pz)) <= R2;
+    // this thread's cells: tile-local indices threadIdx.x and threadIdx.x + 256
+    float px[2], py[2], pz[2];
+    bool valid[2], inside[2], hit[2];
+#pragma unroll
+    for (int u = 0; u < 2; u++) {
+        const int e = threadIdx.x + 256 * u;
+        const int i = i0 + e / (kTile * kTile), j = j0 + (e / kTile) % kTile, l = l0 + e % kTile;
+        valid[u] = i < ni && j < nj && l < nl;
+        px[u] = fs((float)i, cx);
+        py[u] = fs((float)j, cy);
+        pz[u] = fs((float)l, cz);
+        inside[u] = valid[u] && fa(fa(fm(px[u], px[u]), fm(py[u], py[u])), fm(pz[u], pz[u])) <= R2;
+        hit[u] = false;
     }
-    bool hit = false;
+    // the tile's box in point coordinates
+    const float xlo = fs((float)i0, cx), ylo = fs((float)j0, cy), zlo = fs((float)l0, cz);
+    const float xhi = fs((float)min(i0 + kTile - 1, ni - 1), cx), yhi = fs((float)min(j0 + kTile - 1, nj - 1), cy),
+                zhi = fs((float)min(l0 + kTile - 1, nl - 1), cz);
     for (int c0 = 0; c0 < count; c0 += kChunk) {
         __syncthreads();
-        for (int k = threadIdx.x; k < kChunk && c0 + k < count; k += blockDim.x) sw[k] = worms[c0 + k];
-        __syncthreads();
+        if (threadIdx.x == 0) nsurv = 0;
         const int m = count - c0 < kChunk ? count - c0 : kChunk;
-        if (inside && !hit)
-            for (int k = 0; k < m; k++)
-                if (seed_to_worm(sw[k], px, py, pz)) {
-                    hit = true;
-                    break;
-                }
+        for (int k = threadIdx.x; k < m; k += blockDim.x) sw[k] = worms[c0 + k];
+        __syncthreads();
+        if (threadIdx.x < m) {
+            const DW &w = sw[threadIdx.x];
+            const float g = w.r + 1.f;
+            const bool meet = fminf(w.bx, w.ex) - g <= xhi && fmaxf(w.bx, w.ex) + g >= xlo &&
+                              fminf(w.by, w.ey) - g <= yhi && fmaxf(w.by, w.ey) + g >= ylo &&
+                              fminf(w.bz, w.ez) - g <= zhi && fmaxf(w.bz, w.ez) + g >= zlo;
+            if (meet) surv[atomicAdd(&nsurv, 1)] = (short)threadIdx.x;
+        }
+        __syncthreads();
+        const int ns = nsurv;
+#pragma unroll
+        for (int u = 0; u < 2; u++)
+            if (inside[u] && !hit[u])
+                for (int s = 0; s < ns; s++)
+                    if (seed_to_worm(sw[surv[s]], px[u], py[u], pz[u])) {
+                        hit[u] = true;
+                        break;
+                    }
     }
-    if (q < N) occ[q] = hit ? 1 : 0;
-    if (hit) atomicAdd(&block_hits, 1);
+    int mine = 0;
+#pragma unroll
+    for (int u = 0; u < 2; u++) {
+        if (!valid[u]) continue;
+        const int e = threadIdx.x + 256 * u;
+        const int i = i0 + e / (kTile * kTile), j = j0 + (e / kTile) % kTile, l = l0 + e % kTile;
+        occ[((size_t)i * nj + j) * nl + l] = hit[u] ? 1 : 0;
+        mine += hit[u] ? 1 : 0;
+    }
+    if (mine) atomicAdd(&block_hits, mine);
     __syncthreads();
     if (threadIdx.x == 0 && block_hits) atomicAdd(ndip, block_hits);
 }
@@ -455,9 +493,9 @@ cudaError_t anthrax_rasterize(const float *cyl13, int count, int ni, int nj, int
         const float cx = (float)((double)(float)ni / 2. - .5),
                     cy = (float)((double)(float)nj / 2. - .5),
                     cz = (float)((double)(float)nl / 2. - .5);
-        const size_t N = (size_t)ni * nj * nl;
-        rasterize<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(d, count, ni, nj, nl, cx, cy, cz,
-                                                              R * R, occ_dev, ndip_dev);
+        const unsigned tiles = (unsigned)(((ni + kTile - 1) / kTile) * ((nj + kTile - 1) / kTile) *
+                                          ((nl + kTile - 1) / kTile));
+        rasterize<<<tiles, 256, 0, st>>>(d, count, ni, nj, nl, cx, cy, cz, R * R, occ_dev, ndip_dev);
         e = cudaGetLastError();
     }
     cudaFreeAsync(d, st);
