@@ -15,6 +15,7 @@
 // reference.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
@@ -99,8 +100,11 @@ int point_to_worm(const Worm &w, V3 p, float radius)
     return d > max_d ? 0 : 1;
 }
 
-// CrossTwoWorms, particle.cpp:233-300 (including its reuse of the nearest point)
-int cross_two_worms(const Worm &a, const Worm &b)
+// CrossTwoWorms, particle.cpp:233-300, up to its first decision that needs no point test:
+// 1 / 0 for the parallel-axes rule, the line-distance exit and the "nearest points inside
+// both segments" rule (its 2x2 system, signs included); -1 otherwise, with the two line
+// parameters in r0_out / r1_out.
+int cross_head(const Worm &a, const Worm &b, float &r0_out, float &r1_out)
 {
     const V3 v0 = vcross(a.n, b.n);
     float r0 = vabs(v0);
@@ -115,6 +119,17 @@ int cross_two_worms(const Worm &a, const Worm &b)
     r0 = (b1 * a22 - b2 * a12) / r2;
     const float r1 = (b2 * a11 - b1 * a21) / r2;
     if (r0 >= 0.f && r0 <= a.l && r1 >= 0.f && r1 <= b.l) return 1;
+    r0_out = r0;
+    r1_out = r1;
+    return -1;
+}
+
+// CrossTwoWorms, particle.cpp:233-300 (including its reuse of the nearest point)
+int cross_two_worms(const Worm &a, const Worm &b)
+{
+    float r0 = 0.f, r1 = 0.f;
+    const int h = cross_head(a, b, r0, r1);
+    if (h >= 0) return h;
     V3 near = {0.f, 0.f, 0.f};
     int i0 = 0, i1 = 0;
     if (r0 >= 0.f && r0 <= a.l) {
@@ -408,8 +423,9 @@ int anthrax_place(unsigned long long *state, int ni, float radius, float length,
     const float R = (float)((double)(float)ni / 2.), R2 = (R - radius) * (R - radius);
     std::vector<Worm> w;
     w.reserve((size_t)count);
-    // placed monomers' axes, starts and radii, structure of arrays
+    // placed monomers' axes, starts, radii, midpoints and reach (half length + radius)
     std::vector<float> nx_, ny_, nz_, bx_, by_, bz_, r_;
+    std::vector<double> mx_, my_, mz_, reach_;
     std::vector<unsigned char> cand_;
     unsigned long long s = *state;
     long long tries = 0;
@@ -430,26 +446,42 @@ int anthrax_place(unsigned long long *state, int ni, float radius, float length,
             c = make_worm(r1, th1, ph1, r2, th2, ph2, length, radius, R2);
         }
         // The reference tests the candidate against every placed monomer with
-        // CrossTwoWorms and rejects it on the first crossing.  The first steps of that test
-        // -- the axis cross product, the parallel-axes rule and the line-distance exit
-        // (d > r_a + r_b returns 0) -- are evaluated here for all placed monomers at once,
-        // with the same float operations in the same order (a loop the compiler
-        // vectorises); the full test then runs only on the pairs that pass them, in order.
+        // CrossTwoWorms and rejects it on the first crossing; only that yes / no matters.
+        // Here, chunk by chunk of placed monomers: (1) the parallel-axes rule and the
+        // line-distance exit of the test, with the same float operations, for the whole
+        // chunk (a branch-free loop); (2) for the pairs left, the rest of the test up to the
+        // "nearest points inside both segments" rule (cross_head); (3) the point tests only
+        // for pairs whose segments lie within r_a + r_b + 1 cell -- for every other pair
+        // each point test measures a distance beyond its threshold by more than a cell,
+        // far above float rounding, so it returns 0 and the pair's answer is cross_head's.
         if (!w.empty()) {
             const size_t nw = w.size();
             const float cnx = c.n.x, cny = c.n.y, cnz = c.n.z, cbx = c.b.x, cby = c.b.y, cbz = c.b.z;
-            for (size_t j = 0; j < nw; j++) {
-                const float vx = cny * nz_[j] - cnz * ny_[j], vy = cnz * nx_[j] - cnx * nz_[j],
-                            vz = cnx * ny_[j] - cny * nx_[j];
-                const float r0 = std::sqrt(vx * vx + vy * vy + vz * vz);
-                const float ux = bx_[j] - cbx, uy = by_[j] - cby, uz = bz_[j] - cbz;
-                const float dd = std::fabs((ux * vx + uy * vy + uz * vz) / r0);
-                const float r2 = c.r + r_[j];
-                cand_[j] = ((double)r0 <= 1.e-20) | !(dd > r2);
-            }
+            const double mx = 0.5 * ((double)c.b.x + c.e.x), my = 0.5 * ((double)c.b.y + c.e.y),
+                         mz = 0.5 * ((double)c.b.z + c.e.z), reach = 0.5 * (double)c.l + c.r + 1.0;
             l = 0;
-            for (size_t j = 0; j < nw && !l; j++)
-                if (cand_[j]) l = cross_two_worms(c, w[j]);
+            for (size_t j0 = 0; j0 < nw && !l; j0 += 256) {
+                const size_t j1 = std::min(nw, j0 + 256);
+                for (size_t j = j0; j < j1; j++) {
+                    const float vx = cny * nz_[j] - cnz * ny_[j], vy = cnz * nx_[j] - cnx * nz_[j],
+                                vz = cnx * ny_[j] - cny * nx_[j];
+                    const float r0 = std::sqrt(vx * vx + vy * vy + vz * vz);
+                    const float ux = bx_[j] - cbx, uy = by_[j] - cby, uz = bz_[j] - cbz;
+                    const float dd = std::fabs((ux * vx + uy * vy + uz * vz) / r0);
+                    cand_[j] = ((double)r0 <= 1.e-20) | !(dd > c.r + r_[j]);
+                }
+                for (size_t j = j0; j < j1 && !l; j++) {
+                    if (!cand_[j]) continue;
+                    const double dx = mx - mx_[j], dy = my - my_[j], dz = mz - mz_[j],
+                                 rr = reach + reach_[j];
+                    if (dx * dx + dy * dy + dz * dz <= rr * rr) {
+                        l = cross_two_worms(c, w[j]);
+                    } else {
+                        float q0, q1;
+                        l = cross_head(c, w[j], q0, q1) == 1;
+                    }
+                }
+            }
         }
         if (l == 0) {
             w.push_back(c);
@@ -460,6 +492,10 @@ int anthrax_place(unsigned long long *state, int ni, float radius, float length,
             by_.push_back(c.b.y);
             bz_.push_back(c.b.z);
             r_.push_back(c.r);
+            mx_.push_back(0.5 * ((double)c.b.x + c.e.x));
+            my_.push_back(0.5 * ((double)c.b.y + c.e.y));
+            mz_.push_back(0.5 * ((double)c.b.z + c.e.z));
+            reach_.push_back(0.5 * (double)c.l + c.r);
             cand_.push_back(0);
         }
     }
