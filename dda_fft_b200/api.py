@@ -115,6 +115,9 @@ def lib():
         L.ddagpu_set_kernels.argtypes = [_p, _i]
         L.ddagpu_farfield_noalloc.argtypes = [_i, _i, _i, _i, _f, _p, _p, _p, _i, _p, _p, _p]
         L.ddagpu_get_kernels.argtypes = [_p]
+        L.ddagpu_set_solver_graph.argtypes = [_p, _i]
+        L.ddagpu_solver_graph_runs.argtypes = [_p]
+        L.ddagpu_solver_graph_runs.restype = C.c_longlong
         L.ddagpu_rng_seed.argtypes = [C.c_ulonglong, _i]
         L.ddagpu_rng_seed.restype = C.c_ulonglong
         L.ddagpu_anthrax_count.argtypes = [_i, _i, _i, _f, _f, _f]
@@ -541,6 +544,14 @@ class Context:
 
     def set_tiling(self, tile_x=0, rows_g=0):
         _check(lib().ddagpu_set_tiling(self._h, tile_x, rows_g))
+
+    def set_solver_graph(self, on: bool):
+        """Iterations 2..Max_Step of each solve as one CUDA graph launch (default on)."""
+        _check(lib().ddagpu_set_solver_graph(self._h, int(on)))
+
+    @property
+    def solver_graph_runs(self) -> int:
+        return int(lib().ddagpu_solver_graph_runs(self._h))
 
     def set_kernels(self, fast: bool):
         _check(lib().ddagpu_set_kernels(self._h, int(fast)))

@@ -102,6 +102,22 @@ struct ddagpu_ctx {
     size_t occ_stride = 0;          // N while occ_b is in use, 0 otherwise
     int occ_nmat1 = 0, occ_nact = 0;
     long long launches = 0;      // kernels launched by this context
+    // solver iterations 2.. as one CUDA graph: a conditional while node whose body is one
+    // iteration, its step counter on the device (kept per context, rebuilt when the solve's
+    // shape changes)
+    int graph_on = 1;
+    int *step_dev = nullptr;
+    struct GraphKey {
+        int solver, nrhs, max_step, nmat1, fast, tile_x, rows_g, tlen;
+        float tau;
+        double d0;
+        size_t occ_stride;
+        const void *trace, *occ;
+    } gkey{};
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    long long g_per_iter = 0;    // kernels in one recorded iteration
+    long long graph_runs = 0;    // graph launches by this context
     std::mutex mu;
 };
 
@@ -314,55 +330,148 @@ int run_solver(ddagpu_ctx *c, int nrhs, int solver, float tau, int max_step, flo
     res.matvec_it = (solver == 1 || solver == 2) ? 2 : 1;
 
     // ---- iterations (dda_func.cpp:1301-1535)
-    std::vector<int> act((size_t)nrhs);
-    for (int o = 1; o <= max_step; o++) {
-        CK(scal(SC_TOP, o));
-        CK(launch_gated_copy(F, 0, st));   // p -> p_min where this step improved
-        c->launches += 1;
-        CK(cudaMemcpyAsync(act.data(), c->active, nrhs * sizeof(int), cudaMemcpyDeviceToHost, st));
-        CK(cudaStreamSynchronize(st));
-        bool any = false;
-        for (int k = 0; k < nrhs; k++) any = any || act[(size_t)k];
-        if (!any) break;
+    // top of an iteration: convergence test, best-iterate bookkeeping and copy
+    auto top = [&](int o, const int *sdev) -> int {
+        c->launches += 2;
+        CK(launch_scalar(c->state, c->active, c->active, nrhs, SC_TOP, o, trace, tlen, st, sdev));
+        CK(launch_gated_copy(F, 0, st));
+        return DDAGPU_OK;
+    };
+    // the solver's recurrences of one iteration (gated per right-hand side by its flag)
+    auto body = [&](int o, const int *sdev) -> int {
+        auto sc = [&](int stage) {
+            c->launches += 1;
+            return launch_scalar(c->state, c->active, c->active, nrhs, stage, o, trace, tlen, st, sdev);
+        };
         switch (solver) {
         case 0:
             if (o == 1) CK(field(OP_COPY_RS));
             CK(matvec(c->s, c->w, 1.f, c->s, 0));
             CK(field(OP_CG1));
-            CK(scal(SC_CG1, o));
+            CK(sc(SC_CG1));
             CK(field(OP_CG2));
-            CK(scal(SC_CG2, o));
+            CK(sc(SC_CG2));
             CK(field(OP_CG3));
             break;
         case 1:
             CK(matvec(c->s, c->w, 1.f, c->s, 0));
             CK(field(OP_AA1));
-            CK(scal(SC_AA1, o));
+            CK(sc(SC_AA1));
             CK(field(OP_AA2));
-            CK(scal(SC_AA2, o));
+            CK(sc(SC_AA2));
             CK(matvec(c->r, c->w, 1.f, c->r, 1));
             CK(field(OP_AA3));
             break;
         case 2:
             CK(field(OP_B_RHO));
-            CK(scal(SC_B1, o));
+            CK(sc(SC_B1));
             CK(field(OP_B_S));
             CK(matvec(c->s, c->h, 1.f, c->s, 0));
             CK(field(OP_B_GH));
-            CK(scal(SC_B2, o));
+            CK(sc(SC_B2));
             CK(field(OP_B_R));
             CK(matvec(c->r, c->w, 1.f, c->r, 0));
             CK(field(OP_B_WW));
-            CK(scal(SC_B3, o));
+            CK(sc(SC_B3));
             CK(field(OP_B_P));
-            CK(scal(SC_B4, o));
+            CK(sc(SC_B4));
             break;
         case 3:
             CK(matvec(c->p, c->w, 1.f, c->p, 0));
             CK(field(OP_SIMPLE));
-            CK(scal(SC_ERR1, o));
+            CK(sc(SC_ERR1));
             break;
         }
+        return DDAGPU_OK;
+    };
+    // iteration 1 (and all of them without the graph) from the host: the loop stops when
+    // no right-hand side is left active (read back once per iteration)
+    const bool use_graph = c->graph_on && max_step >= 2;
+    std::vector<int> act((size_t)nrhs);
+    int o = 1;
+    for (; o <= (use_graph ? 1 : max_step); o++) {
+        RET(top(o, nullptr));
+        CK(cudaMemcpyAsync(act.data(), c->active, nrhs * sizeof(int), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        bool any = false;
+        for (int k = 0; k < nrhs; k++) any = any || act[(size_t)k];
+        if (!any) break;
+        RET(body(o, nullptr));
+    }
+    if (use_graph && o == 2) {
+        // iterations 2..Max_Step: one graph launch; each pass of the while body is one
+        // iteration and its last kernel decides whether another follows
+        ddagpu_ctx::GraphKey key{};
+        key.solver = solver;
+        key.nrhs = nrhs;
+        key.max_step = max_step;
+        key.nmat1 = nmat1;
+        key.fast = c->fast;
+        key.tile_x = c->tile_x;
+        key.rows_g = c->rows_g;
+        key.tlen = tlen;
+        key.tau = tau;
+        key.d0 = d0;
+        key.occ_stride = c->occ_stride;
+        key.trace = trace;
+        key.occ = c->occ_stride ? (const void *)c->occ_b : (const void *)c->occ;
+        if (!c->gexec || std::memcmp(&key, &c->gkey, sizeof key) != 0) {
+            if (c->gexec) cudaGraphExecDestroy(c->gexec);
+            if (c->graph) cudaGraphDestroy(c->graph);
+            c->gexec = nullptr;
+            c->graph = nullptr;
+            cudaGraph_t g = nullptr;
+            CK(cudaGraphCreate(&g, 0));
+            cudaGraphConditionalHandle h;
+            cudaError_t e = cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault);
+            cudaGraphNodeParams np{};
+            np.type = cudaGraphNodeTypeConditional;
+            np.conditional.handle = h;
+            np.conditional.type = cudaGraphCondTypeWhile;
+            np.conditional.size = 1;
+            cudaGraphNode_t node;
+            if (e == cudaSuccess) e = cudaGraphAddNode(&node, g, nullptr, 0, &np);
+            if (e == cudaSuccess)
+                e = cudaStreamBeginCaptureToGraph(st, np.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                                  cudaStreamCaptureModeThreadLocal);
+            if (e != cudaSuccess) {
+                cudaGraphDestroy(g);
+                return fail(DDAGPU_ECUDA, std::string("solver graph: ") + cudaGetErrorString(e));
+            }
+            const long long l0 = c->launches;
+            int rc = top(0, c->step_dev);
+            if (rc == DDAGPU_OK) rc = body(0, c->step_dev);
+            cudaError_t le = rc == DDAGPU_OK
+                                 ? launch_loop_control(c->active, nrhs, c->step_dev, max_step, h, st)
+                                 : cudaSuccess;
+            cudaGraph_t captured = nullptr;
+            const cudaError_t ee = cudaStreamEndCapture(st, &captured);
+            c->g_per_iter = c->launches - l0 + 1;
+            c->launches = l0;
+            if (rc != DDAGPU_OK || le != cudaSuccess || ee != cudaSuccess) {
+                cudaGraphDestroy(g);
+                if (rc != DDAGPU_OK) return rc;
+                return fail(DDAGPU_ECUDA, std::string("solver graph capture: ") +
+                                              cudaGetErrorString(le != cudaSuccess ? le : ee));
+            }
+            cudaGraphExec_t x = nullptr;
+            e = cudaGraphInstantiate(&x, g, 0);
+            if (e != cudaSuccess) {
+                cudaGraphDestroy(g);
+                return fail(DDAGPU_ECUDA, std::string("solver graph instantiate: ") + cudaGetErrorString(e));
+            }
+            c->graph = g;
+            c->gexec = x;
+            c->gkey = key;
+        }
+        const int first = 2;
+        CK(cudaMemcpyAsync(c->step_dev, &first, sizeof(int), cudaMemcpyHostToDevice, st));
+        CK(cudaGraphLaunch(c->gexec, st));
+        int last = first;
+        CK(cudaMemcpyAsync(&last, c->step_dev, sizeof(int), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        c->launches += (long long)(last - first) * c->g_per_iter;
+        c->graph_runs += 1;
     }
     // ---- rollback (dda_func.cpp:1537-1548), for every right-hand side
     CK(launch_scalar(c->state, nullptr, nullptr, nrhs, SC_FINAL, 0, nullptr, 0, st));
@@ -504,6 +613,7 @@ int ddagpu_create(ddagpu_ctx **out, int device, int i_max, int j_max, int l_max,
     A(dalloc(&c->state, (size_t)max_rhs));
     A(dalloc(&c->active, (size_t)max_rhs));
     A(dalloc(&c->occ, c->N));
+    A(dalloc(&c->step_dev, 1));
     A(dalloc(&c->mv, (size_t)c->nmat_cap));
     A(dalloc(&c->alpha, (size_t)c->nmat_cap * max_rhs));
     A(dalloc(&c->kinc, (size_t)3 * max_rhs));
@@ -546,11 +656,13 @@ int ddagpu_destroy(ddagpu_ctx *c)
     if (c->b32) cudaFree(c->b32);
     if (c->rb) cudaFree(c->rb);
     if (c->x64) cudaFree(c->x64);
+    if (c->gexec) cudaGraphExecDestroy(c->gexec);
+    if (c->graph) cudaGraphDestroy(c->graph);
     void *ptrs[] = {c->ahat, c->tw,     c->work,   c->p,       c->pmin,   c->r,     c->s,
                     c->w,    c->g,      c->h,      c->state,   c->active, c->trace, c->occ,
                     c->mv,   c->alpha,  c->kinc,   c->einc,    c->ksc,    c->esc_acc,
                     c->cc_acc, c->normals, c->mueller, c->esc, c->cabs,   c->cext,
-                    c->occ_b, c->ndip};
+                    c->occ_b, c->ndip, c->step_dev};
     for (void *q : ptrs)
         if (q) cudaFree(q);
     if (c->st) cudaStreamDestroy(c->st);
@@ -1385,6 +1497,16 @@ int ddagpu_anthrax_rasterize(int device, int i_max, int j_max, int l_max, const 
     if (ndip) *ndip = h;
     return DDAGPU_OK;
 }
+
+int ddagpu_set_solver_graph(ddagpu_ctx *c, int on)
+{
+    if (!c) return fail(DDAGPU_EINVAL, "null context");
+    std::lock_guard<std::mutex> lk(c->mu);
+    c->graph_on = on ? 1 : 0;
+    return DDAGPU_OK;
+}
+
+long long ddagpu_solver_graph_runs(ddagpu_ctx *c) { return c ? c->graph_runs : -1; }
 
 int ddagpu_random_ellipsoid_seeds(unsigned long long *rng_state, int i_max, int j_max, int l_max,
                                   float b_a, float c_a, int n_seeds, float *seeds)

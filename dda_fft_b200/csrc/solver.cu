@@ -282,9 +282,11 @@ __device__ float2 fmul_ref(float2 a, float2 b)
 }
 
 __global__ void scalar_stage(RhsState *st, const int *rhs_active_in, int *rhs_active, int nrhs,
-                             int stage, int step, double *trace, int trace_len)
+                             int stage, int step_arg, const int *step_dev, double *trace,
+                             int trace_len)
 {
     const int rhs = blockIdx.x * blockDim.x + threadIdx.x;
+    const int step = step_dev ? *step_dev : step_arg;
     if (rhs >= nrhs) return;
     RhsState &S = st[rhs];
     const bool run = rhs_active_in ? rhs_active_in[rhs] != 0 : true;
@@ -496,10 +498,38 @@ cudaError_t launch_first_approx(const FieldArgs &a, cudaStream_t st)
 }
 
 cudaError_t launch_scalar(RhsState *st_, const int *act_in, int *act_out, int nrhs, int stage,
-                          int step, double *trace, int trace_len, cudaStream_t st)
+                          int step, double *trace, int trace_len, cudaStream_t st,
+                          const int *step_dev)
 {
-    scalar_stage<<<(nrhs + 127) / 128, 128, 0, st>>>(st_, act_in, act_out, nrhs, stage, step, trace,
-                                                     trace_len);
+    scalar_stage<<<(nrhs + 127) / 128, 128, 0, st>>>(st_, act_in, act_out, nrhs, stage, step, step_dev,
+                                                     trace, trace_len);
+    return cudaGetLastError();
+}
+
+// End of one iteration of a solve recorded in a CUDA graph: advance the device step
+// counter and keep looping while some right-hand side is active and the counter has not
+// passed Max_Step (the host loop's test, dda_func.cpp:1301-1313).
+__global__ void __launch_bounds__(256) loop_control(const int *active, int nrhs, int *step_dev,
+                                                    int max_step, cudaGraphConditionalHandle h)
+{
+    __shared__ int any;
+    if (threadIdx.x == 0) any = 0;
+    __syncthreads();
+    int mine = 0;
+    for (int r = threadIdx.x; r < nrhs; r += blockDim.x) mine |= active[r] != 0;
+    if (mine) atomicOr(&any, 1);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int next = *step_dev + 1;
+        *step_dev = next;
+        cudaGraphSetConditional(h, (any && next <= max_step) ? 1u : 0u);
+    }
+}
+
+cudaError_t launch_loop_control(const int *active, int nrhs, int *step_dev, int max_step,
+                                cudaGraphConditionalHandle h, cudaStream_t st)
+{
+    loop_control<<<1, 256, 0, st>>>(active, nrhs, step_dev, max_step, h);
     return cudaGetLastError();
 }
 

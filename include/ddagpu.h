@@ -209,6 +209,17 @@ int ddagpu_anthrax_place(unsigned long long *rng_state, int i_max, float monomer
 int ddagpu_anthrax_rasterize(int device, int i_max, int j_max, int l_max, const float *monomers,
                              int count, signed char *occ, int *ndip);
 
+/* Solver iterations as a CUDA graph (no counterpart in the reference, whose loop is on
+ * the host, dda_func.cpp:1301-1535).  On (the default), iterations 2..Max_Step of every
+ * solve run as one graph launch: a conditional while node whose body is one iteration
+ * and whose last kernel advances a device step counter and stops the loop when no
+ * right-hand side is active or Max_Step is reached, so the host no longer reads the
+ * active flags back every iteration.  The graph is kept per context and rebuilt when the
+ * solve's shape (solver, right-hand sides, Max_Step, materials, kernels) changes.
+ * Results are the same kernels in the same order as with the host loop. */
+int ddagpu_set_solver_graph(ddagpu_ctx *ctx, int on);
+long long ddagpu_solver_graph_runs(ddagpu_ctx *ctx);   /* graph launches so far */
+
 /* Random (Voronoi) ellipsoids (targets 4 and 5, iGenerateRandomEllipsoid,
  * particle.cpp:531-614): seeds[n_seeds][3] drawn on the host from the reference's random
  * stream (returns DDAGPU_EINVAL if the ellipsoid b/a, c/a does not fit the lattice); then
