@@ -184,7 +184,7 @@ def main():
                     help="only run the matvec on NRHS right-hand sides (for ncu captures)")
     ap.add_argument("--grid", type=int, default=GRID)
     ap.add_argument("--workload", default="orientations",
-                    choices=["orientations", "precision", "adjoint", "realizations"])
+                    choices=["orientations", "precision", "adjoint", "realizations", "plain"])
     args = ap.parse_args()
     if args.profile_matvec:
         return profile_matvec(args)
@@ -192,6 +192,8 @@ def main():
         return precision_run(args)
     if args.workload == "adjoint":
         return adjoint_run(args)
+    if args.workload == "plain":
+        return plain_run(args)
     if args.warmup < 3:
         args.warmup = 3
     if args.workload == "realizations":
@@ -462,6 +464,63 @@ def adjoint_run(args):
                       "grad_norm_re": float(np.linalg.norm(m_re.grad.numpy())),
                       "grad_norm_im": float(np.linalg.norm(m_im.grad.numpy()))}), flush=True)
     G.close()
+
+
+def plain_run(args):
+    """The plain-method mid configuration: 64^3 sphere, x = 8, m = 1.5+0.01i, LDR,
+    BiCGStab, Error_max 1e-3, Max_Step 100, 12 planes, theta 0..180 step 1 (2172
+    directions), fixed orientation: one sample (both polarisations) through the batched
+    entry point, with the solver loop as a CUDA graph and on the host, the matvec on 2
+    right-hand sides, and the reference's own sample loop on one host thread (the
+    configuration has one sample, so one worker)."""
+    import torch
+    import dda_fft_b200 as D
+    n, x, mat = 64, 8.0, (1.5, 0.01)
+    kd = 2 * x / n
+    occ = ellipsoid_occ(n, 1.0, 1.0)
+    cfg = D.BatchConfig(occ=occ, materials=[mat], polarizability=5, solver=2, max_step=100,
+                        err_max=1e-3, nplanes=12, theta_step=1.0)
+    out = {"workload": "plain mid: 64^3 sphere x=8 m=1.5+0.01i LDR BiCGStab 1e-3, 12 planes, "
+                       "2172 directions, one sample"}
+    rot = D.fixed_rotation(0, 0, 0)[None]
+    with D.Context(n, kd, max_rhs=2) as ctx:
+        st = torch.cuda.ExternalStream(ctx.stream_ptr)
+        for graph in (True, False):
+            ctx.set_solver_graph(graph)
+            for _ in range(max(args.warmup, 1)):
+                r = ctx.orientation_solves(cfg, rot)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            reps = max(args.steps, 1)
+            l0 = ctx.kernel_launches
+            e0.record(st)
+            for _ in range(reps):
+                r = ctx.orientation_solves(cfg, rot)
+            e1.record(st)
+            torch.cuda.synchronize()
+            out["graph" if graph else "host_loop"] = {
+                "ms_per_sample": e0.elapsed_time(e1) / reps, "steps": r["max_steps"],
+                "kernels_per_sample": (ctx.kernel_launches - l0) / reps}
+        out["cext"], out["cabs"] = float(r["cext"][0]), float(r["cabs"][0])
+        xx = torch.randn(2, 3, n, n, n, dtype=torch.complex64, device="cuda")
+        yy = torch.empty_like(xx)
+        for _ in range(3):
+            ctx.convolution_dev(xx, yy, 2)
+        g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        g0.record(st)
+        for _ in range(20):
+            ctx.convolution_dev(xx, yy, 2)
+        g1.record(st)
+        torch.cuda.synchronize()
+        mv_ms = g0.elapsed_time(g1) / 20
+        out["matvec_2rhs"] = {"ms": mv_ms, "GBs_algorithmic": matvec_bytes(n, 2) / mv_ms / 1e6}
+    if not args.no_cpu:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import pyoracle as P
+        rc = P.make_run_cfg(grid=n, target=1, x=x, materials=(mat,), polarizability=5, solver=2,
+                            max_step=100, nplanes=12, theta_step=1.0)
+        secs, *_ = P.RefLib().run_samples(rc, 1, 1)
+        out["reference_cpu_s_per_sample"] = secs
+    print(json.dumps(out), flush=True)
 
 
 AGG_SIZES, AGG_N, AGG_R, AGG_LR, AGG_RHO = (32, 64, 128), 64, 3.0, 0.0, 0.25

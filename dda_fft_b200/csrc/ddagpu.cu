@@ -388,19 +388,24 @@ int run_solver(ddagpu_ctx *c, int nrhs, int solver, float tau, int max_step, flo
     // no right-hand side is left active (read back once per iteration)
     const bool use_graph = c->graph_on && max_step >= 2;
     std::vector<int> act((size_t)nrhs);
-    int o = 1;
-    for (; o <= (use_graph ? 1 : max_step); o++) {
+    bool graph_from_2 = false;
+    for (int o = 1; o <= max_step; o++) {
         RET(top(o, nullptr));
         CK(cudaMemcpyAsync(act.data(), c->active, nrhs * sizeof(int), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
         bool any = false;
         for (int k = 0; k < nrhs; k++) any = any || act[(size_t)k];
         if (!any) break;
+        if (use_graph && o == 2) {   // the top of step 2 ran; its body starts the graph
+            graph_from_2 = true;
+            break;
+        }
         RET(body(o, nullptr));
     }
-    if (use_graph && o == 2) {
-        // iterations 2..Max_Step: one graph launch; each pass of the while body is one
-        // iteration and its last kernel decides whether another follows
+    if (graph_from_2) {
+        // iterations 2..Max_Step: one graph launch; a pass of the while body is the
+        // recurrences of one step, then the convergence test of the next step, and its
+        // last kernel decides whether another pass follows
         ddagpu_ctx::GraphKey key{};
         key.solver = solver;
         key.nrhs = nrhs;
@@ -439,14 +444,14 @@ int run_solver(ddagpu_ctx *c, int nrhs, int solver, float tau, int max_step, flo
                 return fail(DDAGPU_ECUDA, std::string("solver graph: ") + cudaGetErrorString(e));
             }
             const long long l0 = c->launches;
-            int rc = top(0, c->step_dev);
-            if (rc == DDAGPU_OK) rc = body(0, c->step_dev);
-            cudaError_t le = rc == DDAGPU_OK
-                                 ? launch_loop_control(c->active, nrhs, c->step_dev, max_step, h, st)
-                                 : cudaSuccess;
+            int rc = body(max_step, c->step_dev);
+            cudaError_t le = rc == DDAGPU_OK ? launch_step_advance(c->step_dev, st) : cudaSuccess;
+            if (rc == DDAGPU_OK && le == cudaSuccess) rc = top(max_step, c->step_dev);
+            if (rc == DDAGPU_OK && le == cudaSuccess)
+                le = launch_loop_control(c->active, nrhs, c->step_dev, max_step, h, st);
             cudaGraph_t captured = nullptr;
             const cudaError_t ee = cudaStreamEndCapture(st, &captured);
-            c->g_per_iter = c->launches - l0 + 1;
+            c->g_per_iter = c->launches - l0 + 2;
             c->launches = l0;
             if (rc != DDAGPU_OK || le != cudaSuccess || ee != cudaSuccess) {
                 cudaGraphDestroy(g);
@@ -470,7 +475,7 @@ int run_solver(ddagpu_ctx *c, int nrhs, int solver, float tau, int max_step, flo
         int last = first;
         CK(cudaMemcpyAsync(&last, c->step_dev, sizeof(int), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
-        c->launches += (long long)(last - first) * c->g_per_iter;
+        c->launches += (long long)(last - first) * c->g_per_iter;   // one pass per step advanced
         c->graph_runs += 1;
     }
     // ---- rollback (dda_func.cpp:1537-1548), for every right-hand side

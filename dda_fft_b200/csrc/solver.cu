@@ -286,6 +286,7 @@ __global__ void scalar_stage(RhsState *st, const int *rhs_active_in, int *rhs_ac
                              int trace_len)
 {
     const int rhs = blockIdx.x * blockDim.x + threadIdx.x;
+    // with step_dev the step comes from device memory and step_arg holds Max_Step
     const int step = step_dev ? *step_dev : step_arg;
     if (rhs >= nrhs) return;
     RhsState &S = st[rhs];
@@ -355,7 +356,10 @@ __global__ void scalar_stage(RhsState *st, const int *rhs_active_in, int *rhs_ac
         break;
     case SC_TOP: // dda_func.cpp:1301-1313
         S.need_copy = 0;
-        if (S.err <= S.err_max) {
+        if (step_dev && step > step_arg) {
+            // a graph-recorded iteration past Max_Step (step_arg): the host loop has ended
+            // here, so only the copy flag is cleared
+        } else if (S.err <= S.err_max) {
             S.active = 0;
         } else if (step == 1) {
             // the step-0 iterate is the best one so far (dda_func.cpp:1286-1293); it is
@@ -506,10 +510,10 @@ cudaError_t launch_scalar(RhsState *st_, const int *act_in, int *act_out, int nr
     return cudaGetLastError();
 }
 
-// End of one iteration of a solve recorded in a CUDA graph: advance the device step
-// counter and keep looping while some right-hand side is active and the counter has not
-// passed Max_Step (the host loop's test, dda_func.cpp:1301-1313).
-__global__ void __launch_bounds__(256) loop_control(const int *active, int nrhs, int *step_dev,
+// Last kernel of one iteration of a solve recorded in a CUDA graph, after the convergence
+// test of the next step: keep looping while some right-hand side is active and the step
+// has not passed Max_Step (the host loop's test, dda_func.cpp:1301-1313).
+__global__ void __launch_bounds__(256) loop_control(const int *active, int nrhs, const int *step_dev,
                                                     int max_step, cudaGraphConditionalHandle h)
 {
     __shared__ int any;
@@ -519,14 +523,19 @@ __global__ void __launch_bounds__(256) loop_control(const int *active, int nrhs,
     for (int r = threadIdx.x; r < nrhs; r += blockDim.x) mine |= active[r] != 0;
     if (mine) atomicOr(&any, 1);
     __syncthreads();
-    if (threadIdx.x == 0) {
-        const int next = *step_dev + 1;
-        *step_dev = next;
-        cudaGraphSetConditional(h, (any && next <= max_step) ? 1u : 0u);
-    }
+    if (threadIdx.x == 0) cudaGraphSetConditional(h, (any && *step_dev <= max_step) ? 1u : 0u);
 }
 
-cudaError_t launch_loop_control(const int *active, int nrhs, int *step_dev, int max_step,
+// ++*step_dev
+__global__ void step_advance(int *step_dev) { *step_dev += 1; }
+
+cudaError_t launch_step_advance(int *step_dev, cudaStream_t st)
+{
+    step_advance<<<1, 1, 0, st>>>(step_dev);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_loop_control(const int *active, int nrhs, const int *step_dev, int max_step,
                                 cudaGraphConditionalHandle h, cudaStream_t st)
 {
     loop_control<<<1, 256, 0, st>>>(active, nrhs, step_dev, max_step, h);

@@ -43,13 +43,15 @@ struct FieldArgs {
 
 cudaError_t launch_field_op(int op, const FieldArgs &a, cudaStream_t st);
 cudaError_t launch_first_approx(const FieldArgs &a, cudaStream_t st);
-// step_dev (may be null): read the step number from device memory instead of `step`
+// step_dev (may be null): read the step number from device memory; `step` then holds
+// Max_Step, past which SC_TOP only clears the copy flag
 cudaError_t launch_scalar(RhsState *st_, const int *act_in, int *act_out, int nrhs, int stage,
                           int step, double *trace, int trace_len, cudaStream_t st,
                           const int *step_dev = nullptr);
-// last node of a graph-recorded iteration: ++*step_dev, condition = any active && step <= max
-cudaError_t launch_loop_control(const int *active, int nrhs, int *step_dev, int max_step,
+// last node of a graph-recorded iteration: condition = any active && *step_dev <= max_step
+cudaError_t launch_loop_control(const int *active, int nrhs, const int *step_dev, int max_step,
                                 cudaGraphConditionalHandle h, cudaStream_t st);
+cudaError_t launch_step_advance(int *step_dev, cudaStream_t st);
 cudaError_t launch_gated_copy(const FieldArgs &a, int dir, cudaStream_t st);
 
 // refinement passes: 0 x64 = b; 1 r = b - (x64 - alpha conv) with conv in w, error into

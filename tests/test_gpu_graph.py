@@ -38,6 +38,8 @@ def test_graph_equals_host_loop(D, oracle, solver):
             out[g, "runs"] = ctx.solver_graph_runs - runs0
     a, b = out[False], out[True]
     assert a["steps"] == b["steps"] and a["steps"] >= 2
+    for q in ("step_min", "rolled_back", "matvecs"):
+        assert a[q] == b[q], q
     assert out[True, "runs"] == 1 and out[False, "runs"] == 0
     n = a["steps"] + 1
     np.testing.assert_allclose(b["trace"][:n], a["trace"][:n], rtol=1e-9)
@@ -80,3 +82,23 @@ def test_graph_in_refinement(D, oracle):
                                          solver=2, err_max=1e-8, max_outer=20)
     assert out[True]["err"] <= 1e-8 and out[False]["err"] <= 1e-8
     assert abs(out[True]["cext"] - out[False]["cext"]) <= 1e-6 * abs(out[False]["cext"])
+
+
+@pytest.mark.parametrize("max_step", [1, 2, 3])
+@pytest.mark.parametrize("solver", [0, 2])
+def test_graph_short_runs(D, oracle, solver, max_step):
+    """Max_Step at the edges of the graph (1: no graph; 2: one pass; 3): the same stopping
+    step, best iterate and rollback as the host loop."""
+    occ, kd, alpha, ksc = problem(oracle)
+    out = {}
+    with D.Context(occ.shape, kd) as ctx:
+        for g in (False, True):
+            ctx.set_solver_graph(g)
+            out[g] = ctx.dda_fft(occ, alpha, [0, 1], kd, (0, 0, 1), (1, 0, 0), ksc, solver=solver,
+                                 max_step=max_step, err_max=1e-9)
+    a, b = out[False], out[True]
+    for q in ("steps", "step_min", "rolled_back", "matvecs"):
+        assert a[q] == b[q], q
+    assert a["steps"] == max_step
+    np.testing.assert_allclose(b["trace"], a["trace"], rtol=1e-9)
+    assert abs(b["cext"] - a["cext"]) <= 1e-6 * abs(a["cext"])
