@@ -184,7 +184,8 @@ def main():
                     help="only run the matvec on NRHS right-hand sides (for ncu captures)")
     ap.add_argument("--grid", type=int, default=GRID)
     ap.add_argument("--workload", default="orientations",
-                    choices=["orientations", "precision", "adjoint", "realizations", "plain"])
+                    choices=["orientations", "precision", "adjoint", "realizations", "plain",
+                             "solver_graph"])
     args = ap.parse_args()
     if args.profile_matvec:
         return profile_matvec(args)
@@ -194,6 +195,8 @@ def main():
         return adjoint_run(args)
     if args.workload == "plain":
         return plain_run(args)
+    if args.workload == "solver_graph":
+        return solver_graph_run(args)
     if args.warmup < 3:
         args.warmup = 3
     if args.workload == "realizations":
@@ -520,6 +523,35 @@ def plain_run(args):
                             max_step=100, nplanes=12, theta_step=1.0)
         secs, *_ = P.RefLib().run_samples(rc, 1, 1)
         out["reference_cpu_s_per_sample"] = secs
+    print(json.dumps(out), flush=True)
+
+
+def solver_graph_run(args):
+    """Solves that iterate (BiCGStab to Error_max 1e-6 on ellipsoids b/a 0.8, c/a 0.6,
+    x = n/8, m = 1.6+0.002i): wall time per batched call with iterations 2.. recorded as
+    one CUDA graph launch vs the host loop that reads the active flags every iteration."""
+    import torch
+    import dda_fft_b200 as D
+    out = {"workload": "BiCGStab to 1e-6, ellipsoid 0.8/0.6, x = n/8, m = 1.6+0.002i"}
+    for n, no in ((16, 1), (32, 1), (32, 8), (64, 1), (64, 16)):
+        x = n / 8.0
+        cfg = D.BatchConfig(occ=ellipsoid_occ(n, 0.8, 0.6), materials=[(1.6, 0.002)], solver=2,
+                            err_max=1e-6, max_step=300)
+        rot = D.mc_rotations(SEED, no)
+        row = {}
+        with D.Context(n, 2 * x / n, max_rhs=2 * no) as ctx:
+            for g in (False, True):
+                ctx.set_solver_graph(g)
+                for _ in range(max(args.warmup, 1)):
+                    r = ctx.orientation_solves(cfg, rot)
+                torch.cuda.synchronize()
+                t = time.perf_counter()
+                for _ in range(max(args.steps, 1)):
+                    r = ctx.orientation_solves(cfg, rot)
+                torch.cuda.synchronize()
+                row["graph_ms" if g else "host_loop_ms"] = (time.perf_counter() - t) / max(args.steps, 1) * 1e3
+            row["steps"] = r["max_steps"]
+        out[f"{n}^3 x {2 * no} rhs"] = row
     print(json.dumps(out), flush=True)
 
 
