@@ -221,6 +221,7 @@ def main():
     occ = ellipsoid_occ()
     kd = 2 * X / GRID
     ctx = D.Context(GRID, kd, max_rhs=2 * B, device=dev)
+    ctx.autotune(2 * B)          # pass variants and tiling for this batch (set-up, not timed)
     stream = torch.cuda.ExternalStream(ctx.stream_ptr, device=dev)
     # every rank draws its own contiguous run of the reference's MC stream (worker 0)
     total = (W + K) * B * world
@@ -360,7 +361,8 @@ def main():
             "config": {"workload": WORKLOAD, "grid": GRID, "orientations_per_step": B,
                        "rhs_per_step": 2 * B, "parallelism": f"orientations sharded over {world} GPU(s)",
                        "l2": "working set per step >> L2 (126 MB): no flush needed",
-                       "tiling": list(ctx.tiling())},
+                       "tiling": list(ctx.tiling()), "fast_passes": ctx.fast_kernels,
+                       "fast_variant": list(ctx.fast_variant)},
             "e2e": {"value": e2e, "unit": "orientation-solves/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "plain_gpu": {"value": plain, "unit": "orientation-solves/s",
@@ -632,6 +634,8 @@ def realizations_run(args):
     groups = {n: [k for k, s in enumerate(sizes) if s == n] for n in AGG_SIZES}
     counts = {n: D.Agglomerate.count((n, n, n), AGG_RHO, AGG_R, AGG_LR) for n in AGG_SIZES}
     ctxs = {n: D.Context(n, 2 * X / n, max_rhs=2 * max(len(g), 1)) for n, g in groups.items() if g}
+    for n, c in ctxs.items():
+        c.autotune(2 * len(groups[n]))
     cfg = D.BatchConfig(occ=None, materials=[MAT])
     pool = ThreadPoolExecutor(max_workers=os.cpu_count() or 4)
 

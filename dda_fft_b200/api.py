@@ -115,6 +115,8 @@ def lib():
         L.ddagpu_set_kernels.argtypes = [_p, _i]
         L.ddagpu_farfield_noalloc.argtypes = [_i, _i, _i, _i, _f, _p, _p, _p, _i, _p, _p, _p]
         L.ddagpu_get_kernels.argtypes = [_p]
+        L.ddagpu_set_fast_variant.argtypes = [_p, _i, _i]
+        L.ddagpu_get_fast_variant.argtypes = [_p, C.POINTER(_i), C.POINTER(_i)]
         L.ddagpu_set_solver_graph.argtypes = [_p, _i]
         L.ddagpu_solver_graph_runs.argtypes = [_p]
         L.ddagpu_solver_graph_runs.restype = C.c_longlong
@@ -544,6 +546,16 @@ class Context:
 
     def set_tiling(self, tile_x=0, rows_g=0):
         _check(lib().ddagpu_set_tiling(self._h, tile_x, rows_g))
+
+    def set_fast_variant(self, x_variant: int = 0, yz_variant: int = 0):
+        """Launch variants of the compile-time-sized passes (0/1 each)."""
+        _check(lib().ddagpu_set_fast_variant(self._h, x_variant, yz_variant))
+
+    @property
+    def fast_variant(self):
+        x, yz = _i(), _i()
+        _check(lib().ddagpu_get_fast_variant(self._h, C.byref(x), C.byref(yz)))
+        return x.value, yz.value
 
     def set_solver_graph(self, on: bool):
         """Iterations 2..Max_Step of each solve as one CUDA graph launch (default on)."""

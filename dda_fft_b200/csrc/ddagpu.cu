@@ -75,6 +75,7 @@ struct ddagpu_ctx {
     Lat L{};
     int tile_x = 32, rows_g = 16;
     int fast = 0;                // compile-time-sized passes in use
+    int fx = 0, fyz = 0;         // their launch variants (x pass, y/z passes)
     float2 *ahat = nullptr, *tw = nullptr;
     float2 *work = nullptr, *p = nullptr, *pmin = nullptr, *r = nullptr, *s = nullptr,
            *g = nullptr, *h = nullptr, *w = nullptr;
@@ -108,7 +109,7 @@ struct ddagpu_ctx {
     int graph_on = 1;
     int *step_dev = nullptr;
     struct GraphKey {
-        int solver, nrhs, max_step, nmat1, fast, tile_x, rows_g, tlen;
+        int solver, nrhs, max_step, nmat1, fast, fx, fyz, tile_x, rows_g, tlen;
         float tau;
         double d0;
         size_t occ_stride;
@@ -200,6 +201,8 @@ MatvecArgs mv_args(ddagpu_ctx *c, int nrhs, const float2 *src, float2 *out, int 
     a.tile_x = c->tile_x;
     a.rows_g = c->rows_g;
     a.fast = c->fast;
+    a.fx = c->fx;
+    a.fyz = c->fyz;
     return a;
 }
 
@@ -412,6 +415,8 @@ int run_solver(ddagpu_ctx *c, int nrhs, int solver, float tau, int max_step, flo
         key.max_step = max_step;
         key.nmat1 = nmat1;
         key.fast = c->fast;
+        key.fx = c->fx;
+        key.fyz = c->fyz;
         key.tile_x = c->tile_x;
         key.rows_g = c->rows_g;
         key.tlen = tlen;
@@ -784,14 +789,23 @@ int ddagpu_autotune(ddagpu_ctx *c, int nrhs)
                 brg = rg;
             }
         }
+    int bfx = 0, bfyz = 0;
     if (matvec_fast_supported(c->L)) {
+        // the compile-time-sized passes in each launch variant
         c->fast = 1;
-        float ms = 0;
-        RET(time_it(&ms));
-        if (ms < best) {
-            best = ms;
-            bfast = 1;
-        }
+        for (int vx = 0; vx < 2; vx++)
+            for (int vyz = 0; vyz < 2; vyz++) {
+                c->fx = vx;
+                c->fyz = vyz;
+                float ms = 0;
+                RET(time_it(&ms));
+                if (ms < best) {
+                    best = ms;
+                    bfast = 1;
+                    bfx = vx;
+                    bfyz = vyz;
+                }
+            }
     }
     (void)had_fast;
     cudaEventDestroy(e0);
@@ -799,6 +813,8 @@ int ddagpu_autotune(ddagpu_ctx *c, int nrhs)
     c->fast = 0;
     RET(ddagpu_set_tiling(c, btx, brg));
     c->fast = bfast;
+    c->fx = bfx;
+    c->fyz = bfyz;
     return DDAGPU_OK;
 }
 
@@ -1500,6 +1516,25 @@ int ddagpu_anthrax_rasterize(int device, int i_max, int j_max, int l_max, const 
     CK(e);
     CK(e2);
     if (ndip) *ndip = h;
+    return DDAGPU_OK;
+}
+
+int ddagpu_set_fast_variant(ddagpu_ctx *c, int x_variant, int yz_variant)
+{
+    if (!c) return fail(DDAGPU_EINVAL, "null context");
+    if (x_variant < 0 || x_variant > 1 || yz_variant < 0 || yz_variant > 1)
+        return fail(DDAGPU_EINVAL, "launch variants are 0 or 1");
+    std::lock_guard<std::mutex> lk(c->mu);
+    c->fx = x_variant;
+    c->fyz = yz_variant;
+    return DDAGPU_OK;
+}
+
+int ddagpu_get_fast_variant(ddagpu_ctx *c, int *x_variant, int *yz_variant)
+{
+    if (!c || !x_variant || !yz_variant) return fail(DDAGPU_EINVAL, "null argument");
+    *x_variant = c->fx;
+    *yz_variant = c->fyz;
     return DDAGPU_OK;
 }
 

@@ -68,6 +68,7 @@ struct MatvecArgs {
     int tile_x;             // columns per CTA of the x pass (generic kernels)
     int rows_g;             // rows per staging group of the y/z passes (generic kernels)
     int fast;               // 1: compile-time-sized kernels of matvec_fast.cu
+    int fx, fyz;            // launch variants of the fast x pass and y/z passes (0 default, 1)
 };
 
 // kernels (matvec.cu)

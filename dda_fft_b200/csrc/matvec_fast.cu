@@ -168,8 +168,14 @@ __global__ void __launch_bounds__(NT) k1f(MatvecArgs a)
 // ------------------------------------------------------------------------------ K2
 // CTA (spectral row js, TL spectral columns): forward x (both halves), 3x3 product,
 // inverse x, in place.  Shared B[c][h][pos][t].
+// at least this many CTAs per SM: about 128 registers a thread (80 for the 16-point lines)
+constexpr int k2_min_blocks(int NI, int threads)
+{
+    return NI == 16 ? (6 * 128) / threads : (512 / threads > 0 ? 512 / threads : 1);
+}
+
 template <int NI, int TL>
-__global__ void __launch_bounds__(Sp<NI>::RM * TL, NI == 16 ? 6 : 2) k2f(MatvecArgs a)
+__global__ void __launch_bounds__(Sp<NI>::RM * TL, k2_min_blocks(NI, Sp<NI>::RM * TL)) k2f(MatvecArgs a)
 {
     using S = Sp<NI>;
     constexpr int R1 = S::R1, R2 = S::R2, RM = S::RM;
@@ -487,11 +493,15 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(NT) k3f(MatvecArgs a
     cl.sync();
 }
 
+// Launch variants the autotuner chooses between (variant 0 is the default): block size of
+// the y/z passes, columns per CTA of the x pass.
 template <int NJ, int NL>
-constexpr int yz_threads()
+constexpr int yz_threads(int v)
 {
-    // enough threads for the column role on all NL columns and the row role on all rows
-    return (Sp<NJ>::RM * NL) > 256 ? 512 : 256;
+    // variant 0: enough threads for the column role on all NL columns and the row role on
+    // all rows; variant 1: the other of 256 / 512
+    const int t0 = (Sp<NJ>::RM * NL) > 256 ? 512 : 256;
+    return v == 0 ? t0 : (t0 == 512 ? 256 : 512);
 }
 
 template <int NJ, int NL>
@@ -500,19 +510,26 @@ constexpr size_t yz_smem()
     return (size_t)NJ * Sp<NL>::PS * sizeof(float2);   // one plane, 128 KB at 128 x 128
 }
 
-template <int NJ, int NL>
-void launch_yz(const MatvecArgs &a, int fwd, cudaStream_t st)
+template <int NJ, int NL, int V>
+void launch_yz_v(const MatvecArgs &a, int fwd, cudaStream_t st)
 {
-    constexpr int NT = yz_threads<NJ, NL>();
+    constexpr int NT = yz_threads<NJ, NL>(V);
     constexpr size_t S = yz_smem<NJ, NL>();
     if (fwd) k1f<NJ, NL, NT><<<dim3(2 * a.L.ni, 3, a.nrhs), NT, S, st>>>(a);
     else k3f<NJ, NL, NT><<<dim3(2 * a.L.ni, 3, a.nrhs), NT, S, st>>>(a);
 }
 
 template <int NJ, int NL>
-cudaError_t prep_yz()
+void launch_yz(const MatvecArgs &a, int fwd, cudaStream_t st)
 {
-    constexpr int NT = yz_threads<NJ, NL>();
+    if (a.fyz) launch_yz_v<NJ, NL, 1>(a, fwd, st);
+    else launch_yz_v<NJ, NL, 0>(a, fwd, st);
+}
+
+template <int NJ, int NL, int V>
+cudaError_t prep_yz_v()
+{
+    constexpr int NT = yz_threads<NJ, NL>(V);
     constexpr int S = (int)yz_smem<NJ, NL>();
     cudaError_t e = cudaFuncSetAttribute(k1f<NJ, NL, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, S);
     if (e == cudaSuccess)
@@ -520,27 +537,50 @@ cudaError_t prep_yz()
     return e;
 }
 
-template <int NI>
-constexpr int x_tile()
+template <int NJ, int NL>
+cudaError_t prep_yz()
 {
-    return NI <= 32 ? 32 : (NI == 64 ? 32 : 16);
+    cudaError_t e = prep_yz_v<NJ, NL, 0>();
+    return e == cudaSuccess ? prep_yz_v<NJ, NL, 1>() : e;
 }
 
 template <int NI>
-void launch_x(const MatvecArgs &a, cudaStream_t st)
+constexpr int x_tile(int v)
 {
-    constexpr int TL = x_tile<NI>();
+    // variant 0: 32 columns per CTA (16 at NI = 128); variant 1: half of that
+    const int t0 = NI <= 64 ? 32 : 16;
+    return v == 0 ? t0 : t0 / 2;
+}
+
+template <int NI, int V>
+void launch_x_v(const MatvecArgs &a, cudaStream_t st)
+{
+    constexpr int TL = x_tile<NI>(V);
     const int ncol = 2 * a.L.nl;
     const size_t smem = (size_t)6 * NI * TL * sizeof(float2);
     k2f<NI, TL><<<dim3(2 * a.L.nj, ncol / TL, a.nrhs), Sp<NI>::RM * TL, smem, st>>>(a);
 }
 
 template <int NI>
-cudaError_t prep_x()
+void launch_x(const MatvecArgs &a, cudaStream_t st)
 {
-    constexpr int TL = x_tile<NI>();
+    if (a.fx) launch_x_v<NI, 1>(a, st);
+    else launch_x_v<NI, 0>(a, st);
+}
+
+template <int NI, int V>
+cudaError_t prep_x_v()
+{
+    constexpr int TL = x_tile<NI>(V);
     return cudaFuncSetAttribute(k2f<NI, TL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)(6 * NI * TL * sizeof(float2)));
+}
+
+template <int NI>
+cudaError_t prep_x()
+{
+    cudaError_t e = prep_x_v<NI, 0>();
+    return e == cudaSuccess ? prep_x_v<NI, 1>() : e;
 }
 
 bool fast_edge(int n) { return n == 16 || n == 32 || n == 64 || n == 128; }

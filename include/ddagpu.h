@@ -209,6 +209,14 @@ int ddagpu_anthrax_place(unsigned long long *rng_state, int i_max, float monomer
 int ddagpu_anthrax_rasterize(int device, int i_max, int j_max, int l_max, const float *monomers,
                              int count, signed char *occ, int *ndip);
 
+/* Launch variants of the compile-time-sized matvec passes (edges 16..128): x_variant 0/1
+ * = 32 or 16 spectral columns per x-pass CTA (16 or 8 at edge 128); yz_variant 0/1 = the
+ * default block size of the y/z passes or the other of 256 / 512 threads.
+ * ddagpu_autotune times every combination (and the generic passes) and keeps the
+ * fastest.  No counterpart in the reference. */
+int ddagpu_set_fast_variant(ddagpu_ctx *ctx, int x_variant, int yz_variant);
+int ddagpu_get_fast_variant(ddagpu_ctx *ctx, int *x_variant, int *yz_variant);
+
 /* Solver iterations as a CUDA graph (no counterpart in the reference, whose loop is on
  * the host, dda_func.cpp:1301-1535).  On (the default), iterations 2..Max_Step of every
  * solve run as one graph launch: a conditional while node whose body is one iteration

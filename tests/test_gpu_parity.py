@@ -132,6 +132,39 @@ def test_fast_and_generic_agree_128(D, grid):
         assert rel(outs[True, conj], outs[False, conj]) < 2e-6
 
 
+@pytest.mark.parametrize("grid", [(16, 16, 16), (64, 64, 64), (128, 64, 32), (32, 128, 16)])
+def test_fast_launch_variants_agree(D, oracle, grid):
+    """Every launch variant of the specialised passes gives the oracle's convolution, and
+    the autotuner's pick does too."""
+    import torch
+    rng = np.random.default_rng(9)
+    p = crand(rng, (2, 3) + grid)
+    kd = 2 * 3.0 / grid[0]
+    ref = [oracle.convolution(oracle.green_hat(*grid, kd), p[r].transpose(1, 2, 3, 0).astype(np.complex128))
+           for r in range(2)] if max(grid) <= 64 else None
+    with D.Context(grid, kd, max_rhs=2) as ctx:
+        x = torch.from_numpy(p).cuda()
+        outs = []
+        for vx in (0, 1):
+            for vyz in (0, 1):
+                ctx.set_fast_variant(vx, vyz)
+                assert ctx.fast_variant == (vx, vyz)
+                y = torch.empty_like(x)
+                ctx.convolution_dev(x, y, 2)
+                torch.cuda.synchronize()
+                outs.append(y.cpu().numpy())
+        ctx.autotune(2)
+        y = torch.empty_like(x)
+        ctx.convolution_dev(x, y, 2)
+        torch.cuda.synchronize()
+        outs.append(y.cpu().numpy())
+    for o in outs[1:]:
+        assert rel(o, outs[0]) < 2e-6
+    if ref is not None:
+        for r in range(2):
+            assert rel(outs[0][r].transpose(1, 2, 3, 0), ref[r]) < CONV_TOL
+
+
 def test_convolution_linearity_128(D):
     n, kd = 128, 0.25
     rng = np.random.default_rng(9)
