@@ -793,8 +793,8 @@ int ddagpu_autotune(ddagpu_ctx *c, int nrhs)
     if (matvec_fast_supported(c->L)) {
         // the compile-time-sized passes in each launch variant
         c->fast = 1;
-        for (int vx = 0; vx < 2; vx++)
-            for (int vyz = 0; vyz < 2; vyz++) {
+        for (int vx = 0; vx < kFastVariants; vx++)
+            for (int vyz = 0; vyz < kFastVariants; vyz++) {
                 c->fx = vx;
                 c->fyz = vyz;
                 float ms = 0;
@@ -1522,8 +1522,8 @@ int ddagpu_anthrax_rasterize(int device, int i_max, int j_max, int l_max, const 
 int ddagpu_set_fast_variant(ddagpu_ctx *c, int x_variant, int yz_variant)
 {
     if (!c) return fail(DDAGPU_EINVAL, "null context");
-    if (x_variant < 0 || x_variant > 1 || yz_variant < 0 || yz_variant > 1)
-        return fail(DDAGPU_EINVAL, "launch variants are 0 or 1");
+    if (x_variant < 0 || x_variant >= kFastVariants || yz_variant < 0 || yz_variant >= kFastVariants)
+        return fail(DDAGPU_EINVAL, "launch variants are 0, 1 or 2");
     std::lock_guard<std::mutex> lk(c->mu);
     c->fx = x_variant;
     c->fyz = yz_variant;

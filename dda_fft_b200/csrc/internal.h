@@ -68,7 +68,7 @@ struct MatvecArgs {
     int tile_x;             // columns per CTA of the x pass (generic kernels)
     int rows_g;             // rows per staging group of the y/z passes (generic kernels)
     int fast;               // 1: compile-time-sized kernels of matvec_fast.cu
-    int fx, fyz;            // launch variants of the fast x pass and y/z passes (0 default, 1)
+    int fx, fyz;            // launch variants of the fast x pass and y/z passes (0 default .. 2)
 };
 
 // kernels (matvec.cu)
@@ -79,6 +79,7 @@ cudaError_t matvec_prepare(const Lat &L, int tile_x, int rows_g);
 
 // compile-time-sized passes for edges in {16, 32, 64} (matvec_fast.cu)
 bool matvec_fast_supported(const Lat &L);
+constexpr int kFastVariants = 3;   // launch variants per fast pass
 cudaError_t matvec_fast_prepare(const Lat &L);
 cudaError_t launch_matvec_fast(const MatvecArgs &a, cudaStream_t st);
 

@@ -499,9 +499,9 @@ template <int NJ, int NL>
 constexpr int yz_threads(int v)
 {
     // variant 0: enough threads for the column role on all NL columns and the row role on
-    // all rows; variant 1: the other of 256 / 512
+    // all rows; variant 1: the other of 256 / 512; variant 2: 128
     const int t0 = (Sp<NJ>::RM * NL) > 256 ? 512 : 256;
-    return v == 0 ? t0 : (t0 == 512 ? 256 : 512);
+    return v == 0 ? t0 : v == 1 ? (t0 == 512 ? 256 : 512) : 128;
 }
 
 template <int NJ, int NL>
@@ -522,7 +522,8 @@ void launch_yz_v(const MatvecArgs &a, int fwd, cudaStream_t st)
 template <int NJ, int NL>
 void launch_yz(const MatvecArgs &a, int fwd, cudaStream_t st)
 {
-    if (a.fyz) launch_yz_v<NJ, NL, 1>(a, fwd, st);
+    if (a.fyz == 2) launch_yz_v<NJ, NL, 2>(a, fwd, st);
+    else if (a.fyz == 1) launch_yz_v<NJ, NL, 1>(a, fwd, st);
     else launch_yz_v<NJ, NL, 0>(a, fwd, st);
 }
 
@@ -541,15 +542,16 @@ template <int NJ, int NL>
 cudaError_t prep_yz()
 {
     cudaError_t e = prep_yz_v<NJ, NL, 0>();
-    return e == cudaSuccess ? prep_yz_v<NJ, NL, 1>() : e;
+    if (e == cudaSuccess) e = prep_yz_v<NJ, NL, 1>();
+    return e == cudaSuccess ? prep_yz_v<NJ, NL, 2>() : e;
 }
 
 template <int NI>
 constexpr int x_tile(int v)
 {
-    // variant 0: 32 columns per CTA (16 at NI = 128); variant 1: half of that
+    // variant 0: 32 columns per CTA (16 at NI = 128); variants 1, 2: a half, a quarter
     const int t0 = NI <= 64 ? 32 : 16;
-    return v == 0 ? t0 : t0 / 2;
+    return t0 >> v;
 }
 
 template <int NI, int V>
@@ -564,7 +566,8 @@ void launch_x_v(const MatvecArgs &a, cudaStream_t st)
 template <int NI>
 void launch_x(const MatvecArgs &a, cudaStream_t st)
 {
-    if (a.fx) launch_x_v<NI, 1>(a, st);
+    if (a.fx == 2) launch_x_v<NI, 2>(a, st);
+    else if (a.fx == 1) launch_x_v<NI, 1>(a, st);
     else launch_x_v<NI, 0>(a, st);
 }
 
@@ -580,7 +583,8 @@ template <int NI>
 cudaError_t prep_x()
 {
     cudaError_t e = prep_x_v<NI, 0>();
-    return e == cudaSuccess ? prep_x_v<NI, 1>() : e;
+    if (e == cudaSuccess) e = prep_x_v<NI, 1>();
+    return e == cudaSuccess ? prep_x_v<NI, 2>() : e;
 }
 
 bool fast_edge(int n) { return n == 16 || n == 32 || n == 64 || n == 128; }
