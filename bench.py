@@ -183,6 +183,8 @@ def main():
     ap.add_argument("--profile-matvec", type=int, default=0, metavar="NRHS",
                     help="only run the matvec on NRHS right-hand sides (for ncu captures)")
     ap.add_argument("--grid", type=int, default=GRID)
+    ap.add_argument("--variant", type=int, nargs=2, default=None, metavar=("X", "YZ"),
+                    help="with --profile-matvec: launch variants instead of autotuning")
     ap.add_argument("--workload", default="orientations",
                     choices=["orientations", "precision", "adjoint", "realizations", "plain",
                              "solver_graph"])
@@ -391,13 +393,18 @@ def profile_matvec(args):
     import dda_fft_b200 as D
     n, nrhs = args.grid, args.profile_matvec
     ctx = D.Context(n, 2 * X / n, max_rhs=nrhs)
+    if args.variant:
+        ctx.set_fast_variant(*args.variant)
+    else:
+        ctx.autotune(nrhs)
     x = torch.randn(nrhs, 3, n, n, n, dtype=torch.complex64, device="cuda")
     y = torch.empty_like(x)
     torch.cuda.synchronize()
     for _ in range(args.warmup + args.steps):
         ctx.convolution_dev(x, y, nrhs)
     torch.cuda.synchronize()
-    print(json.dumps({"profile_matvec": nrhs, "grid": n, "launches": ctx.kernel_launches}))
+    print(json.dumps({"profile_matvec": nrhs, "grid": n, "launches": ctx.kernel_launches,
+                      "fast_variant": list(ctx.fast_variant)}))
     ctx.close()
 
 
