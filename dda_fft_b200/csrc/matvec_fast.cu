@@ -101,20 +101,26 @@ __global__ void __launch_bounds__(NT) k1f(MatvecArgs a)
     {
         constexpr int RM = SL::RM, RPP = NT / RM;   // rows per pass
         const int sub = threadIdx.x % RM, rr = threadIdx.x / RM;
+        // the next pass's row is loaded while this pass's row is transformed
+        auto load = [&](int row, float2 (&v)[SL::R1]) {
+            if (row < NJ && sub < SL::R2) {
+#pragma unroll
+                for (int r = 0; r < SL::R1; r++) v[r] = src[row * NL + sub + SL::R2 * r];
+            }
+        };
+        float2 v[SL::R1], vn[SL::R1];
+        load(rr, v);
 #pragma unroll 1
         for (int r0 = 0; r0 < NJ; r0 += RPP) {
             const int row = r0 + rr;
-            float2 v[SL::R1];
-            if (row < NJ && sub < SL::R2) {
+            if (r0 + RPP < NJ) load(row + RPP, vn);
+            if (hl && row < NJ && sub < SL::R2) {
 #pragma unroll
-                for (int r = 0; r < SL::R1; r++) {
-                    const int l = sub + SL::R2 * r;
-                    float2 x = src[row * NL + l];
-                    if (hl) x = cmul(x, __ldg(&hwl[l]));
-                    v[r] = x;
-                }
+                for (int r = 0; r < SL::R1; r++) v[r] = cmul(v[r], __ldg(&hwl[sub + SL::R2 * r]));
             }
             row_fft_from_regs<NL, false>(Z + (row < NJ ? row : 0) * PS, sub, row < NJ, v, twl);
+#pragma unroll
+            for (int r = 0; r < SL::R1; r++) v[r] = vn[r];
         }
     }
     __syncthreads();
@@ -404,13 +410,19 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(NT) k3f(MatvecArgs a
             const int col = cbase + col0;
             const bool ok = col < NL;
             float2 y0[R2];
-#pragma unroll 1
-            for (int hy = 0; hy < 2; hy++) {
-                if (ok && sub < R2) {
-                    float2 v[R1];
+            // both y halves' loads in flight before the first transform
+            float2 vh[2][R1];
+            if (ok && sub < R2) {
+#pragma unroll
+                for (int hy = 0; hy < 2; hy++)
 #pragma unroll
                     for (int r = 0; r < R1; r++)
-                        v[r] = src[(size_t)(hy * NJ + sub + R2 * r) * (2 * NL) + col];
+                        vh[hy][r] = src[(size_t)(hy * NJ + sub + R2 * r) * (2 * NL) + col];
+            }
+#pragma unroll
+            for (int hy = 0; hy < 2; hy++) {
+                if (ok && sub < R2) {
+                    float2 (&v)[R1] = vh[hy];
                     dft_reg<R1, true>(v);
 #pragma unroll
                     for (int k1 = 1; k1 < R1; k1++) v[k1] = cmul(v[k1], twid<true>(twj, sub * k1));
