@@ -18,80 +18,136 @@ namespace ddagpu {
 
 namespace {
 
-constexpr int FF_DIRS = 32;   // directions per CTA (one per lane)
-constexpr int FF_ROWS = 16;   // lattice rows staged per round
+// Far-field tiling: a CTA takes one lattice plane i of one right-hand side and up to
+// FF_DMAX directions; a thread accumulates FF_DPT directions x 3 components for the rows
+// rg, rg + RG, ... of each staged group and the columns of its column group lg, so every
+// staged dipole value and phase factor it loads from shared memory feeds 4 to 12 complex
+// multiply-adds.
+constexpr int FF_DMAX = 32;
+constexpr int FF_DPT = 4;
+constexpr int FF_CELLS = 2048;   // lattice cells staged per round
 
-// grid (dir chunks, ni, nrhs), 256 threads: lane = direction, warp = row of the slab
-__global__ void __launch_bounds__(256) farfield_sum(PostArgs a)
+struct FFShape {
+    int D, DG, rows, RG, LG, threads;
+};
+
+FFShape ff_shape(int ndir, int nj, int nl)
+{
+    FFShape s;
+    s.D = ndir >= FF_DMAX ? FF_DMAX : ((ndir + FF_DPT - 1) / FF_DPT) * FF_DPT;
+    if (s.D < FF_DPT) s.D = FF_DPT;
+    s.DG = s.D / FF_DPT;
+    s.rows = FF_CELLS / nl < nj ? FF_CELLS / nl : nj;
+    if (s.rows < 1) s.rows = 1;
+    s.RG = 256 / s.DG < s.rows ? 256 / s.DG : s.rows;
+    // column groups: a power of two (it divides nl), at least 8 columns each
+    s.LG = 1;
+    while (2 * s.LG * s.DG * s.RG <= 256 && 2 * s.LG * 8 <= nl) s.LG *= 2;
+    s.threads = s.DG * s.RG * s.LG;
+    return s;
+}
+
+size_t ff_smem(const FFShape &s, int nj, int nl)
+{
+    const size_t tables = (size_t)(nl + nj + 1) * s.D;
+    const size_t staged = (size_t)s.rows * (3 * nl + 1);
+    const size_t red = (size_t)s.threads * FF_DPT * 3;
+    return (tables + (staged > red ? staged : red)) * sizeof(float2);
+}
+
+// grid (direction chunks of D, ni, nrhs)
+__global__ void __launch_bounds__(256) farfield_sum(PostArgs a, FFShape s)
 {
     extern __shared__ float2 sm[];
-    const int nj = a.nj, nl = a.nl;
-    const int dbase = blockIdx.x * FF_DIRS, i = blockIdx.y, rhs = blockIdx.z;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    float2 *ez = sm;                       // [nl][32]
-    float2 *ey = ez + nl * FF_DIRS;        // [nj][32]
-    float2 *P = ey + nj * FF_DIRS;         // [FF_ROWS][nl][3]
-    __shared__ float2 ex[FF_DIRS];
-    __shared__ double red[8][FF_DIRS][6];
+    const int nj = a.nj, nl = a.nl, D = s.D;
+    const int dbase = blockIdx.x * D, i = blockIdx.y, rhs = blockIdx.z;
+    const int dg = threadIdx.x % s.DG, rest = threadIdx.x / s.DG;
+    const int lg = rest % s.LG, rg = rest / s.LG;
+    const int PSR = 3 * nl + 1;            // staged row stride (odd: rows fall on other banks)
+    float2 *ez = sm;                       // [nl][D]
+    float2 *ey = ez + (size_t)nl * D;      // [nj][D]
+    float2 *ex = ey + (size_t)nj * D;      // [D]
+    float2 *P = ex + D;                    // [rows][PSR], later the reduction buffer
     const double cx = (a.ni - 1) * a.d0 / 2, cy = (nj - 1) * a.d0 / 2, cz = (nl - 1) * a.d0 / 2;
     const double *K = a.ksc + (size_t)rhs * a.ndir * 3;
-    for (int e = threadIdx.x; e < (nl + nj + 1) * FF_DIRS; e += blockDim.x) {
-        const int dl = e % FF_DIRS, pos = e / FF_DIRS, d = dbase + dl;
+    for (int e = threadIdx.x; e < (nl + nj + 1) * D; e += blockDim.x) {
+        const int dl = e % D, pos = e / D, dd = dbase + dl;
         float2 val = czero();
-        if (d < a.ndir) {
+        if (dd < a.ndir) {
             double ph;
-            if (pos < nl) ph = K[3 * d + 2] * (pos * a.d0 - cz);
-            else if (pos < nl + nj) ph = K[3 * d + 1] * ((pos - nl) * a.d0 - cy);
-            else ph = K[3 * d + 0] * (i * a.d0 - cx);
+            if (pos < nl) ph = K[3 * dd + 2] * (pos * a.d0 - cz);
+            else if (pos < nl + nj) ph = K[3 * dd + 1] * ((pos - nl) * a.d0 - cy);
+            else ph = K[3 * dd + 0] * (i * a.d0 - cx);
             val = expi_reduced(ph);
         }
-        if (pos < nl) ez[pos * FF_DIRS + dl] = val;
-        else if (pos < nl + nj) ey[(pos - nl) * FF_DIRS + dl] = val;
-        else ex[dl] = val;
+        ez[e] = val;   // ez, ey, ex are consecutive [pos][D] blocks
     }
     const size_t N = a.N;
     const float2 *p = a.p + (size_t)rhs * 3 * N + (size_t)i * nj * nl;
     const signed char *occ = a.occ + (size_t)rhs * a.occ_stride + (size_t)i * nj * nl;
-    float2 acc0 = czero(), acc1 = czero(), acc2 = czero();
-    for (int j0 = 0; j0 < nj; j0 += FF_ROWS) {
-        const int rows = nj - j0 < FF_ROWS ? nj - j0 : FF_ROWS;
+    const int lcnt = nl / s.LG, l0 = lg * lcnt;
+    float2 acc[FF_DPT][3];
+#pragma unroll
+    for (int u = 0; u < FF_DPT; u++)
+#pragma unroll
+        for (int c = 0; c < 3; c++) acc[u][c] = czero();
+    for (int j0 = 0; j0 < nj; j0 += s.rows) {
+        const int rows = nj - j0 < s.rows ? nj - j0 : s.rows;
         __syncthreads();
         for (int e = threadIdx.x; e < rows * nl; e += blockDim.x) {
+            const int rr = e / nl, l = e - rr * nl;
             const size_t q = (size_t)j0 * nl + e;
             const bool act = a.mv[(int)occ[q]] != 0;
 #pragma unroll
-            for (int c = 0; c < 3; c++) P[e * 3 + c] = act ? p[c * N + q] : czero();
+            for (int c = 0; c < 3; c++) P[rr * PSR + 3 * l + c] = act ? p[c * N + q] : czero();
         }
         __syncthreads();
-        for (int rr = warp; rr < rows; rr += nw) {
-            float2 t0 = czero(), t1 = czero(), t2 = czero();
-            const float2 *row = P + (size_t)rr * nl * 3;
-#pragma unroll 4
-            for (int l = 0; l < nl; l++) {
-                const float2 e = ez[l * FF_DIRS + lane];
-                t0 = cadd(t0, cmul(e, row[3 * l + 0]));
-                t1 = cadd(t1, cmul(e, row[3 * l + 1]));
-                t2 = cadd(t2, cmul(e, row[3 * l + 2]));
+        for (int rr = rg; rr < rows; rr += s.RG) {
+            float2 t[FF_DPT][3];
+#pragma unroll
+            for (int u = 0; u < FF_DPT; u++)
+#pragma unroll
+                for (int c = 0; c < 3; c++) t[u][c] = czero();
+            const float2 *row = P + rr * PSR;
+#pragma unroll 2
+            for (int l = l0; l < l0 + lcnt; l++) {
+                const float4 e01 = *reinterpret_cast<const float4 *>(ez + (size_t)l * D + FF_DPT * dg);
+                const float4 e23 = *reinterpret_cast<const float4 *>(ez + (size_t)l * D + FF_DPT * dg + 2);
+                const float2 ev[FF_DPT] = {make_float2(e01.x, e01.y), make_float2(e01.z, e01.w),
+                                           make_float2(e23.x, e23.y), make_float2(e23.z, e23.w)};
+                const float2 pv[3] = {row[3 * l], row[3 * l + 1], row[3 * l + 2]};
+#pragma unroll
+                for (int u = 0; u < FF_DPT; u++)
+#pragma unroll
+                    for (int c = 0; c < 3; c++) t[u][c] = cadd(t[u][c], cmul(ev[u], pv[c]));
             }
-            const float2 eyv = ey[(j0 + rr) * FF_DIRS + lane];
-            acc0 = cadd(acc0, cmul(eyv, t0));
-            acc1 = cadd(acc1, cmul(eyv, t1));
-            acc2 = cadd(acc2, cmul(eyv, t2));
+            const float2 *eyr = ey + (size_t)(j0 + rr) * D + FF_DPT * dg;
+#pragma unroll
+            for (int u = 0; u < FF_DPT; u++)
+#pragma unroll
+                for (int c = 0; c < 3; c++) acc[u][c] = cadd(acc[u][c], cmul(eyr[u], t[u][c]));
         }
     }
-    const float2 exv = ex[lane];
-    acc0 = cmul(exv, acc0);
-    acc1 = cmul(exv, acc1);
-    acc2 = cmul(exv, acc2);
-    red[warp][lane][0] = acc0.x; red[warp][lane][1] = acc0.y;
-    red[warp][lane][2] = acc1.x; red[warp][lane][3] = acc1.y;
-    red[warp][lane][4] = acc2.x; red[warp][lane][5] = acc2.y;
+    // x phase, then the sum over row and column groups in FP64
     __syncthreads();
-    if (threadIdx.x < FF_DIRS * 6) {
-        const int dl = threadIdx.x / 6, k = threadIdx.x % 6, d = dbase + dl;
-        double s = 0.0;
-        for (int w = 0; w < nw; w++) s += red[w][dl][k];
-        if (d < a.ndir && s != 0.0) atomicAdd(a.esc_acc + ((size_t)rhs * a.ndir + d) * 6 + k, s);
+    float2 *red = P;   // [threads][FF_DPT][3]
+#pragma unroll
+    for (int u = 0; u < FF_DPT; u++) {
+        const float2 xv = ex[FF_DPT * dg + u];
+#pragma unroll
+        for (int c = 0; c < 3; c++) red[((size_t)threadIdx.x * FF_DPT + u) * 3 + c] = cmul(xv, acc[u][c]);
+    }
+    __syncthreads();
+    for (int o = threadIdx.x; o < D * 6; o += blockDim.x) {
+        const int dl = o / 6, k = o % 6, u = dl % FF_DPT, g = dl / FF_DPT, c = k >> 1;
+        const int dd = dbase + dl;
+        if (dd >= a.ndir) continue;
+        double sum = 0.0;
+        for (int r = 0; r < s.RG * s.LG; r++) {
+            const float2 v = red[((size_t)(g + s.DG * r) * FF_DPT + u) * 3 + c];
+            sum += (k & 1) ? v.y : v.x;
+        }
+        if (sum != 0.0) atomicAdd(a.esc_acc + ((size_t)rhs * a.ndir + dd) * 6 + k, sum);
     }
 }
 
@@ -255,7 +311,13 @@ inline unsigned nblk(size_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
 size_t farfield_smem(int nj, int nl)
 {
-    return ((size_t)(nl + nj) * FF_DIRS + (size_t)FF_ROWS * nl * 3) * sizeof(float2);
+    // the largest shape any direction count gives on this lattice
+    size_t m = 0;
+    for (int nd = FF_DPT; nd <= FF_DMAX; nd += FF_DPT) {
+        const size_t b = ff_smem(ff_shape(nd, nj, nl), nj, nl);
+        m = b > m ? b : m;
+    }
+    return m;
 }
 
 cudaError_t post_prepare(int nj, int nl)
@@ -270,7 +332,10 @@ cudaError_t launch_post(const PostArgs &a, float2 *esc, float *cabs, float *cext
     if ((e = cudaMemsetAsync(a.esc_acc, 0, (size_t)a.nrhs * a.ndir * 6 * sizeof(double), st))) return e;
     if ((e = cudaMemsetAsync(a.cc_acc, 0, (size_t)a.nrhs * 2 * sizeof(double), st))) return e;
     if (a.ndir > 0)
-        farfield_sum<<<dim3(nblk(a.ndir, FF_DIRS), a.ni, a.nrhs), 256, farfield_smem(a.nj, a.nl), st>>>(a);
+    {
+        const FFShape s = ff_shape(a.ndir, a.nj, a.nl);
+        farfield_sum<<<dim3(nblk(a.ndir, s.D), a.ni, a.nrhs), s.threads, ff_smem(s, a.nj, a.nl), st>>>(a, s);
+    }
     cabs_cext_sum<<<dim3(a.ni, a.nrhs), 256, (a.nj + a.nl) * sizeof(float2), st>>>(a);
     const size_t nd = (size_t)a.nrhs * a.ndir;
     const size_t nt = nd > (size_t)a.nrhs ? nd : (size_t)a.nrhs;
@@ -343,7 +408,8 @@ cudaError_t farfield_noalloc(const PostArgs &in, const float *ksc_dev, float2 *e
     if ((e = cudaMemsetAsync(a.esc_acc, 0, (size_t)a.ndir * 6 * sizeof(double), st))) return e;
     const int n3 = 3 * a.ndir;
     ksc_to_double<<<nblk((size_t)n3, 256), 256, 0, st>>>(ksc_dev, kscd, n3);
-    farfield_sum<<<dim3(nblk(a.ndir, FF_DIRS), a.ni, 1), 256, farfield_smem(a.nj, a.nl), st>>>(a);
+    const FFShape s = ff_shape(a.ndir, a.nj, a.nl);
+    farfield_sum<<<dim3(nblk(a.ndir, s.D), a.ni, 1), s.threads, ff_smem(s, a.nj, a.nl), st>>>(a, s);
     post_finalize<<<nblk((size_t)a.ndir, 256), 256, 0, st>>>(a, esc_dev, nullptr, nullptr);
     return cudaGetLastError();
 }
