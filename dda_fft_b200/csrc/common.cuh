@@ -17,6 +17,16 @@ DDA_DEV float2 cmul(float2 a, float2 b)
 {
     return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
 }
+// acc + a * b as four fused multiply-adds
+DDA_DEV float2 cfma(float2 a, float2 b, float2 acc)
+{
+    acc.x = fmaf(a.x, b.x, acc.x);
+    acc.x = fmaf(-a.y, b.y, acc.x);
+    acc.y = fmaf(a.x, b.y, acc.y);
+    acc.y = fmaf(a.y, b.x, acc.y);
+    return acc;
+}
+
 DDA_DEV float2 cmulc(float2 a, float2 b) // a * conj(b)
 {
     return make_float2(fmaf(a.x, b.x, a.y * b.y), fmaf(a.y, b.x, -a.x * b.y));

@@ -18,14 +18,15 @@ namespace ddagpu {
 
 namespace {
 
-// Far-field tiling: a CTA takes one lattice plane i of one right-hand side and up to
-// FF_DMAX directions; a thread accumulates FF_DPT directions x 3 components for the rows
-// rg, rg + RG, ... of each staged group and the columns of its column group lg, so every
-// staged dipole value and phase factor it loads from shared memory feeds 4 to 12 complex
-// multiply-adds.
+// Far-field tiling: a CTA takes FF_PLANES lattice planes i of one right-hand side and up
+// to FF_DMAX directions (the phase tables, one per axis, are built once for them); a
+// thread accumulates FF_DPT directions x 3 components for the rows rg, rg + RG, ... of
+// each staged group and the columns of its column group lg, so every staged dipole value
+// and phase factor it loads from shared memory feeds 4 to 12 complex multiply-adds.
 constexpr int FF_DMAX = 32;
 constexpr int FF_DPT = 4;
 constexpr int FF_CELLS = 2048;   // lattice cells staged per round
+constexpr int FF_PLANES = 8;     // lattice planes per CTA
 
 struct FFShape {
     int D, DG, rows, RG, LG, threads;
@@ -49,48 +50,56 @@ FFShape ff_shape(int ndir, int nj, int nl)
 
 size_t ff_smem(const FFShape &s, int nj, int nl)
 {
-    const size_t tables = (size_t)(nl + nj + 1) * s.D;
+    const size_t tables = (size_t)(nl + nj + FF_PLANES) * s.D;
     const size_t staged = (size_t)s.rows * (3 * nl + 1);
     const size_t red = (size_t)s.threads * FF_DPT * 3;
     return (tables + (staged > red ? staged : red)) * sizeof(float2);
 }
 
-// grid (direction chunks of D, ni, nrhs)
+// grid (direction chunks of D, plane groups of FF_PLANES, nrhs)
 __global__ void __launch_bounds__(256) farfield_sum(PostArgs a, FFShape s)
 {
     extern __shared__ float2 sm[];
     const int nj = a.nj, nl = a.nl, D = s.D;
-    const int dbase = blockIdx.x * D, i = blockIdx.y, rhs = blockIdx.z;
+    const int dbase = blockIdx.x * D, i0 = blockIdx.y * FF_PLANES, rhs = blockIdx.z;
+    const int np = a.ni - i0 < FF_PLANES ? a.ni - i0 : FF_PLANES;
     const int dg = threadIdx.x % s.DG, rest = threadIdx.x / s.DG;
     const int lg = rest % s.LG, rg = rest / s.LG;
     const int PSR = 3 * nl + 1;            // staged row stride (odd: rows fall on other banks)
     float2 *ez = sm;                       // [nl][D]
     float2 *ey = ez + (size_t)nl * D;      // [nj][D]
-    float2 *ex = ey + (size_t)nj * D;      // [D]
-    float2 *P = ex + D;                    // [rows][PSR], later the reduction buffer
+    float2 *ex = ey + (size_t)nj * D;      // [FF_PLANES][D]
+    float2 *P = ex + FF_PLANES * D;        // [rows][PSR], later the reduction buffer
     const double cx = (a.ni - 1) * a.d0 / 2, cy = (nj - 1) * a.d0 / 2, cz = (nl - 1) * a.d0 / 2;
     const double *K = a.ksc + (size_t)rhs * a.ndir * 3;
-    for (int e = threadIdx.x; e < (nl + nj + 1) * D; e += blockDim.x) {
+    for (int e = threadIdx.x; e < (nl + nj + np) * D; e += blockDim.x) {
         const int dl = e % D, pos = e / D, dd = dbase + dl;
         float2 val = czero();
         if (dd < a.ndir) {
             double ph;
             if (pos < nl) ph = K[3 * dd + 2] * (pos * a.d0 - cz);
             else if (pos < nl + nj) ph = K[3 * dd + 1] * ((pos - nl) * a.d0 - cy);
-            else ph = K[3 * dd + 0] * (i * a.d0 - cx);
+            else ph = K[3 * dd + 0] * ((i0 + pos - nl - nj) * a.d0 - cx);
             val = expi_reduced(ph);
         }
         ez[e] = val;   // ez, ey, ex are consecutive [pos][D] blocks
     }
     const size_t N = a.N;
-    const float2 *p = a.p + (size_t)rhs * 3 * N + (size_t)i * nj * nl;
-    const signed char *occ = a.occ + (size_t)rhs * a.occ_stride + (size_t)i * nj * nl;
     const int lcnt = nl / s.LG, l0 = lg * lcnt;
     float2 acc[FF_DPT][3];
 #pragma unroll
     for (int u = 0; u < FF_DPT; u++)
 #pragma unroll
         for (int c = 0; c < 3; c++) acc[u][c] = czero();
+#pragma unroll 1
+    for (int ip = 0; ip < np; ip++) {
+    const int i = i0 + ip;
+    const float2 *p = a.p + (size_t)rhs * 3 * N + (size_t)i * nj * nl;
+    const signed char *occ = a.occ + (size_t)rhs * a.occ_stride + (size_t)i * nj * nl;
+    // x phase of this plane folded into the row factors
+    float2 exv[FF_DPT];
+#pragma unroll
+    for (int u = 0; u < FF_DPT; u++) exv[u] = ex[ip * D + FF_DPT * dg + u];
     for (int j0 = 0; j0 < nj; j0 += s.rows) {
         const int rows = nj - j0 < s.rows ? nj - j0 : s.rows;
         __syncthreads();
@@ -119,24 +128,25 @@ __global__ void __launch_bounds__(256) farfield_sum(PostArgs a, FFShape s)
 #pragma unroll
                 for (int u = 0; u < FF_DPT; u++)
 #pragma unroll
-                    for (int c = 0; c < 3; c++) t[u][c] = cadd(t[u][c], cmul(ev[u], pv[c]));
+                    for (int c = 0; c < 3; c++) t[u][c] = cfma(ev[u], pv[c], t[u][c]);
             }
             const float2 *eyr = ey + (size_t)(j0 + rr) * D + FF_DPT * dg;
 #pragma unroll
-            for (int u = 0; u < FF_DPT; u++)
+            for (int u = 0; u < FF_DPT; u++) {
+                const float2 f = cmul(eyr[u], exv[u]);
 #pragma unroll
-                for (int c = 0; c < 3; c++) acc[u][c] = cadd(acc[u][c], cmul(eyr[u], t[u][c]));
+                for (int c = 0; c < 3; c++) acc[u][c] = cfma(f, t[u][c], acc[u][c]);
+            }
         }
     }
-    // x phase, then the sum over row and column groups in FP64
+    }   // planes of this CTA
+    // the sum over row and column groups in FP64
     __syncthreads();
     float2 *red = P;   // [threads][FF_DPT][3]
 #pragma unroll
-    for (int u = 0; u < FF_DPT; u++) {
-        const float2 xv = ex[FF_DPT * dg + u];
+    for (int u = 0; u < FF_DPT; u++)
 #pragma unroll
-        for (int c = 0; c < 3; c++) red[((size_t)threadIdx.x * FF_DPT + u) * 3 + c] = cmul(xv, acc[u][c]);
-    }
+        for (int c = 0; c < 3; c++) red[((size_t)threadIdx.x * FF_DPT + u) * 3 + c] = acc[u][c];
     __syncthreads();
     for (int o = threadIdx.x; o < D * 6; o += blockDim.x) {
         const int dl = o / 6, k = o % 6, u = dl % FF_DPT, g = dl / FF_DPT, c = k >> 1;
@@ -334,7 +344,8 @@ cudaError_t launch_post(const PostArgs &a, float2 *esc, float *cabs, float *cext
     if (a.ndir > 0)
     {
         const FFShape s = ff_shape(a.ndir, a.nj, a.nl);
-        farfield_sum<<<dim3(nblk(a.ndir, s.D), a.ni, a.nrhs), s.threads, ff_smem(s, a.nj, a.nl), st>>>(a, s);
+        farfield_sum<<<dim3(nblk(a.ndir, s.D), nblk(a.ni, FF_PLANES), a.nrhs), s.threads,
+                       ff_smem(s, a.nj, a.nl), st>>>(a, s);
     }
     cabs_cext_sum<<<dim3(a.ni, a.nrhs), 256, (a.nj + a.nl) * sizeof(float2), st>>>(a);
     const size_t nd = (size_t)a.nrhs * a.ndir;
@@ -409,7 +420,8 @@ cudaError_t farfield_noalloc(const PostArgs &in, const float *ksc_dev, float2 *e
     const int n3 = 3 * a.ndir;
     ksc_to_double<<<nblk((size_t)n3, 256), 256, 0, st>>>(ksc_dev, kscd, n3);
     const FFShape s = ff_shape(a.ndir, a.nj, a.nl);
-    farfield_sum<<<dim3(nblk(a.ndir, s.D), a.ni, 1), s.threads, ff_smem(s, a.nj, a.nl), st>>>(a, s);
+    farfield_sum<<<dim3(nblk(a.ndir, s.D), nblk(a.ni, FF_PLANES), 1), s.threads, ff_smem(s, a.nj, a.nl),
+                   st>>>(a, s);
     post_finalize<<<nblk((size_t)a.ndir, 256), 256, 0, st>>>(a, esc_dev, nullptr, nullptr);
     return cudaGetLastError();
 }
