@@ -12,6 +12,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -110,13 +111,21 @@ struct ddagpu_ctx {
     int *step_dev = nullptr;
     struct GraphKey {
         int solver, nrhs, max_step, nmat1, fast, fx, fyz, tile_x, rows_g, tlen;
-        float tau;
+        float tau, err_max;
         double d0;
         size_t occ_stride;
         const void *trace, *occ;
+        long long post;
     } gkey{};
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t gexec = nullptr;
+    GraphKey wkey{};                 // the whole-solve graph of batched calls
+    cudaGraph_t wgraph = nullptr;
+    cudaGraphExec_t wexec = nullptr;
+    long long w_fixed = 0, w_per_iter = 0;
+    int w_matvec0 = 0, w_matvec_it = 0;
+    int *nact_dev = nullptr;         // [cap] active cells per right-hand side
+    long long post_key = 0;          // shape of the post-processing recorded with a solve
     long long g_per_iter = 0;    // kernels in one recorded iteration
     long long graph_runs = 0;    // graph launches by this context
     std::mutex mu;
@@ -247,9 +256,147 @@ struct SolveResult {
 
 // The solver of DDA_FFT for nrhs right-hand sides whose occ, mv, alpha, kinc and einc are
 // already on the device.  Leaves the final (or rolled-back) dipoles in c->p.
+// The whole solve of a batch as one graph launch: step 0, the iterations as a conditional
+// while node, the rollback and the post-processing.  Captured once per solve shape and
+// kept in the context; the inputs (fields, tables, occupancy, nact) are device buffers
+// the host fills before each launch.
+template <class Step0, class Top, class Body>
+int run_whole_graph(ddagpu_ctx *c, int nrhs, int solver, float tau, int max_step, float err_max,
+                    int nmat1, double d0, int nact, const int *nact_per, SolveResult &res,
+                    Step0 &step0, Top &top, Body &body, const std::function<int()> &post)
+{
+    cudaStream_t st = c->st;
+    std::vector<int> na((size_t)nrhs);
+    for (int k = 0; k < nrhs; k++) na[(size_t)k] = nact_per ? nact_per[k] : nact;
+    CK(cudaMemcpyAsync(c->nact_dev, na.data(), nrhs * sizeof(int), cudaMemcpyHostToDevice, st));
+    ddagpu_ctx::GraphKey key{};
+    key.solver = solver;
+    key.nrhs = nrhs;
+    key.max_step = max_step;
+    key.nmat1 = nmat1;
+    key.fast = c->fast;
+    key.fx = c->fx;
+    key.fyz = c->fyz;
+    key.tile_x = c->tile_x;
+    key.rows_g = c->rows_g;
+    key.tlen = -1;                       // marks the whole-solve graph
+    key.tau = tau;
+    key.err_max = err_max;
+    key.d0 = d0;
+    key.occ_stride = c->occ_stride;
+    key.trace = nullptr;
+    key.occ = c->occ_stride ? (const void *)c->occ_b : (const void *)c->occ;
+    key.post = c->post_key;
+    const long long l_before = c->launches;
+    if (!c->wexec || std::memcmp(&key, &c->wkey, sizeof key) != 0) {
+        if (c->wexec) cudaGraphExecDestroy(c->wexec);
+        if (c->wgraph) cudaGraphDestroy(c->wgraph);
+        c->wexec = nullptr;
+        c->wgraph = nullptr;
+        cudaGraph_t g = nullptr;
+        CK(cudaGraphCreate(&g, 0));
+        auto give_up = [&](int rc, cudaError_t e, const char *what) {
+            cudaStreamCaptureStatus cs;
+            if (cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone) {
+                cudaGraph_t t = nullptr;
+                cudaStreamEndCapture(st, &t);
+                if (t && t != g) cudaGraphDestroy(t);
+            }
+            cudaGraphDestroy(g);
+            if (rc != DDAGPU_OK) return rc;
+            return fail(DDAGPU_ECUDA, std::string("solve graph (") + what + "): " + cudaGetErrorString(e));
+        };
+        cudaGraphConditionalHandle h;
+        cudaError_t e = cudaGraphConditionalHandleCreate(&h, g, 0, 0);
+        if (e != cudaSuccess) return give_up(DDAGPU_OK, e, "handle");
+        const long long l0 = c->launches;
+        // phase 1: fresh state, step 0, the convergence test of step 1, the loop condition
+        e = cudaStreamBeginCaptureToGraph(st, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) return give_up(DDAGPU_OK, e, "capture");
+        int rc = DDAGPU_OK;
+        e = launch_init_state(c->state, c->active, nrhs, (double)err_max, c->nact_dev, st);
+        if (e == cudaSuccess) rc = step0();
+        if (rc == DDAGPU_OK && e == cudaSuccess) e = launch_step_set(c->step_dev, 1, st);
+        if (rc == DDAGPU_OK && e == cudaSuccess) rc = top(max_step, c->step_dev);
+        if (rc == DDAGPU_OK && e == cudaSuccess)
+            e = launch_loop_control(c->active, nrhs, c->step_dev, max_step, h, st);
+        if (rc != DDAGPU_OK || e != cudaSuccess) return give_up(rc, e, "step 0");
+        cudaStreamCaptureStatus cs;
+        const cudaGraphNode_t *deps = nullptr;
+        size_t ndeps = 0;
+        e = cudaStreamGetCaptureInfo(st, &cs, nullptr, nullptr, &deps, &ndeps);
+        if (e != cudaSuccess) return give_up(DDAGPU_OK, e, "capture info");
+        std::vector<cudaGraphNode_t> leaves(deps, deps + ndeps);
+        cudaGraph_t t = nullptr;
+        e = cudaStreamEndCapture(st, &t);
+        if (e != cudaSuccess) return give_up(DDAGPU_OK, e, "end capture");
+        const long long n_head = c->launches - l0 + 3;   // + init, step set, loop control
+        // the while node and its body: one iteration, the next step's test, the condition
+        cudaGraphNodeParams np{};
+        np.type = cudaGraphNodeTypeConditional;
+        np.conditional.handle = h;
+        np.conditional.type = cudaGraphCondTypeWhile;
+        np.conditional.size = 1;
+        cudaGraphNode_t cn;
+        e = cudaGraphAddNode(&cn, g, leaves.data(), leaves.size(), &np);
+        if (e != cudaSuccess) return give_up(DDAGPU_OK, e, "while node");
+        const long long l1 = c->launches;
+        e = cudaStreamBeginCaptureToGraph(st, np.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                          cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) return give_up(DDAGPU_OK, e, "body capture");
+        rc = body(max_step, c->step_dev, true);
+        if (rc == DDAGPU_OK) e = launch_step_advance(c->step_dev, st);
+        if (rc == DDAGPU_OK && e == cudaSuccess) rc = top(max_step, c->step_dev);
+        if (rc == DDAGPU_OK && e == cudaSuccess)
+            e = launch_loop_control(c->active, nrhs, c->step_dev, max_step, h, st);
+        if (rc != DDAGPU_OK || e != cudaSuccess) return give_up(rc, e, "body");
+        e = cudaStreamEndCapture(st, &t);
+        if (e != cudaSuccess) return give_up(DDAGPU_OK, e, "end body capture");
+        const long long n_body = c->launches - l1 + 2;
+        // phase 3: rollback and post-processing after the loop
+        const long long l2 = c->launches;
+        e = cudaStreamBeginCaptureToGraph(st, g, &cn, nullptr, 1, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) return give_up(DDAGPU_OK, e, "tail capture");
+        FieldArgs F = fa_args(c, nrhs, nmat1, d0, tau);
+        e = launch_scalar(c->state, nullptr, nullptr, nrhs, SC_FINAL, 0, nullptr, 0, st);
+        if (e == cudaSuccess) e = launch_gated_copy(F, 1, st);
+        if (e == cudaSuccess) rc = post();
+        if (rc != DDAGPU_OK || e != cudaSuccess) return give_up(rc, e, "tail");
+        e = cudaStreamEndCapture(st, &t);
+        if (e != cudaSuccess) return give_up(DDAGPU_OK, e, "end tail capture");
+        const long long n_tail = c->launches - l2 + 2;
+        cudaGraphExec_t x = nullptr;
+        e = cudaGraphInstantiate(&x, g, 0);
+        if (e != cudaSuccess) return give_up(DDAGPU_OK, e, "instantiate");
+        c->wgraph = g;
+        c->wexec = x;
+        c->wkey = key;
+        c->w_fixed = n_head + n_tail;
+        c->w_per_iter = n_body;
+        c->w_matvec0 = res.matvec0;
+        c->w_matvec_it = res.matvec_it;
+    }
+    c->launches = l_before;
+    CK(cudaGraphLaunch(c->wexec, st));
+    int last = 1;
+    res.st.resize((size_t)nrhs);
+    CK(cudaMemcpyAsync(res.st.data(), c->state, nrhs * sizeof(RhsState), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(&last, c->step_dev, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    c->launches += c->w_fixed + (long long)(last - 1) * c->w_per_iter;
+    res.matvec0 = c->w_matvec0;
+    res.matvec_it = c->w_matvec_it;
+    c->graph_runs += 1;
+    return DDAGPU_OK;
+}
+
+// post (may be null): kernels issued after the solve on the context's stream (far field,
+// cross sections, Mueller); with the solver graph on and no trace, step 0, the iterations,
+// the rollback and post become one graph launch.
 int run_solver(ddagpu_ctx *c, int nrhs, int solver, float tau, int max_step, float err_max,
                int nmat1, double d0, int nact, SolveResult &res, bool want_trace,
-               const float2 *rhs_in = nullptr, const int *nact_per = nullptr)
+               const float2 *rhs_in = nullptr, const int *nact_per = nullptr,
+               const std::function<int()> *post = nullptr)
 {
     if (solver < 0 || solver > 3) return fail(DDAGPU_EINVAL, "solver must be 0..3");
     if (max_step < 0) return fail(DDAGPU_EINVAL, "Max_Step must be >= 0");
@@ -264,17 +411,20 @@ int run_solver(ddagpu_ctx *c, int nrhs, int solver, float tau, int max_step, flo
     }
     double *trace = want_trace ? c->trace : nullptr;
     const int tlen = want_trace ? tl : 0;
-    std::vector<RhsState> init((size_t)nrhs);
-    for (int k = 0; k < nrhs; k++) {
-        RhsState &S = init[(size_t)k];
-        std::memset(&S, 0, sizeof S);
-        S.err_max = (double)err_max;
-        S.active = 1;
-        S.nact = nact_per ? nact_per[k] : nact;
+    const bool whole = post && c->graph_on && !want_trace && !rhs_in;
+    if (!whole) {
+        std::vector<RhsState> init((size_t)nrhs);
+        for (int k = 0; k < nrhs; k++) {
+            RhsState &S = init[(size_t)k];
+            std::memset(&S, 0, sizeof S);
+            S.err_max = (double)err_max;
+            S.active = 1;
+            S.nact = nact_per ? nact_per[k] : nact;
+        }
+        CK(cudaMemcpyAsync(c->state, init.data(), nrhs * sizeof(RhsState), cudaMemcpyHostToDevice, st));
+        std::vector<int> ones((size_t)nrhs, 1);
+        CK(cudaMemcpyAsync(c->active, ones.data(), nrhs * sizeof(int), cudaMemcpyHostToDevice, st));
     }
-    CK(cudaMemcpyAsync(c->state, init.data(), nrhs * sizeof(RhsState), cudaMemcpyHostToDevice, st));
-    std::vector<int> ones((size_t)nrhs, 1);
-    CK(cudaMemcpyAsync(c->active, ones.data(), nrhs * sizeof(int), cudaMemcpyHostToDevice, st));
 
     FieldArgs F = fa_args(c, nrhs, nmat1, d0, tau);
     F.rhs_in = rhs_in;
@@ -293,6 +443,7 @@ int run_solver(ddagpu_ctx *c, int nrhs, int solver, float tau, int max_step, flo
     };
 
     // ---- step 0 (dda_func.cpp:1102-1293): p = p_inc, or the given right-hand side
+    auto step0 = [&]() -> int {
     if (rhs_in) CK(launch_refine(4, F, st));
     else CK(launch_first_approx(F, st));
     c->launches += 1;
@@ -331,6 +482,8 @@ int run_solver(ddagpu_ctx *c, int nrhs, int solver, float tau, int max_step, flo
     CK(scal(SC_START, 0));
     // p_min = p (the step-0 iterate) is copied by the gated copy of the first iteration
     res.matvec_it = (solver == 1 || solver == 2) ? 2 : 1;
+    return DDAGPU_OK;
+    };
 
     // ---- iterations (dda_func.cpp:1301-1535)
     // top of an iteration: convergence test, best-iterate bookkeeping and copy
@@ -340,15 +493,23 @@ int run_solver(ddagpu_ctx *c, int nrhs, int solver, float tau, int max_step, flo
         CK(launch_gated_copy(F, 0, st));
         return DDAGPU_OK;
     };
-    // the solver's recurrences of one iteration (gated per right-hand side by its flag)
-    auto body = [&](int o, const int *sdev) -> int {
+    // the solver's recurrences of one iteration (gated per right-hand side by its flag);
+    // gate_copy: CG's deferred s = r decided on the device (graph of the whole solve)
+    auto body = [&](int o, const int *sdev, bool gate_copy = false) -> int {
         auto sc = [&](int stage) {
             c->launches += 1;
             return launch_scalar(c->state, c->active, c->active, nrhs, stage, o, trace, tlen, st, sdev);
         };
         switch (solver) {
         case 0:
-            if (o == 1) CK(field(OP_COPY_RS));
+            if (gate_copy) {
+                FieldArgs G = F;
+                G.step_gate = sdev;
+                c->launches += 1;
+                CK(launch_field_op(OP_COPY_RS, G, st));
+            } else if (o == 1) {
+                CK(field(OP_COPY_RS));
+            }
             CK(matvec(c->s, c->w, 1.f, c->s, 0));
             CK(field(OP_CG1));
             CK(sc(SC_CG1));
@@ -387,6 +548,9 @@ int run_solver(ddagpu_ctx *c, int nrhs, int solver, float tau, int max_step, flo
         }
         return DDAGPU_OK;
     };
+    if (whole) return run_whole_graph(c, nrhs, solver, tau, max_step, err_max, nmat1, d0, nact,
+                                      nact_per, res, step0, top, body, *post);
+    RET(step0());
     // iteration 1 (and all of them without the graph) from the host: the loop stops when
     // no right-hand side is left active (read back once per iteration)
     const bool use_graph = c->graph_on && max_step >= 2;
@@ -487,6 +651,7 @@ int run_solver(ddagpu_ctx *c, int nrhs, int solver, float tau, int max_step, flo
     CK(launch_scalar(c->state, nullptr, nullptr, nrhs, SC_FINAL, 0, nullptr, 0, st));
     CK(launch_gated_copy(F, 1, st));
     c->launches += 2;
+    if (post) RET((*post)());
     res.st.resize((size_t)nrhs);
     CK(cudaMemcpyAsync(res.st.data(), c->state, nrhs * sizeof(RhsState), cudaMemcpyDeviceToHost, st));
     if (want_trace) {
@@ -624,6 +789,7 @@ int ddagpu_create(ddagpu_ctx **out, int device, int i_max, int j_max, int l_max,
     A(dalloc(&c->active, (size_t)max_rhs));
     A(dalloc(&c->occ, c->N));
     A(dalloc(&c->step_dev, 1));
+    A(dalloc(&c->nact_dev, (size_t)max_rhs));
     A(dalloc(&c->mv, (size_t)c->nmat_cap));
     A(dalloc(&c->alpha, (size_t)c->nmat_cap * max_rhs));
     A(dalloc(&c->kinc, (size_t)3 * max_rhs));
@@ -668,11 +834,13 @@ int ddagpu_destroy(ddagpu_ctx *c)
     if (c->x64) cudaFree(c->x64);
     if (c->gexec) cudaGraphExecDestroy(c->gexec);
     if (c->graph) cudaGraphDestroy(c->graph);
+    if (c->wexec) cudaGraphExecDestroy(c->wexec);
+    if (c->wgraph) cudaGraphDestroy(c->wgraph);
     void *ptrs[] = {c->ahat, c->tw,     c->work,   c->p,       c->pmin,   c->r,     c->s,
                     c->w,    c->g,      c->h,      c->state,   c->active, c->trace, c->occ,
                     c->mv,   c->alpha,  c->kinc,   c->einc,    c->ksc,    c->esc_acc,
                     c->cc_acc, c->normals, c->mueller, c->esc, c->cabs,   c->cext,
-                    c->occ_b, c->ndip, c->step_dev};
+                    c->occ_b, c->ndip, c->step_dev, c->nact_dev};
     for (void *q : ptrs)
         if (q) cudaFree(q);
     if (c->st) cudaStreamDestroy(c->st);
@@ -1003,12 +1171,18 @@ int batch_chunk(ddagpu_ctx *c, const ddagpu_batch_cfg *cfg, const BatchGeom &g, 
     CK(cudaMemcpyAsync(c->normals, nv.data(), nv.size() * sizeof(double), cudaMemcpyHostToDevice, c->st));
     CK(cudaMemcpyAsync(c->alpha, al.data(), al.size() * sizeof(float2), cudaMemcpyHostToDevice, c->st));
     SolveResult res;
+    // far field, cross sections and the plane-averaged Mueller matrices, after the solve
+    // (recorded with it when the solve is one graph launch)
+    const std::function<int()> post = [&]() -> int {
+        RET(run_post(c, nr, nmat1, d0, ndir));
+        MuellerArgs m{no, nP, nA, ndir, c->kinc, c->einc, c->ksc, c->normals, c->esc, c->mueller};
+        CK(launch_mueller(m, c->st));
+        c->launches += 1;
+        return DDAGPU_OK;
+    };
+    c->post_key = ((long long)ndir << 40) | ((long long)no << 24) | ((long long)nP << 12) | nA;
     RET(run_solver(c, nr, cfg->solver, cfg->tau, cfg->max_step, cfg->err_max, nmat1, d0, nact, res,
-                   false, nullptr, nact_per));
-    RET(run_post(c, nr, nmat1, d0, ndir));
-    MuellerArgs m{no, nP, nA, ndir, c->kinc, c->einc, c->ksc, c->normals, c->esc, c->mueller};
-    CK(launch_mueller(m, c->st));
-    c->launches += 1;
+                   false, nullptr, nact_per, &post));
     std::vector<float> ca((size_t)nr), ce((size_t)nr);
     std::vector<double> mo((size_t)no * nA * 16);
     CK(cudaMemcpyAsync(ca.data(), c->cabs, nr * sizeof(float), cudaMemcpyDeviceToHost, c->st));

@@ -75,6 +75,7 @@ __global__ void __launch_bounds__(256) field_op(FieldArgs a)
     __shared__ double scratch[8 * 4];
     const int rhs = blockIdx.y;
     if (a.rhs_active && !a.rhs_active[rhs]) return;
+    if (OP == OP_COPY_RS && a.step_gate && *a.step_gate != 1) return;   // first iteration only
     RhsState &S = a.st[rhs];
     const size_t N = a.N, off = (size_t)rhs * 3 * N;
     float2 *p = a.p ? a.p + off : nullptr, *r = a.r ? a.r + off : nullptr;
@@ -526,12 +527,43 @@ __global__ void __launch_bounds__(256) loop_control(const int *active, int nrhs,
     if (threadIdx.x == 0) cudaGraphSetConditional(h, (any && *step_dev <= max_step) ? 1u : 0u);
 }
 
-// ++*step_dev
-__global__ void step_advance(int *step_dev) { *step_dev += 1; }
+// ++*step_dev, or *step_dev = value
+__global__ void step_advance(int *step_dev, int set, int value)
+{
+    *step_dev = set ? value : *step_dev + 1;
+}
 
 cudaError_t launch_step_advance(int *step_dev, cudaStream_t st)
 {
-    step_advance<<<1, 1, 0, st>>>(step_dev);
+    step_advance<<<1, 1, 0, st>>>(step_dev, 0, 0);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_step_set(int *step_dev, int value, cudaStream_t st)
+{
+    step_advance<<<1, 1, 0, st>>>(step_dev, 1, value);
+    return cudaGetLastError();
+}
+
+// Fresh solver state for a solve recorded in a graph (the host loop uploads it instead):
+// all scalars zero, the threshold, active, and the active-cell count of each right-hand side.
+__global__ void init_state(RhsState *st, int *active, int nrhs, double err_max, const int *nact)
+{
+    const int rhs = blockIdx.x * blockDim.x + threadIdx.x;
+    if (rhs >= nrhs) return;
+    RhsState S;
+    memset(&S, 0, sizeof S);
+    S.err_max = err_max;
+    S.active = 1;
+    S.nact = nact[rhs];
+    st[rhs] = S;
+    active[rhs] = 1;
+}
+
+cudaError_t launch_init_state(RhsState *st_, int *active, int nrhs, double err_max, const int *nact,
+                              cudaStream_t st)
+{
+    init_state<<<(nrhs + 127) / 128, 128, 0, st>>>(st_, active, nrhs, err_max, nact);
     return cudaGetLastError();
 }
 

@@ -39,6 +39,7 @@ struct FieldArgs {
     float2 *rb;               // [nrhs][3][N] right-hand side of the inner solve (float r)
     double2 *x64;             // [nrhs][3][N] FP64 solution
     const float2 *rhs_in;     // step 0 starts from p = rhs_in instead of p_inc when set
+    const int *step_gate;     // OP_COPY_RS runs only when *step_gate == 1 (if set)
 };
 
 cudaError_t launch_field_op(int op, const FieldArgs &a, cudaStream_t st);
@@ -52,6 +53,9 @@ cudaError_t launch_scalar(RhsState *st_, const int *act_in, int *act_out, int nr
 cudaError_t launch_loop_control(const int *active, int nrhs, const int *step_dev, int max_step,
                                 cudaGraphConditionalHandle h, cudaStream_t st);
 cudaError_t launch_step_advance(int *step_dev, cudaStream_t st);
+cudaError_t launch_step_set(int *step_dev, int value, cudaStream_t st);
+cudaError_t launch_init_state(RhsState *st_, int *active, int nrhs, double err_max, const int *nact,
+                              cudaStream_t st);
 cudaError_t launch_gated_copy(const FieldArgs &a, int dir, cudaStream_t st);
 
 // refinement passes: 0 x64 = b; 1 r = b - (x64 - alpha conv) with conv in w, error into
