@@ -156,8 +156,22 @@ void twiddles(int n, float2 *out)
         out[n + j] = make_float2((float)std::cos(-pi * j / n), (float)std::sin(-pi * j / n));
 }
 
+// Forget the recorded solve graphs (they hold buffer addresses about to change).
+void drop_graphs(ddagpu_ctx *c)
+{
+    if (c->gexec) cudaGraphExecDestroy(c->gexec);
+    if (c->graph) cudaGraphDestroy(c->graph);
+    if (c->wexec) cudaGraphExecDestroy(c->wexec);
+    if (c->wgraph) cudaGraphDestroy(c->wgraph);
+    c->gexec = nullptr;
+    c->graph = nullptr;
+    c->wexec = nullptr;
+    c->wgraph = nullptr;
+}
+
 int ensure_post(ddagpu_ctx *c, int ndir, int nplanes, int nangles)
 {
+    if (ndir > c->ndir_cap || nplanes > c->nplane_cap || nangles > c->nangle_cap) drop_graphs(c);
     if (ndir > c->ndir_cap) {
         cudaFree(c->ksc);
         cudaFree(c->esc_acc);

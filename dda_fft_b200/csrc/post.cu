@@ -84,6 +84,7 @@ __global__ void __launch_bounds__(256) farfield_sum(PostArgs a, FFShape s)
         }
         ez[e] = val;   // ez, ey, ex are consecutive [pos][D] blocks
     }
+    __syncthreads();   // the tables are read below before the first staging barrier
     const size_t N = a.N;
     const int lcnt = nl / s.LG, l0 = lg * lcnt;
     float2 acc[FF_DPT][3];
