@@ -217,14 +217,16 @@ int ddagpu_anthrax_rasterize(int device, int i_max, int j_max, int l_max, const 
 int ddagpu_set_fast_variant(ddagpu_ctx *ctx, int x_variant, int yz_variant);
 int ddagpu_get_fast_variant(ddagpu_ctx *ctx, int *x_variant, int *yz_variant);
 
-/* Solver iterations as a CUDA graph (no counterpart in the reference, whose loop is on
- * the host, dda_func.cpp:1301-1535).  On (the default), iterations 2..Max_Step of every
- * solve run as one graph launch: a conditional while node whose body is one iteration
- * and whose last kernel advances a device step counter and stops the loop when no
- * right-hand side is active or Max_Step is reached, so the host no longer reads the
- * active flags back every iteration.  The graph is kept per context and rebuilt when the
- * solve's shape (solver, right-hand sides, Max_Step, materials, kernels) changes.
- * Results are the same kernels in the same order as with the host loop. */
+/* Solves as CUDA graphs (no counterpart in the reference, whose loop is on the host,
+ * dda_func.cpp:1301-1535).  On (the default): every chunk of a batched call
+ * (ddagpu_orientation_solves, ddagpu_realization_solves, ddagpu_agglomerate_solves) is one
+ * graph launch -- state set-up, step 0, the iterations as a conditional while node whose
+ * body ends with a kernel that stops the loop when no right-hand side is active or
+ * Max_Step is reached, the rollback and the post-processing; the single-solve entry
+ * points run iterations 2..Max_Step that way.  The host no longer reads the active flags
+ * back every iteration.  Graphs are kept per context and rebuilt when the solve's shape
+ * (solver, right-hand sides, Max_Step, materials, kernels, directions) changes.  Results
+ * are the same kernels in the same order as with the host loop (off). */
 int ddagpu_set_solver_graph(ddagpu_ctx *ctx, int on);
 long long ddagpu_solver_graph_runs(ddagpu_ctx *ctx);   /* graph launches so far */
 
