@@ -184,7 +184,10 @@ def main():
                     help="only run the matvec on NRHS right-hand sides (for ncu captures)")
     ap.add_argument("--grid", type=int, default=GRID)
     ap.add_argument("--variant", type=int, nargs=2, default=None, metavar=("X", "YZ"),
-                    help="with --profile-matvec: launch variants instead of autotuning")
+                    help="launch variants of the specialised passes instead of autotuning")
+    ap.add_argument("--no-graph", action="store_true",
+                    help="host-driven solver loop instead of one graph launch per batch (for "
+                         "per-kernel launch lists: profilers list graph-launched kernels apart)")
     ap.add_argument("--workload", default="orientations",
                     choices=["orientations", "precision", "adjoint", "realizations", "plain",
                              "solver_graph"])
@@ -223,7 +226,12 @@ def main():
     occ = ellipsoid_occ()
     kd = 2 * X / GRID
     ctx = D.Context(GRID, kd, max_rhs=2 * B, device=dev)
-    ctx.autotune(2 * B)          # pass variants and tiling for this batch (set-up, not timed)
+    if args.variant:
+        ctx.set_fast_variant(*args.variant)
+    else:
+        ctx.autotune(2 * B)      # pass variants and tiling for this batch (set-up, not timed)
+    if args.no_graph:
+        ctx.set_solver_graph(False)
     stream = torch.cuda.ExternalStream(ctx.stream_ptr, device=dev)
     # every rank draws its own contiguous run of the reference's MC stream (worker 0)
     total = (W + K) * B * world
@@ -364,7 +372,8 @@ def main():
                        "rhs_per_step": 2 * B, "parallelism": f"orientations sharded over {world} GPU(s)",
                        "l2": "working set per step >> L2 (126 MB): no flush needed",
                        "tiling": list(ctx.tiling()), "fast_passes": ctx.fast_kernels,
-                       "fast_variant": list(ctx.fast_variant)},
+                       "fast_variant": list(ctx.fast_variant),
+                       "solve_graph": not args.no_graph},
             "e2e": {"value": e2e, "unit": "orientation-solves/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "plain_gpu": {"value": plain, "unit": "orientation-solves/s",
