@@ -7,6 +7,7 @@ executable (oracle/_ref/dda_fft.out).  Run in a container that has the reference
 
     make -f oracle/Makefile all && python tests/golden/make_golden.py
     python tests/golden/make_golden.py targets          # targets_v72.npz
+    python tests/golden/make_golden.py configs          # configs_v72.npz (64^3, minutes)
 
 The fixtures are small (.npz, a few MB in all) and are committed; the tests read
 them without needing the reference.
@@ -214,7 +215,33 @@ def agglomerates(R, out):
         out[f"{name}_count_next"] = np.array([n, nxt], np.int64)
 
 
+def full_configs(R, R64, out):
+    """The mid and batching configurations at their full 64^3 size through the reference's
+    sample loop (float and FP64 builds, one worker): sums of Cabs, Cext and the Mueller
+    matrices, as the .dst holds them."""
+    cfgs = {
+        # 64^3 sphere, x = 8, m = 1.5+0.01i, LDR, BiCGStab, 100 steps, 12 planes, step 1 deg
+        "c2": (make_run_cfg(grid=64, target=1, x=8.0, materials=((1.5, 0.01),), polarizability=5,
+                            solver=2, max_step=100, nplanes=12, theta_step=1.0, seed=1), 1),
+        # 64^3 ellipsoid 0.7/0.5, x = 6, m = 1.55+0.005i, CM, CG, MC orientations seed 7
+        "c3a32": (make_run_cfg(grid=64, target=2, b_a=0.7, c_a=0.5, x=6.0,
+                               materials=((1.55, 0.005),), orientation=1, seed=7), 32),
+    }
+    for name, (cfg, ns) in cfgs.items():
+        _, ca, ce, mm = R.run_samples(cfg, ns, 1)
+        out[name] = np.concatenate([[ca, ce], mm.ravel()])
+        _, ca, ce, mm = R64.run_samples(cfg, ns, 1)
+        out[name + "_64"] = np.concatenate([[ca, ce], mm.ravel()])
+
+
 def main():
+    if sys.argv[1:] == ["configs"]:
+        out: dict = {}
+        full_configs(RefLib(), RefLib(REF64_SO), out)
+        path = os.path.join(HERE, "configs_v72.npz")
+        np.savez_compressed(path, **out)
+        print(f"wrote {path}: {os.path.getsize(path) / 1e6:.2f} MB, {len(out)} arrays")
+        return
     if sys.argv[1:] == ["targets"]:
         out: dict = {}
         agglomerates(RefLib(), out)
