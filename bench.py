@@ -432,7 +432,7 @@ def precision_run(args):
     out = {"workload": "precision: 128^3 sphere x=16 m=1.6+0.0005i BiCGStab, 91 angles",
            "kernels": None}
     esc = {"plain": [], "refined": []}
-    with D.Context(n, kd) as ctx:
+    with D.Context(n, kd, max_rhs=2) as ctx:
         out["kernels"] = "specialised" if ctx.fast_kernels else "generic"
         for q, e in enumerate(((1, 0, 0), (0, 1, 0))):
             t0 = time.perf_counter()
