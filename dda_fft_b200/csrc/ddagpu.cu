@@ -125,6 +125,7 @@ struct ddagpu_ctx {
     long long w_fixed = 0, w_per_iter = 0;
     int w_matvec0 = 0, w_matvec_it = 0;
     int *nact_dev = nullptr;         // [cap] active cells per right-hand side
+    int *err_dev = nullptr;          // set by a kernel whose bounded wait gave up
     long long post_key = 0;          // shape of the post-processing recorded with a solve
     long long g_per_iter = 0;    // kernels in one recorded iteration
     long long graph_runs = 0;    // graph launches by this context
@@ -154,6 +155,16 @@ void twiddles(int n, float2 *out)
         out[k] = make_float2((float)std::cos(-2.0 * pi * k / n), (float)std::sin(-2.0 * pi * k / n));
     for (int j = 0; j < n; j++)
         out[n + j] = make_float2((float)std::cos(-pi * j / n), (float)std::sin(-pi * j / n));
+}
+
+// A kernel of the context gave up a bounded wait (its bulk copies did not complete):
+// report it and clear the flag for the next call.
+int device_wait_error(ddagpu_ctx *c, int flag)
+{
+    if (!flag) return DDAGPU_OK;
+    cudaMemsetAsync(c->err_dev, 0, sizeof(int), c->st);
+    cudaStreamSynchronize(c->st);
+    return fail(DDAGPU_ECUDA, "a device wait ran out (asynchronous copy not completed)");
 }
 
 // Forget the recorded solve graphs (they hold buffer addresses about to change).
@@ -226,6 +237,7 @@ MatvecArgs mv_args(ddagpu_ctx *c, int nrhs, const float2 *src, float2 *out, int 
     a.fast = c->fast;
     a.fx = c->fx;
     a.fyz = c->fyz;
+    a.err = c->err_dev;
     return a;
 }
 
@@ -396,7 +408,10 @@ int run_whole_graph(ddagpu_ctx *c, int nrhs, int solver, float tau, int max_step
     res.st.resize((size_t)nrhs);
     CK(cudaMemcpyAsync(res.st.data(), c->state, nrhs * sizeof(RhsState), cudaMemcpyDeviceToHost, st));
     CK(cudaMemcpyAsync(&last, c->step_dev, sizeof(int), cudaMemcpyDeviceToHost, st));
+    int werr = 0;
+    CK(cudaMemcpyAsync(&werr, c->err_dev, sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
+    RET(device_wait_error(c, werr));
     c->launches += c->w_fixed + (long long)(last - 1) * c->w_per_iter;
     res.matvec0 = c->w_matvec0;
     res.matvec_it = c->w_matvec_it;
@@ -673,7 +688,10 @@ int run_solver(ddagpu_ctx *c, int nrhs, int solver, float tau, int max_step, flo
         CK(cudaMemcpyAsync(res.trace.data(), c->trace, res.trace.size() * sizeof(double),
                            cudaMemcpyDeviceToHost, st));
     }
+    int werr = 0;
+    CK(cudaMemcpyAsync(&werr, c->err_dev, sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
+    RET(device_wait_error(c, werr));
     return DDAGPU_OK;
 }
 
@@ -804,6 +822,7 @@ int ddagpu_create(ddagpu_ctx **out, int device, int i_max, int j_max, int l_max,
     A(dalloc(&c->occ, c->N));
     A(dalloc(&c->step_dev, 1));
     A(dalloc(&c->nact_dev, (size_t)max_rhs));
+    A(dalloc(&c->err_dev, 1));
     A(dalloc(&c->mv, (size_t)c->nmat_cap));
     A(dalloc(&c->alpha, (size_t)c->nmat_cap * max_rhs));
     A(dalloc(&c->kinc, (size_t)3 * max_rhs));
@@ -834,6 +853,8 @@ int ddagpu_create(ddagpu_ctx **out, int device, int i_max, int j_max, int l_max,
         (e = cudaStreamSynchronize(c->st)) != cudaSuccess)
         return bail(fail(DDAGPU_ECUDA, std::string("setup: ") + cudaGetErrorString(e)));
     c->fast = matvec_fast_supported(c->L) ? 1 : 0;
+    if (cudaMemset(c->err_dev, 0, sizeof(int)) != cudaSuccess)
+        return bail(fail(DDAGPU_ECUDA, "setup: error flag"));
     *out = c;
     return DDAGPU_OK;
 }
@@ -854,7 +875,7 @@ int ddagpu_destroy(ddagpu_ctx *c)
                     c->w,    c->g,      c->h,      c->state,   c->active, c->trace, c->occ,
                     c->mv,   c->alpha,  c->kinc,   c->einc,    c->ksc,    c->esc_acc,
                     c->cc_acc, c->normals, c->mueller, c->esc, c->cabs,   c->cext,
-                    c->occ_b, c->ndip, c->step_dev, c->nact_dev};
+                    c->occ_b, c->ndip, c->step_dev, c->nact_dev, c->err_dev};
     for (void *q : ptrs)
         if (q) cudaFree(q);
     if (c->st) cudaStreamDestroy(c->st);
@@ -975,8 +996,8 @@ int ddagpu_autotune(ddagpu_ctx *c, int nrhs)
     if (matvec_fast_supported(c->L)) {
         // the compile-time-sized passes in each launch variant
         c->fast = 1;
-        for (int vx = 0; vx < kFastVariants; vx++)
-            for (int vyz = 0; vyz < kFastVariants; vyz++) {
+        for (int vx = 0; vx < kXVariants; vx++)
+            for (int vyz = 0; vyz < kYZVariants; vyz++) {
                 c->fx = vx;
                 c->fyz = vyz;
                 float ms = 0;
@@ -1710,8 +1731,8 @@ int ddagpu_anthrax_rasterize(int device, int i_max, int j_max, int l_max, const 
 int ddagpu_set_fast_variant(ddagpu_ctx *c, int x_variant, int yz_variant)
 {
     if (!c) return fail(DDAGPU_EINVAL, "null context");
-    if (x_variant < 0 || x_variant >= kFastVariants || yz_variant < 0 || yz_variant >= kFastVariants)
-        return fail(DDAGPU_EINVAL, "launch variants are 0, 1 or 2");
+    if (x_variant < 0 || x_variant >= kXVariants || yz_variant < 0 || yz_variant >= kYZVariants)
+        return fail(DDAGPU_EINVAL, "launch variants: x 0..5, y/z 0..2");
     std::lock_guard<std::mutex> lk(c->mu);
     c->fx = x_variant;
     c->fyz = yz_variant;

@@ -68,7 +68,8 @@ struct MatvecArgs {
     int tile_x;             // columns per CTA of the x pass (generic kernels)
     int rows_g;             // rows per staging group of the y/z passes (generic kernels)
     int fast;               // 1: compile-time-sized kernels of matvec_fast.cu
-    int fx, fyz;            // launch variants of the fast x pass and y/z passes (0 default .. 2)
+    int fx, fyz;            // launch variants of the fast x pass (0..5) and y/z passes (0..2)
+    int *err;               // device flag set by a kernel whose bounded wait gave up (or null)
 };
 
 // kernels (matvec.cu)
@@ -79,7 +80,8 @@ cudaError_t matvec_prepare(const Lat &L, int tile_x, int rows_g);
 
 // compile-time-sized passes for edges in {16, 32, 64} (matvec_fast.cu)
 bool matvec_fast_supported(const Lat &L);
-constexpr int kFastVariants = 3;   // launch variants per fast pass
+constexpr int kXVariants = 6;      // launch variants of the fast x pass
+constexpr int kYZVariants = 3;     // launch variants of the fast y/z passes
 cudaError_t matvec_fast_prepare(const Lat &L);
 cudaError_t launch_matvec_fast(const MatvecArgs &a, cudaStream_t st);
 

@@ -180,12 +180,51 @@ constexpr int k2_min_blocks(int NI, int threads)
     return NI == 16 ? (6 * 128) / threads : (512 / threads > 0 ? 512 / threads : 1);
 }
 
-template <int NI, int TL>
+// ---- bulk asynchronous copies (the copy engine moves global rows into shared memory and
+// signals an mbarrier; no multicast)
+DDA_DEV unsigned smem_addr(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+DDA_DEV void mbar_init(unsigned long long *bar, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+DDA_DEV void mbar_expect_tx(unsigned long long *bar, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+
+DDA_DEV void bulk_g2s(void *dst, const void *src, unsigned bytes, unsigned long long *bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+                     "r"(smem_addr(dst)), "l"(src), "r"(bytes), "r"(smem_addr(bar))
+                 : "memory");
+}
+
+// Waits for the barrier's phase `parity` to complete, at most ~2^22 polls; false if it did
+// not (the caller reports it through the error flag instead of hanging).
+DDA_DEV bool mbar_wait(unsigned long long *bar, unsigned parity)
+{
+    const unsigned a = smem_addr(bar);
+    for (int it = 0; it < (1 << 22); it++) {
+        unsigned done;
+        asm volatile("{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+                     : "=r"(done)
+                     : "r"(a), "r"(parity)
+                     : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+template <int NI, int TL, bool BULK>
 __global__ void __launch_bounds__(Sp<NI>::RM * TL, k2_min_blocks(NI, Sp<NI>::RM * TL)) k2f(MatvecArgs a)
 {
     using S = Sp<NI>;
     constexpr int R1 = S::R1, R2 = S::R2, RM = S::RM;
-    extern __shared__ float2 B[];   // [6][NI][TL]
+    extern __shared__ __align__(128) float2 B[];   // [6][NI][TL]
     const int js = blockIdx.x, rhs = blockIdx.z;
     if (a.rhs_active && !a.rhs_active[rhs]) return;
     const int nj = a.L.nj, nl = a.L.nl;
@@ -196,6 +235,49 @@ __global__ void __launch_bounds__(Sp<NI>::RM * TL, k2_min_blocks(NI, Sp<NI>::RM 
     const float2 *tw = a.L.tw_i, *hw = a.L.tw_i + NI;
     auto Bat = [&](int c, int h, int pos) -> float2 & { return B[((c * 2 + h) * NI + pos) * TL + t]; };
 
+    // ---- bulk variant: the 3 x NI input rows of TL columns arrive in the half-0 planes of B
+    // by asynchronous bulk copies (one per row, 16-byte aligned: l0 and TL are multiples
+    // of 4 float2); step A then reads them from shared memory and works in place
+    if constexpr (BULK && R2 > 1) {
+        __shared__ __align__(8) unsigned long long bar;
+        if (threadIdx.x == 0) {
+            mbar_init(&bar, 1);
+            mbar_expect_tx(&bar, 3u * NI * TL * (unsigned)sizeof(float2));
+        }
+        __syncthreads();
+        const float2 *row0 = a.work + (size_t)rhs * a.wstride + (size_t)js * (2 * nl) + l0;
+        for (int q = threadIdx.x; q < 3 * NI; q += blockDim.x) {
+            const int c = q / NI, i = q - c * NI;
+            bulk_g2s(&B[((c * 2) * NI + i) * TL], row0 + c * cstr + (size_t)i * plane,
+                     TL * (unsigned)sizeof(float2), &bar);
+        }
+        const bool got = mbar_wait(&bar, 0);
+        if (!__syncthreads_and(got)) {   // the same decision for every thread
+            if (threadIdx.x == 0 && a.err) atomicExch(a.err, 1);
+            mbar_wait(&bar, 0);           // one more bounded wait for the copies in flight
+            return;
+        }
+        if (sub < R2) {
+            auto step_a_smem = [&](int c) {
+                float2 v[R1], w[R1];
+#pragma unroll
+                for (int r = 0; r < R1; r++) {
+                    v[r] = Bat(c, 0, sub + R2 * r);
+                    w[r] = cmul(v[r], __ldg(&hw[sub + R2 * r]));
+                }
+                dft_reg<R1, false>(v);
+                dft_reg<R1, false>(w);
+#pragma unroll
+                for (int k1 = 0; k1 < R1; k1++) {
+                    const float2 tk = k1 ? twid<false>(tw, sub * k1) : make_float2(1.f, 0.f);
+                    Bat(c, 0, sub + R2 * k1) = k1 ? cmul(v[k1], tk) : v[k1];
+                    Bat(c, 1, sub + R2 * k1) = k1 ? cmul(w[k1], tk) : w[k1];
+                }
+            };
+#pragma unroll 1
+            for (int c = 0; c < 3; c++) step_a_smem(c);
+        }
+    } else
     // ---- forward step A (both halves from one load)
     if (R2 == 1) {
         if (sub == 0) {
@@ -231,7 +313,9 @@ __global__ void __launch_bounds__(Sp<NI>::RM * TL, k2_min_blocks(NI, Sp<NI>::RM 
                 Bat(c, 1, sub + R2 * k1) = k1 ? cmul(w[k1], tk) : w[k1];
             }
         };
-        if constexpr (3 * R1 <= 24) {
+        if constexpr (BULK) {
+            // unreachable: the bulk variant loads below, before this branch
+        } else if constexpr (3 * R1 <= 24) {
             // all three components' loads in flight before any arithmetic
             float2 v0[R1], v1[R1], v2[R1];
 #pragma unroll
@@ -566,28 +650,35 @@ constexpr int x_tile(int v)
     return t0 >> v;
 }
 
+// x variants 0..2: register loads with 32 / 16 / 8 columns (16 / 8 / 4 at edge 128);
+// 3..5: the same tiles fed by bulk asynchronous copies
 template <int NI, int V>
 void launch_x_v(const MatvecArgs &a, cudaStream_t st)
 {
-    constexpr int TL = x_tile<NI>(V);
+    constexpr int TL = x_tile<NI>(V % 3);
     const int ncol = 2 * a.L.nl;
     const size_t smem = (size_t)6 * NI * TL * sizeof(float2);
-    k2f<NI, TL><<<dim3(2 * a.L.nj, ncol / TL, a.nrhs), Sp<NI>::RM * TL, smem, st>>>(a);
+    k2f<NI, TL, (V >= 3)><<<dim3(2 * a.L.nj, ncol / TL, a.nrhs), Sp<NI>::RM * TL, smem, st>>>(a);
 }
 
 template <int NI>
 void launch_x(const MatvecArgs &a, cudaStream_t st)
 {
-    if (a.fx == 2) launch_x_v<NI, 2>(a, st);
-    else if (a.fx == 1) launch_x_v<NI, 1>(a, st);
-    else launch_x_v<NI, 0>(a, st);
+    switch (a.fx) {
+    case 5: launch_x_v<NI, 5>(a, st); break;
+    case 4: launch_x_v<NI, 4>(a, st); break;
+    case 3: launch_x_v<NI, 3>(a, st); break;
+    case 2: launch_x_v<NI, 2>(a, st); break;
+    case 1: launch_x_v<NI, 1>(a, st); break;
+    default: launch_x_v<NI, 0>(a, st); break;
+    }
 }
 
 template <int NI, int V>
 cudaError_t prep_x_v()
 {
-    constexpr int TL = x_tile<NI>(V);
-    return cudaFuncSetAttribute(k2f<NI, TL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    constexpr int TL = x_tile<NI>(V % 3);
+    return cudaFuncSetAttribute(k2f<NI, TL, (V >= 3)>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)(6 * NI * TL * sizeof(float2)));
 }
 
@@ -596,7 +687,10 @@ cudaError_t prep_x()
 {
     cudaError_t e = prep_x_v<NI, 0>();
     if (e == cudaSuccess) e = prep_x_v<NI, 1>();
-    return e == cudaSuccess ? prep_x_v<NI, 2>() : e;
+    if (e == cudaSuccess) e = prep_x_v<NI, 2>();
+    if (e == cudaSuccess) e = prep_x_v<NI, 3>();
+    if (e == cudaSuccess) e = prep_x_v<NI, 4>();
+    return e == cudaSuccess ? prep_x_v<NI, 5>() : e;
 }
 
 bool fast_edge(int n) { return n == 16 || n == 32 || n == 64 || n == 128; }

@@ -210,8 +210,10 @@ int ddagpu_anthrax_rasterize(int device, int i_max, int j_max, int l_max, const 
                              int count, signed char *occ, int *ndip);
 
 /* Launch variants of the compile-time-sized matvec passes (edges 16..128): x_variant
- * 0/1/2 = 32, 16 or 8 spectral columns per x-pass CTA (16, 8, 4 at edge 128); yz_variant
- * 0/1/2 = the default block size of the y/z passes, the other of 256 / 512, or 128 threads.
+ * 0/1/2 = 32, 16 or 8 spectral columns per x-pass CTA (16, 8, 4 at edge 128), 3/4/5 = the
+ * same with the input rows moved into shared memory by bulk asynchronous copies;
+ * yz_variant 0/1/2 = the default block size of the y/z passes, the other of 256 / 512, or
+ * 128 threads.
  * ddagpu_autotune times every combination (and the generic passes) and keeps the
  * fastest.  No counterpart in the reference. */
 int ddagpu_set_fast_variant(ddagpu_ctx *ctx, int x_variant, int yz_variant);

@@ -145,7 +145,7 @@ def test_fast_launch_variants_agree(D, oracle, grid):
     with D.Context(grid, kd, max_rhs=2) as ctx:
         x = torch.from_numpy(p).cuda()
         outs = []
-        for vx in (0, 1, 2):
+        for vx in range(6):          # 3..5: x pass fed by bulk asynchronous copies
             for vyz in (0, 1, 2):
                 ctx.set_fast_variant(vx, vyz)
                 assert ctx.fast_variant == (vx, vyz)
