@@ -118,6 +118,7 @@ def lib():
         L.ddagpu_set_fast_variant.argtypes = [_p, _i, _i]
         L.ddagpu_get_fast_variant.argtypes = [_p, C.POINTER(_i), C.POINTER(_i)]
         L.ddagpu_set_solver_graph.argtypes = [_p, _i]
+        L.ddagpu_selftest_wait_timeout.argtypes = [_p, _i]
         L.ddagpu_solver_graph_runs.argtypes = [_p]
         L.ddagpu_solver_graph_runs.restype = C.c_longlong
         L.ddagpu_rng_seed.argtypes = [C.c_ulonglong, _i]
@@ -556,6 +557,10 @@ class Context:
         x, yz = _i(), _i()
         _check(lib().ddagpu_get_fast_variant(self._h, C.byref(x), C.byref(yz)))
         return x.value, yz.value
+
+    def selftest_wait_timeout(self, on: bool):
+        """Diagnostic: make the bulk-copy x pass's bounded wait run out (see the header)."""
+        _check(lib().ddagpu_selftest_wait_timeout(self._h, int(on)))
 
     def set_solver_graph(self, on: bool):
         """Iterations 2..Max_Step of each solve as one CUDA graph launch (default on)."""

@@ -126,6 +126,7 @@ struct ddagpu_ctx {
     int w_matvec0 = 0, w_matvec_it = 0;
     int *nact_dev = nullptr;         // [cap] active cells per right-hand side
     int *err_dev = nullptr;          // set by a kernel whose bounded wait gave up
+    int wait_selftest = 0;           // 1: the x pass's wait waits for a phase nothing completes
     long long post_key = 0;          // shape of the post-processing recorded with a solve
     long long g_per_iter = 0;    // kernels in one recorded iteration
     long long graph_runs = 0;    // graph launches by this context
@@ -238,6 +239,7 @@ MatvecArgs mv_args(ddagpu_ctx *c, int nrhs, const float2 *src, float2 *out, int 
     a.fx = c->fx;
     a.fyz = c->fyz;
     a.err = c->err_dev;
+    a.wait_selftest = c->wait_selftest;
     return a;
 }
 
@@ -1035,7 +1037,10 @@ int ddagpu_convolution(ddagpu_ctx *c, const float *p, float *out, int conj)
     MatvecArgs a = mv_args(c, 1, c->p, c->r, 0, 0.f, nullptr, conj ? 1 : 0, 1, false);
     CK(launch_matvec(a, c->st));
     CK(cudaMemcpyAsync(soa.data(), c->r, 3 * N * sizeof(float2), cudaMemcpyDeviceToHost, c->st));
+    int werr = 0;
+    CK(cudaMemcpyAsync(&werr, c->err_dev, sizeof(int), cudaMemcpyDeviceToHost, c->st));
     CK(cudaStreamSynchronize(c->st));
+    RET(device_wait_error(c, werr));
     for (size_t q = 0; q < N; q++)
         for (int k = 0; k < 3; k++) {
             out[6 * q + 2 * k] = soa[k * N + q].x;
@@ -1744,6 +1749,15 @@ int ddagpu_get_fast_variant(ddagpu_ctx *c, int *x_variant, int *yz_variant)
     if (!c || !x_variant || !yz_variant) return fail(DDAGPU_EINVAL, "null argument");
     *x_variant = c->fx;
     *yz_variant = c->fyz;
+    return DDAGPU_OK;
+}
+
+int ddagpu_selftest_wait_timeout(ddagpu_ctx *c, int on)
+{
+    if (!c) return fail(DDAGPU_EINVAL, "null context");
+    std::lock_guard<std::mutex> lk(c->mu);
+    c->wait_selftest = on ? 1 : 0;
+    drop_graphs(c);   // recorded launches hold the old setting
     return DDAGPU_OK;
 }
 

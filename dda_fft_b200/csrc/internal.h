@@ -70,6 +70,7 @@ struct MatvecArgs {
     int fast;               // 1: compile-time-sized kernels of matvec_fast.cu
     int fx, fyz;            // launch variants of the fast x pass (0..5) and y/z passes (0..2)
     int *err;               // device flag set by a kernel whose bounded wait gave up (or null)
+    int wait_selftest;      // 1: the bulk-copy wait waits (briefly) for a phase that never completes
 };
 
 // kernels (matvec.cu)

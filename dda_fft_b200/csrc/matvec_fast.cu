@@ -203,12 +203,12 @@ DDA_DEV void bulk_g2s(void *dst, const void *src, unsigned bytes, unsigned long 
                  : "memory");
 }
 
-// Waits for the barrier's phase `parity` to complete, at most ~2^22 polls; false if it did
+// Waits for the barrier's phase `parity` to complete, at most `polls` polls; false if it did
 // not (the caller reports it through the error flag instead of hanging).
-DDA_DEV bool mbar_wait(unsigned long long *bar, unsigned parity)
+DDA_DEV bool mbar_wait(unsigned long long *bar, unsigned parity, int polls = 1 << 22)
 {
     const unsigned a = smem_addr(bar);
-    for (int it = 0; it < (1 << 22); it++) {
+    for (int it = 0; it < polls; it++) {
         unsigned done;
         asm volatile("{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
                      : "=r"(done)
@@ -251,7 +251,9 @@ __global__ void __launch_bounds__(Sp<NI>::RM * TL, k2_min_blocks(NI, Sp<NI>::RM 
             bulk_g2s(&B[((c * 2) * NI + i) * TL], row0 + c * cstr + (size_t)i * plane,
                      TL * (unsigned)sizeof(float2), &bar);
         }
-        const bool got = mbar_wait(&bar, 0);
+        // (self-test: after the copies, wait briefly for the next phase, which nothing completes)
+        bool got = mbar_wait(&bar, 0);
+        if (got && a.wait_selftest) got = mbar_wait(&bar, 1, 1 << 10);
         if (!__syncthreads_and(got)) {   // the same decision for every thread
             if (threadIdx.x == 0 && a.err) atomicExch(a.err, 1);
             mbar_wait(&bar, 0);           // one more bounded wait for the copies in flight

@@ -219,6 +219,13 @@ int ddagpu_anthrax_rasterize(int device, int i_max, int j_max, int l_max, const 
 int ddagpu_set_fast_variant(ddagpu_ctx *ctx, int x_variant, int yz_variant);
 int ddagpu_get_fast_variant(ddagpu_ctx *ctx, int *x_variant, int *yz_variant);
 
+/* Self-test of the bounded device waits: on != 0 makes the bulk-copy x-pass variants
+ * (ddagpu_set_fast_variant x 3..5) wait briefly for a barrier phase that nothing completes,
+ * so that the wait runs out; the call then fails with DDAGPU_ECUDA ("a device wait ran
+ * out") and the context stays usable once the self-test is switched off.  Diagnostic
+ * only; no counterpart in the reference. */
+int ddagpu_selftest_wait_timeout(ddagpu_ctx *ctx, int on);
+
 /* Solves as CUDA graphs (no counterpart in the reference, whose loop is on the host,
  * dda_func.cpp:1301-1535).  On (the default): every chunk of a batched call
  * (ddagpu_orientation_solves, ddagpu_realization_solves, ddagpu_agglomerate_solves) is one

@@ -102,3 +102,25 @@ def test_graph_short_runs(D, oracle, solver, max_step):
     assert a["steps"] == max_step
     np.testing.assert_allclose(b["trace"], a["trace"], rtol=1e-9)
     assert abs(b["cext"] - a["cext"]) <= 1e-6 * abs(a["cext"])
+
+
+def test_bounded_wait_reports_and_recovers(D, oracle):
+    """The x pass's bounded wait on its bulk copies: a wait made to run out (self-test: a
+    barrier phase nothing completes) fails the call with DDAGPU_ECUDA instead of hanging,
+    and the context computes correctly again afterwards."""
+    occ, kd, alpha, ksc = problem(oracle)
+    rng = np.random.default_rng(2)
+    p = (rng.standard_normal(occ.shape + (3,)) + 1j * rng.standard_normal(occ.shape + (3,))).astype(np.complex64)
+    with D.Context(occ.shape, kd) as ctx:
+        ctx.set_fast_variant(3, 0)
+        ref = ctx.convolution(p)
+        ctx.selftest_wait_timeout(True)
+        with pytest.raises(D.DDAGPUError, match="wait ran out"):
+            ctx.convolution(p)
+        with pytest.raises(D.DDAGPUError, match="wait ran out"):
+            ctx.dda_fft(occ, alpha, [0, 1], kd, (0, 0, 1), (1, 0, 0), ksc, max_step=5)
+        ctx.selftest_wait_timeout(False)
+        again = ctx.convolution(p)
+        np.testing.assert_array_equal(again, ref)
+        r = ctx.dda_fft(occ, alpha, [0, 1], kd, (0, 0, 1), (1, 0, 0), ksc, max_step=5)
+        assert r["steps"] >= 1
