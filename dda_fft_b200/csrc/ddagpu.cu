@@ -126,6 +126,8 @@ struct ddagpu_ctx {
     int w_matvec0 = 0, w_matvec_it = 0;
     int *nact_dev = nullptr;         // [cap] active cells per right-hand side
     int *err_dev = nullptr;          // set by a kernel whose bounded wait gave up
+    void *worm_buf = nullptr;        // monomers of the realisation being rasterised
+    size_t worm_bytes = 0;
     int wait_selftest = 0;           // 1: the x pass's wait waits for a phase nothing completes
     long long post_key = 0;          // shape of the post-processing recorded with a solve
     long long g_per_iter = 0;    // kernels in one recorded iteration
@@ -877,7 +879,7 @@ int ddagpu_destroy(ddagpu_ctx *c)
                     c->w,    c->g,      c->h,      c->state,   c->active, c->trace, c->occ,
                     c->mv,   c->alpha,  c->kinc,   c->einc,    c->ksc,    c->esc_acc,
                     c->cc_acc, c->normals, c->mueller, c->esc, c->cabs,   c->cext,
-                    c->occ_b, c->ndip, c->step_dev, c->nact_dev, c->err_dev};
+                    c->occ_b, c->ndip, c->step_dev, c->nact_dev, c->err_dev, c->worm_buf};
     for (void *q : ptrs)
         if (q) cudaFree(q);
     if (c->st) cudaStreamDestroy(c->st);
@@ -1948,8 +1950,17 @@ int ddagpu_agglomerate_solves(ddagpu_ctx *c, const ddagpu_batch_cfg *cfg, int n_
         const int no = std::min(per, n_real - o0);
         for (int k = 0; k < no; k++) {
             const int r = o0 + k;
+            const size_t need = anthrax_scratch_bytes(counts[r]);
+            if (need > c->worm_bytes) {   // grow the context's monomer buffer (stream-ordered)
+                CK(cudaStreamSynchronize(c->st));
+                cudaFree(c->worm_buf);
+                c->worm_buf = nullptr;
+                c->worm_bytes = 0;
+                CK(cudaMalloc(&c->worm_buf, need));
+                c->worm_bytes = need;
+            }
             CK(anthrax_rasterize(monomers + 13 * first[(size_t)r], counts[r], c->ni, c->nj, c->nl,
-                                 c->occ_b + 2 * k * N, c->ndip + k, c->st));
+                                 c->occ_b + 2 * k * N, c->ndip + k, c->st, c->worm_buf, c->worm_bytes));
             CK(cudaMemcpyAsync(c->occ_b + (2 * k + 1) * N, c->occ_b + 2 * k * N, N,
                                cudaMemcpyDeviceToDevice, c->st));
             c->launches += 1;

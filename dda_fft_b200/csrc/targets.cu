@@ -509,8 +509,11 @@ int anthrax_place(unsigned long long *state, int ni, float radius, float length,
     return 0;
 }
 
+size_t anthrax_scratch_bytes(int count) { return (size_t)(count ? count : 1) * sizeof(DW); }
+
 cudaError_t anthrax_rasterize(const float *cyl13, int count, int ni, int nj, int nl,
-                              signed char *occ_dev, int *ndip_dev, cudaStream_t st)
+                              signed char *occ_dev, int *ndip_dev, cudaStream_t st, void *scratch,
+                              size_t scratch_bytes)
 {
     // iGenerateAnthrax rasterisation, particle.cpp:62-83: centre n/2 - 0.5, radius n/2
     std::vector<DW> h((size_t)count);
@@ -518,8 +521,10 @@ cudaError_t anthrax_rasterize(const float *cyl13, int count, int ni, int nj, int
         const float *c = cyl13 + 13 * (size_t)k;
         h[(size_t)k] = DW{c[0], c[1], c[2], c[3], c[4], c[5], c[6], c[7], c[8], c[9], c[10]};
     }
-    DW *d = nullptr;
-    cudaError_t e = cudaMallocAsync(&d, (count ? count : 1) * sizeof(DW), st);
+    // the caller's device scratch when it is large enough, else a stream-ordered allocation
+    const bool own = !scratch || scratch_bytes < anthrax_scratch_bytes(count);
+    DW *d = own ? nullptr : static_cast<DW *>(scratch);
+    cudaError_t e = own ? cudaMallocAsync(&d, anthrax_scratch_bytes(count), st) : cudaSuccess;
     if (e) return e;
     // pageable source: the copy has taken the host data when the call returns
     if (count) e = cudaMemcpyAsync(d, h.data(), count * sizeof(DW), cudaMemcpyHostToDevice, st);
@@ -534,7 +539,7 @@ cudaError_t anthrax_rasterize(const float *cyl13, int count, int ni, int nj, int
         rasterize<<<tiles, 256, 0, st>>>(d, count, ni, nj, nl, cx, cy, cz, R * R, occ_dev, ndip_dev);
         e = cudaGetLastError();
     }
-    cudaFreeAsync(d, st);
+    if (own) cudaFreeAsync(d, st);
     return e;
 }
 
