@@ -216,11 +216,15 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    # under torchrun the process group exists whatever the rank count (the reduction of the
+    # job's sums then goes through NCCL even on one rank)
+    distributed = "RANK" in os.environ and "WORLD_SIZE" in os.environ
     torch.cuda.set_device(local)
     dev = local
+    if distributed:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120),
+                                device_id=torch.device(f"cuda:{local}"))
 
     B, K, W = args.batch, args.steps, args.warmup
     occ = ellipsoid_occ()
@@ -241,12 +245,12 @@ def main():
     cfg_res = D.BatchConfig(occ=None, materials=[MAT], nplanes=1)
 
     def barrier():
-        if world > 1:
+        if distributed:
             dist.barrier()
         torch.cuda.synchronize(dev)
 
     def maxrank(v):
-        if world == 1:
+        if not distributed:
             return v
         t = torch.tensor([v], device=f"cuda:{dev}", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -392,7 +396,7 @@ def main():
         }
         print(json.dumps(line), flush=True)
     ctx.close()
-    if world > 1:
+    if distributed:
         dist.destroy_process_group()
 
 
