@@ -70,6 +70,7 @@ __global__ void __launch_bounds__(256) farfield_sum(PostArgs a, FFShape s)
     float2 *ey = ez + (size_t)nl * D;      // [nj][D]
     float2 *ex = ey + (size_t)nj * D;      // [FF_PLANES][D]
     float2 *P = ex + FF_PLANES * D;        // [rows][PSR], later the reduction buffer
+    __shared__ int span[2 * FF_CELLS / 8]; // first and last dipole column of each staged row
     const double cx = (a.ni - 1) * a.d0 / 2, cy = (nj - 1) * a.d0 / 2, cz = (nl - 1) * a.d0 / 2;
     const double *K = a.ksc + (size_t)rhs * a.ndir * 3;
     for (int e = threadIdx.x; e < (nl + nj + np) * D; e += blockDim.x) {
@@ -104,15 +105,29 @@ __global__ void __launch_bounds__(256) farfield_sum(PostArgs a, FFShape s)
     for (int j0 = 0; j0 < nj; j0 += s.rows) {
         const int rows = nj - j0 < s.rows ? nj - j0 : s.rows;
         __syncthreads();
+        for (int rr = threadIdx.x; rr < rows; rr += blockDim.x) {
+            span[2 * rr] = nl;
+            span[2 * rr + 1] = -1;
+        }
+        __syncthreads();
         for (int e = threadIdx.x; e < rows * nl; e += blockDim.x) {
             const int rr = e / nl, l = e - rr * nl;
             const size_t q = (size_t)j0 * nl + e;
             const bool act = a.mv[(int)occ[q]] != 0;
 #pragma unroll
             for (int c = 0; c < 3; c++) P[rr * PSR + 3 * l + c] = act ? p[c * N + q] : czero();
+            if (act) {
+                atomicMin(&span[2 * rr], l);
+                atomicMax(&span[2 * rr + 1], l);
+            }
         }
         __syncthreads();
         for (int rr = rg; rr < rows; rr += s.RG) {
+            // only the columns between the row's first and last dipole contribute (the
+            // others are zeros; skipping them changes no sum)
+            const int lb = span[2 * rr] > l0 ? span[2 * rr] : l0;
+            const int le = span[2 * rr + 1] + 1 < l0 + lcnt ? span[2 * rr + 1] + 1 : l0 + lcnt;
+            if (lb >= le) continue;
             float2 t[FF_DPT][3];
 #pragma unroll
             for (int u = 0; u < FF_DPT; u++)
@@ -120,7 +135,7 @@ __global__ void __launch_bounds__(256) farfield_sum(PostArgs a, FFShape s)
                 for (int c = 0; c < 3; c++) t[u][c] = czero();
             const float2 *row = P + rr * PSR;
 #pragma unroll 2
-            for (int l = l0; l < l0 + lcnt; l++) {
+            for (int l = lb; l < le; l++) {
                 const float4 e01 = *reinterpret_cast<const float4 *>(ez + (size_t)l * D + FF_DPT * dg);
                 const float4 e23 = *reinterpret_cast<const float4 *>(ez + (size_t)l * D + FF_DPT * dg + 2);
                 const float2 ev[FF_DPT] = {make_float2(e01.x, e01.y), make_float2(e01.z, e01.w),
