@@ -151,3 +151,26 @@ def test_agglomerate_sample_loop_vs_reference(D, oracle, fx):
     assert (np.abs(M[sig] - M64[sig]) / np.abs(M64[sig])).max() < 1e-3
     sig = np.abs(ref[2:]) > 1e-3 * np.abs(ref[2:]).max()
     assert (np.abs(M[sig] - ref[2:][sig]) / np.abs(ref[2:][sig])).max() < 3e-3
+
+
+@pytest.mark.parametrize("grid,solver", [((32, 16, 32), 2), ((8, 16, 4), 0), ((16, 32, 16), 1)])
+def test_rectangular_batches_vs_oracle(D, oracle, grid, solver):
+    """Batched Monte-Carlo orientations on rectangular lattices (specialised passes for
+    32 x 16 x 32 and 16 x 32 x 16, generic passes for 8 x 16 x 4) with BiCGStab, CG and AA*
+    against the FP64 sample loop, summed over 3 orientations; two planes."""
+    occ, _ = oracle.gen_ellipsoid(*grid, 0.5 if grid[1] < grid[0] else 1.0,
+                                  1.0 if grid[2] >= grid[0] else 0.5)
+    x = 0.125 * grid[0]
+    cfg = D.BatchConfig(occ=occ, materials=[(1.5, 0.02)], solver=solver, err_max=1e-4,
+                        max_step=200, nplanes=2)
+    with D.Context(grid, 2 * x / grid[0], max_rhs=4) as ctx:
+        r = ctx.orientation_solves(cfg, D.mc_rotations(11, 3))
+    o = orientation_solves(oracle, grid, x, [(1.5, 0.02)], 3,
+                           b_a=0.5 if grid[1] < grid[0] else 1.0,
+                           c_a=1.0 if grid[2] >= grid[0] else 0.5, target=2, solver=solver,
+                           err_max=1e-4, max_step=200, nplanes=2, orientation=1, seed=11, occ=occ)
+    for q in ("cabs", "cext"):
+        assert abs(r[q].sum() - o[q]) <= 1e-4 * abs(o[q]), (q, r[q].sum(), o[q])
+    M, Mo = r["mueller"].sum(axis=0).ravel(), o["mueller"].ravel()
+    sig = np.abs(Mo) > 1e-3 * np.abs(Mo).max()
+    assert (np.abs(M[sig] - Mo[sig]) / np.abs(Mo[sig])).max() < 1e-3
