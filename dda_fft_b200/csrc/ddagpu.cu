@@ -99,6 +99,9 @@ struct ddagpu_ctx {
     float2 *b32 = nullptr, *rb = nullptr;   // refinement: outer and inner right-hand sides
     double2 *x64 = nullptr;                 // refinement: FP64 solution
     bool occ_valid = false;      // occupancy of the last batched call is resident
+    std::vector<signed char> occ_host;   // host copy of the occupancy in c->occ (if cached)
+    std::vector<int> mv_host;            // and the material flags it was counted with
+    int occ_host_nact = 0;
     signed char *occ_b = nullptr;   // [cap][N] per-right-hand-side occupancy (realisations)
     int *ndip = nullptr;            // [cap] dipoles of each rasterised realisation
     size_t occ_stride = 0;          // N while occ_b is in use, 0 otherwise
@@ -1055,14 +1058,28 @@ int ddagpu_convolution(ddagpu_ctx *c, const float *p, float *out, int conj)
 
 namespace {
 
-// Upload the per-solve material tables and occupancy.
-int upload_materials(ddagpu_ctx *c, const int *mv, int nmat1, const signed char *occ)
+// Upload the per-solve material tables and occupancy; *nact (may be null) receives the
+// active-cell count.  The reference calls DDA_FFT for both polarisations of a sample with
+// the same occupancy, so an occupancy and material flags equal to the last ones uploaded
+// (compared byte for byte) are neither checked, counted nor copied again.
+int upload_materials(ddagpu_ctx *c, const int *mv, int nmat1, const signed char *occ,
+                     int *nact = nullptr)
 {
     if (nmat1 < 1 || nmat1 > c->nmat_cap) return fail(DDAGPU_EINVAL, "n_mat outside 0..254");
-    RET(check_occ(occ, c->N, nmat1));
     c->occ_valid = false;
     CK(cudaMemcpyAsync(c->mv, mv, nmat1 * sizeof(int), cudaMemcpyHostToDevice, c->st));
-    CK(cudaMemcpyAsync(c->occ, occ, c->N, cudaMemcpyHostToDevice, c->st));
+    const bool same = c->occ_host.size() == c->N && c->mv_host.size() == (size_t)nmat1 &&
+                      std::memcmp(c->mv_host.data(), mv, nmat1 * sizeof(int)) == 0 &&
+                      std::memcmp(c->occ_host.data(), occ, c->N) == 0;
+    if (!same) {
+        c->occ_host.clear();
+        RET(check_occ(occ, c->N, nmat1));
+        CK(cudaMemcpyAsync(c->occ, occ, c->N, cudaMemcpyHostToDevice, c->st));
+        c->occ_host_nact = count_active(occ, c->N, mv, nmat1);
+        c->occ_host.assign(occ, occ + c->N);
+        c->mv_host.assign(mv, mv + nmat1);
+    }
+    if (nact) *nact = c->occ_host_nact;
     return DDAGPU_OK;
 }
 
@@ -1269,7 +1286,8 @@ int ddagpu_dda_fft(ddagpu_ctx *c, int iNoIllumination, int solver, float rTau, i
     std::lock_guard<std::mutex> lk(c->mu);
     DevGuard dg(c->dev);
     const int nmat1 = n_mat + 1, ndir = iNoScPl * iNoA;
-    RET(upload_materials(c, iListMV, nmat1, cAlpha));
+    int nact = 0;
+    RET(upload_materials(c, iListMV, nmat1, cAlpha, &nact));
     RET(ensure_post(c, std::max(ndir, 1), std::max(iNoScPl, 1), std::max(iNoA, 1)));
     std::vector<float2> al((size_t)nmat1);
     for (int m = 0; m < nmat1; m++) al[(size_t)m] = make_float2(cListMaterials[2 * m], cListMaterials[2 * m + 1]);
@@ -1282,7 +1300,7 @@ int ddagpu_dda_fft(ddagpu_ctx *c, int iNoIllumination, int solver, float rTau, i
     CK(cudaMemcpyAsync(c->kinc, kd3, sizeof kd3, cudaMemcpyHostToDevice, c->st));
     CK(cudaMemcpyAsync(c->einc, ed6, sizeof ed6, cudaMemcpyHostToDevice, c->st));
     if (ndir) CK(cudaMemcpyAsync(c->ksc, kd.data(), kd.size() * sizeof(double), cudaMemcpyHostToDevice, c->st));
-    const int nact = count_active(cAlpha, c->N, iListMV, nmat1);
+    // nact: counted by upload_materials
     if (nact == 0) return fail(DDAGPU_EINVAL, "no active dipoles");
     SolveResult res;
     RET(run_solver(c, 1, solver, rTau, Max_Step, Error_max, nmat1, d0, nact, res, trace != nullptr));
@@ -1405,11 +1423,12 @@ int ddagpu_solve_linear(ddagpu_ctx *c, int solver, float rTau, const float *cLis
         CK(dalloc(&c->rb, n3));
         CK(dalloc(&c->x64, n3));
     }
-    RET(upload_materials(c, iListMV, nmat1, cAlpha));
+    int nact = 0;
+    RET(upload_materials(c, iListMV, nmat1, cAlpha, &nact));
     std::vector<float2> al((size_t)nmat1);
     for (int m = 0; m < nmat1; m++) al[(size_t)m] = make_float2(cListMaterials[2 * m], cListMaterials[2 * m + 1]);
     CK(cudaMemcpyAsync(c->alpha, al.data(), nmat1 * sizeof(float2), cudaMemcpyHostToDevice, c->st));
-    const int nact = count_active(cAlpha, c->N, iListMV, nmat1);
+    // nact: counted by upload_materials
     if (nact == 0) return fail(DDAGPU_EINVAL, "no active dipoles");
     std::vector<float2> soa(n3);
     aos_to_soa(rhs, soa.data(), c->N);
@@ -1470,7 +1489,8 @@ int ddagpu_dda_fft_refined(ddagpu_ctx *c, int solver, float rTau, const float *c
         CK(dalloc(&c->rb, n3));
         CK(dalloc(&c->x64, n3));
     }
-    RET(upload_materials(c, iListMV, nmat1, cAlpha));
+    int nact = 0;
+    RET(upload_materials(c, iListMV, nmat1, cAlpha, &nact));
     RET(ensure_post(c, std::max(ndir, 1), std::max(iNoScPl, 1), std::max(iNoA, 1)));
     std::vector<float2> al((size_t)nmat1);
     for (int m = 0; m < nmat1; m++) al[(size_t)m] = make_float2(cListMaterials[2 * m], cListMaterials[2 * m + 1]);
@@ -1482,7 +1502,7 @@ int ddagpu_dda_fft_refined(ddagpu_ctx *c, int solver, float rTau, const float *c
     CK(cudaMemcpyAsync(c->kinc, kd3, sizeof kd3, cudaMemcpyHostToDevice, c->st));
     CK(cudaMemcpyAsync(c->einc, ed6, sizeof ed6, cudaMemcpyHostToDevice, c->st));
     if (ndir) CK(cudaMemcpyAsync(c->ksc, kdir.data(), kdir.size() * sizeof(double), cudaMemcpyHostToDevice, c->st));
-    const int nact = count_active(cAlpha, c->N, iListMV, nmat1);
+    // nact: counted by upload_materials
     if (nact == 0) return fail(DDAGPU_EINVAL, "no active dipoles");
     // outer right-hand side b = p_inc (FirstApproximation), x = b
     {
@@ -1527,7 +1547,8 @@ int ddagpu_farfield(ddagpu_ctx *c, const int *iListMV, int n_mat, const signed c
     std::lock_guard<std::mutex> lk(c->mu);
     DevGuard dg(c->dev);
     const int nmat1 = n_mat + 1;
-    RET(upload_materials(c, iListMV, nmat1, cAlpha));
+    int nact = 0;
+    RET(upload_materials(c, iListMV, nmat1, cAlpha, &nact));
     RET(ensure_post(c, std::max(ndir, 1), 1, 1));
     const size_t N = c->N;
     std::vector<float2> soa(3 * N);
@@ -1857,8 +1878,7 @@ int ddagpu_orientation_solves(ddagpu_ctx *c, const ddagpu_batch_cfg *cfg, int n_
     // occupancy shared by every orientation
     int nact = 0;
     if (cfg->occ) {
-        RET(upload_materials(c, g.mv.data(), g.nmat1, cfg->occ));
-        nact = count_active(cfg->occ, c->N, g.mv.data(), g.nmat1);
+        RET(upload_materials(c, g.mv.data(), g.nmat1, cfg->occ, &nact));
         c->occ_valid = true;
         c->occ_nmat1 = g.nmat1;
         c->occ_nact = nact;

@@ -327,3 +327,35 @@ def test_workspace_mismatch_and_bad_material(D):
                               1e-3, 0.5, P(k), P(e), 0, 1, 1, P(ksc), P(esc), C.byref(ca),
                               C.byref(ce), None, None)
         assert rc == 0 and np.isfinite(ce.value) and ce.value != 0.0
+
+
+def test_occupancy_changes_between_calls(D, oracle):
+    """A context keeps the last occupancy it uploaded and skips the upload when the next
+    call's occupancy is the same; a changed occupancy (or material flags), even in the same
+    host buffer, must still be used."""
+    n, kd = 16, 0.4
+    a, _ = oracle.gen_ellipsoid(n, n, n, 1.0, 1.0)
+    b, _ = oracle.gen_ellipsoid(n, n, n, 0.6, 0.5)
+    alpha = np.array([0, 0.02 + 0.001j], np.complex64)
+    ksc = np.array([[[0.0, 0.0, 1.0], [1.0, 0.0, 0.0]]])
+
+    def run(ctx, occ, mv=(0, 1)):
+        return ctx.dda_fft(occ, alpha, list(mv), kd, (0, 0, 1), (1, 0, 0), ksc, max_step=30,
+                           err_max=1e-6)["cext"]
+
+    with D.Context(n, kd) as fresh:
+        ref_a, ref_b = run(fresh, a), None
+    with D.Context(n, kd) as fresh:
+        ref_b = run(fresh, b)
+    with D.Context(n, kd) as ctx:
+        buf = a.copy()
+        got = [run(ctx, buf), run(ctx, buf)]
+        buf[...] = b                       # same host buffer, new contents
+        got.append(run(ctx, buf))
+        buf[...] = a
+        got.append(run(ctx, buf))
+        with pytest.raises(D.DDAGPUError):  # all materials inactive: no dipoles
+            run(ctx, buf, mv=(0, 0))
+        got.append(run(ctx, buf))
+    for g, r in zip(got, (ref_a, ref_a, ref_b, ref_a, ref_a)):
+        assert abs(g - r) <= 1e-6 * abs(r)
