@@ -62,23 +62,34 @@ class ClockSampler:
         self.lines: list[str] = []
 
     def start(self):
+        """Start sampling every 50 ms and return once the first sample has arrived (so that
+        sampling is running when the timed region begins); samples from then on count."""
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.th = threading.Thread(target=self._read, daemon=True)
             self.th.start()
+            t0 = time.time()
+            while not self.lines and time.time() - t0 < 5.0 and self.proc.poll() is None:
+                time.sleep(0.01)
         except Exception:
             self.proc = None
+        self.first = len(self.lines)
 
     def _read(self):
         for ln in self.proc.stdout:
             self.lines.append(ln.strip())
 
     def stop(self):
+        """Stop sampling; a timed region shorter than the sampling period still gets the
+        sample taken right after it (waited for, up to 0.5 s)."""
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        t0 = time.time()
+        while len(self.lines) <= self.first and time.time() - t0 < 0.5 and self.proc.poll() is None:
+            time.sleep(0.005)
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
@@ -86,7 +97,7 @@ class ClockSampler:
             self.proc.kill()
         sm, smax, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        for ln in self.lines[self.first:]:
             f = [x.strip() for x in ln.split(",")]
             if len(f) < 9:
                 continue
