@@ -1083,9 +1083,11 @@ int upload_materials(ddagpu_ctx *c, const int *mv, int nmat1, const signed char 
     return DDAGPU_OK;
 }
 
-int run_post(ddagpu_ctx *c, int nrhs, int nmat1, double d0, int ndir)
+// pairs: right-hand sides 2k and 2k+1 are the two polarisations of one orientation
+int run_post(ddagpu_ctx *c, int nrhs, int nmat1, double d0, int ndir, bool pairs = false)
 {
     PostArgs pa{};
+    pa.pairs = pairs ? 1 : 0;
     pa.N = c->N;
     pa.nrhs = nrhs;
     pa.ni = c->ni;
@@ -1105,7 +1107,7 @@ int run_post(ddagpu_ctx *c, int nrhs, int nmat1, double d0, int ndir)
     pa.esc_acc = c->esc_acc;
     pa.cc_acc = c->cc_acc;
     CK(launch_post(pa, c->esc, c->cabs, c->cext, c->st));
-    c->launches += ndir > 0 ? 3 : 2;
+    c->launches += 2;
     return DDAGPU_OK;
 }
 
@@ -1233,7 +1235,7 @@ int batch_chunk(ddagpu_ctx *c, const ddagpu_batch_cfg *cfg, const BatchGeom &g, 
     // far field, cross sections and the plane-averaged Mueller matrices, after the solve
     // (recorded with it when the solve is one graph launch)
     const std::function<int()> post = [&]() -> int {
-        RET(run_post(c, nr, nmat1, d0, ndir));
+        RET(run_post(c, nr, nmat1, d0, ndir, true));
         MuellerArgs m{no, nP, nA, ndir, c->kinc, c->einc, c->ksc, c->normals, c->esc, c->mueller};
         CK(launch_mueller(m, c->st));
         c->launches += 1;

@@ -18,162 +18,427 @@ namespace ddagpu {
 
 namespace {
 
-// Far-field tiling: a CTA takes FF_PLANES lattice planes i of one right-hand side and up
-// to FF_DMAX directions (the phase tables, one per axis, are built once for them); a
-// thread accumulates FF_DPT directions x 3 components for the rows rg, rg + RG, ... of
-// each staged group and the columns of its column group lg, so every staged dipole value
-// and phase factor it loads from shared memory feeds 4 to 12 complex multiply-adds.
+// Far-field tiling.  A CTA takes FF_PLANES lattice planes i of one right-hand side and up to
+// FF_DMAX directions, whose phase tables (one per axis) it builds once.  Thread (dg, w)
+// accumulates DPT directions x 3 components; the RW threads w of one direction group are
+// workers that split the plane's dipoles evenly:
+//   1. the plane's occupancy is staged in shared memory and each row's span -- first to
+//      last active column -- found with warp ballots; a prefix sum over the rows gives
+//      every span cell a position in one list (inactive cells inside a span stay in it,
+//      with zero dipoles);
+//   2. the list is taken in chunks of ff_cap cells: the dipoles of a chunk are copied into
+//      shared memory (cp.async) with their row, column and material packed in one word,
+//      and worker w sums positions [w len / RW, (w + 1) len / RW) of the chunk:
+//      t += exp(i kz z) P along a row, and at each row end acc += exp(i (kx x + ky y)) t.
+// So every lane does the same number of cells whatever the target's shape.  With NR = 2 a
+// CTA takes the two right-hand sides of one orientation (both incident polarisations: the
+// same scattering directions and occupancy), so each phase factor it loads feeds both and
+// the occupancy, spans and list are built once for the pair; a thread then takes DPT = 2
+// directions, which keeps its accumulators in registers.  With CC set, the CTAs of the
+// first direction chunk also sum Cext and Cabs over the staged cells, so the dipoles are
+// read from HBM once for both.
 constexpr int FF_DMAX = 32;
-constexpr int FF_DPT = 4;
-constexpr int FF_CELLS = 2048;   // lattice cells staged per round
+constexpr int FF_DQ = 4;         // directions per CTA are padded to a multiple of this
 constexpr int FF_PLANES = 8;     // lattice planes per CTA
 
+// list cells per chunk
+__host__ __device__ constexpr int ff_cap(int nr) { return nr == 2 ? 512 : 1024; }
+
 struct FFShape {
-    int D, DG, rows, RG, LG, threads;
+    int D, dpt, DG, RW, threads;
 };
 
-FFShape ff_shape(int ndir, int nj, int nl)
+FFShape ff_shape(int ndir, int dpt)
 {
     FFShape s;
-    s.D = ndir >= FF_DMAX ? FF_DMAX : ((ndir + FF_DPT - 1) / FF_DPT) * FF_DPT;
-    if (s.D < FF_DPT) s.D = FF_DPT;
-    s.DG = s.D / FF_DPT;
-    s.rows = FF_CELLS / nl < nj ? FF_CELLS / nl : nj;
-    if (s.rows < 1) s.rows = 1;
-    s.RG = 256 / s.DG < s.rows ? 256 / s.DG : s.rows;
-    // column groups: a power of two (it divides nl), at least 8 columns each
-    s.LG = 1;
-    while (2 * s.LG * s.DG * s.RG <= 256 && 2 * s.LG * 8 <= nl) s.LG *= 2;
-    s.threads = s.DG * s.RG * s.LG;
+    s.D = ndir >= FF_DMAX ? FF_DMAX : ((ndir + FF_DQ - 1) / FF_DQ) * FF_DQ;
+    if (s.D < FF_DQ) s.D = FF_DQ;
+    s.dpt = dpt;
+    s.DG = s.D / dpt;
+    // the block is a whole number of warps, at most 256 threads
+    if (s.DG <= 8) {
+        const int k = 8 / s.DG;
+        s.RW = 32 * (k > 1 ? k : 1);
+    } else {
+        s.RW = 16;   // DG even (D is a multiple of 4 and dpt 2), so 16 DG is a whole number of warps
+    }
+    s.threads = s.DG * s.RW;
     return s;
 }
 
-size_t ff_smem(const FFShape &s, int nj, int nl)
+template <int DPT>
+DDA_DEV void ld_dirs(const float2 *p, float2 (&v)[DPT])
 {
-    const size_t tables = (size_t)(nl + nj + FF_PLANES) * s.D;
-    const size_t staged = (size_t)s.rows * (3 * nl + 1);
-    const size_t red = (size_t)s.threads * FF_DPT * 3;
-    return (tables + (staged > red ? staged : red)) * sizeof(float2);
+#pragma unroll
+    for (int k = 0; k < DPT; k += 2) {
+        const float4 q = *reinterpret_cast<const float4 *>(p + k);
+        v[k] = make_float2(q.x, q.y);
+        v[k + 1] = make_float2(q.z, q.w);
+    }
 }
 
-// grid (direction chunks of D, plane groups of FF_PLANES, nrhs)
+// Shared-memory layout (byte offsets, 16-byte aligned blocks).
+struct FFLayout {
+    size_t tab, eyx, P, cc, idx, ints, occ, total;
+};
+
+__host__ __device__ inline size_t ff_al16(size_t b) { return (b + 15) & ~(size_t)15; }
+
+__host__ __device__ inline FFLayout ff_layout(FFShape s, int nj, int nl, int nmat1, bool cc, int nr)
+{
+    const size_t f2 = sizeof(float2);
+    size_t pz = (size_t)ff_cap(nr) * 3 * nr;
+    const size_t red = (size_t)s.threads * s.dpt * 3 * nr;   // the reduction reuses the dipole buffer
+    if (red > pz) pz = red;
+    FFLayout L;
+    L.tab = 0;                                                          // ez [nl][D], ey [nj][D], ex [8][D]
+    L.eyx = ff_al16(L.tab + (size_t)(nl + nj + FF_PLANES) * s.D * f2);  // [nj][D] row factors of a plane
+    L.P = ff_al16(L.eyx + (size_t)nj * s.D * f2);                       // [cap][nr][3]
+    L.cc = ff_al16(L.P + pz * f2);                                      // CC: cy [nj], cz [nl], cx [8], weights
+    L.idx = ff_al16(L.cc + (cc ? (size_t)(nj + nl + FF_PLANES) * f2 + (size_t)nr * nmat1 * sizeof(double) : 0));
+    L.ints = ff_al16(L.idx + (size_t)ff_cap(nr) * sizeof(unsigned));    // sb, len [nj], off [nj+1], mv, modes, misc
+    L.occ = ff_al16(L.ints + (size_t)(3 * nj + 1 + (1 + nr) * nmat1 + 4) * sizeof(int));
+    L.total = ff_al16(L.occ + (size_t)nj * nl);
+    return L;
+}
+
+DDA_DEV void cp_async8(void *dst, const void *src)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((unsigned)__cvta_generic_to_shared(dst)),
+                 "l"(src)
+                 : "memory");
+}
+DDA_DEV void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+DDA_DEV void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+// grid (direction chunks of D, plane groups of FF_PLANES, nrhs / NR); the lattice has
+// nj, nl < 4096
+template <bool CC, int NR, int DPT>
 __global__ void __launch_bounds__(256) farfield_sum(PostArgs a, FFShape s)
 {
-    extern __shared__ float2 sm[];
-    const int nj = a.nj, nl = a.nl, D = s.D;
-    const int dbase = blockIdx.x * D, i0 = blockIdx.y * FF_PLANES, rhs = blockIdx.z;
+    constexpr int CAP = ff_cap(NR);
+    extern __shared__ __align__(16) unsigned char smraw[];
+    const int nj = a.nj, nl = a.nl, D = s.D, T = blockDim.x, nmat1 = a.nmat1;
+    const int dbase = blockIdx.x * D, i0 = blockIdx.y * FF_PLANES, rhs = NR * blockIdx.z;
     const int np = a.ni - i0 < FF_PLANES ? a.ni - i0 : FF_PLANES;
-    const int dg = threadIdx.x % s.DG, rest = threadIdx.x / s.DG;
-    const int lg = rest % s.LG, rg = rest / s.LG;
-    const int PSR = 3 * nl + 1;            // staged row stride (odd: rows fall on other banks)
-    float2 *ez = sm;                       // [nl][D]
-    float2 *ey = ez + (size_t)nl * D;      // [nj][D]
-    float2 *ex = ey + (size_t)nj * D;      // [FF_PLANES][D]
-    float2 *P = ex + FF_PLANES * D;        // [rows][PSR], later the reduction buffer
-    __shared__ int span[2 * FF_CELLS / 8]; // first and last dipole column of each staged row
-    const double cx = (a.ni - 1) * a.d0 / 2, cy = (nj - 1) * a.d0 / 2, cz = (nl - 1) * a.d0 / 2;
+    const bool cc = CC && blockIdx.x == 0;
+    const int dg = threadIdx.x % s.DG, w = threadIdx.x / s.DG;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = T >> 5;
+    const FFLayout L = ff_layout(s, nj, nl, nmat1, CC, NR);
+    float2 *ez = reinterpret_cast<float2 *>(smraw + L.tab);   // [nl][D]
+    float2 *ey = ez + (size_t)nl * D;                          // [nj][D]
+    float2 *ex = ey + (size_t)nj * D;                          // [FF_PLANES][D]
+    float2 *eyx = reinterpret_cast<float2 *>(smraw + L.eyx);   // [nj][D]
+    float2 *P = reinterpret_cast<float2 *>(smraw + L.P);       // [CAP][NR][3], later the reduction
+    float2 *cy = reinterpret_cast<float2 *>(smraw + L.cc);     // CC: [nj], [nl], [FF_PLANES]
+    float2 *cz = cy + nj, *cx = cz + nl;
+    double *cwt = reinterpret_cast<double *>(cx + FF_PLANES);  // CC: [NR][nmat1]
+    unsigned *idx = reinterpret_cast<unsigned *>(smraw + L.idx);   // [CAP] l | row << 12 | m << 24
+    int *sb = reinterpret_cast<int *>(smraw + L.ints);         // [nj] first column of each row's span
+    int *ln = sb + nj;                                         // [nj] span length (0: no dipole)
+    int *off = ln + nj;                                        // [nj + 1] list position of each span
+    int *mvs = off + nj + 1;                                   // [nmat1]
+    int *ccm = mvs + nmat1;                                    // [NR][nmat1]
+    int *misc = ccm + NR * nmat1;                              // [0]: some material in mode 2
+    signed char *occs = reinterpret_cast<signed char *>(smraw + L.occ);   // [nj][nl] one plane
+
+    const double cxf = (a.ni - 1) * a.d0 / 2, cyf = (nj - 1) * a.d0 / 2, czf = (nl - 1) * a.d0 / 2;
     const double *K = a.ksc + (size_t)rhs * a.ndir * 3;
-    for (int e = threadIdx.x; e < (nl + nj + np) * D; e += blockDim.x) {
+    for (int e = threadIdx.x; e < (nl + nj + np) * D; e += T) {
         const int dl = e % D, pos = e / D, dd = dbase + dl;
         float2 val = czero();
         if (dd < a.ndir) {
             double ph;
-            if (pos < nl) ph = K[3 * dd + 2] * (pos * a.d0 - cz);
-            else if (pos < nl + nj) ph = K[3 * dd + 1] * ((pos - nl) * a.d0 - cy);
-            else ph = K[3 * dd + 0] * ((i0 + pos - nl - nj) * a.d0 - cx);
+            if (pos < nl) ph = K[3 * dd + 2] * (pos * a.d0 - czf);
+            else if (pos < nl + nj) ph = K[3 * dd + 1] * ((pos - nl) * a.d0 - cyf);
+            else ph = K[3 * dd + 0] * ((i0 + pos - nl - nj) * a.d0 - cxf);
             val = expi_reduced(ph);
         }
         ez[e] = val;   // ez, ey, ex are consecutive [pos][D] blocks
     }
-    __syncthreads();   // the tables are read below before the first staging barrier
-    const size_t N = a.N;
-    const int lcnt = nl / s.LG, l0 = lg * lcnt;
-    float2 acc[FF_DPT][3];
+    if (threadIdx.x == 0) misc[0] = 0;
+    __syncthreads();
+    for (int e = threadIdx.x; e < nmat1; e += T) {
+        const int mv = a.mv[e];
+        mvs[e] = mv;
+        if (CC) {
+            // cross-section mode of a material: 0 no polarisability (skipped), 1 dipoles
+            // staged, 2 a polarisability but switched off in the activity list (its dipoles
+            // are read from global memory); weight Im(1 / conj(alpha))
 #pragma unroll
-    for (int u = 0; u < FF_DPT; u++)
-#pragma unroll
-        for (int c = 0; c < 3; c++) acc[u][c] = czero();
-#pragma unroll 1
-    for (int ip = 0; ip < np; ip++) {
-    const int i = i0 + ip;
-    const float2 *p = a.p + (size_t)rhs * 3 * N + (size_t)i * nj * nl;
-    const signed char *occ = a.occ + (size_t)rhs * a.occ_stride + (size_t)i * nj * nl;
-    // x phase of this plane folded into the row factors
-    float2 exv[FF_DPT];
-#pragma unroll
-    for (int u = 0; u < FF_DPT; u++) exv[u] = ex[ip * D + FF_DPT * dg + u];
-    for (int j0 = 0; j0 < nj; j0 += s.rows) {
-        const int rows = nj - j0 < s.rows ? nj - j0 : s.rows;
-        __syncthreads();
-        for (int rr = threadIdx.x; rr < rows; rr += blockDim.x) {
-            span[2 * rr] = nl;
-            span[2 * rr + 1] = -1;
-        }
-        __syncthreads();
-        for (int e = threadIdx.x; e < rows * nl; e += blockDim.x) {
-            const int rr = e / nl, l = e - rr * nl;
-            const size_t q = (size_t)j0 * nl + e;
-            const bool act = a.mv[(int)occ[q]] != 0;
-#pragma unroll
-            for (int c = 0; c < 3; c++) P[rr * PSR + 3 * l + c] = act ? p[c * N + q] : czero();
-            if (act) {
-                atomicMin(&span[2 * rr], l);
-                atomicMax(&span[2 * rr + 1], l);
-            }
-        }
-        __syncthreads();
-        for (int rr = rg; rr < rows; rr += s.RG) {
-            // only the columns between the row's first and last dipole contribute (the
-            // others are zeros; skipping them changes no sum)
-            const int lb = span[2 * rr] > l0 ? span[2 * rr] : l0;
-            const int le = span[2 * rr + 1] + 1 < l0 + lcnt ? span[2 * rr + 1] + 1 : l0 + lcnt;
-            if (lb >= le) continue;
-            float2 t[FF_DPT][3];
-#pragma unroll
-            for (int u = 0; u < FF_DPT; u++)
-#pragma unroll
-                for (int c = 0; c < 3; c++) t[u][c] = czero();
-            const float2 *row = P + rr * PSR;
-#pragma unroll 2
-            for (int l = lb; l < le; l++) {
-                const float4 e01 = *reinterpret_cast<const float4 *>(ez + (size_t)l * D + FF_DPT * dg);
-                const float4 e23 = *reinterpret_cast<const float4 *>(ez + (size_t)l * D + FF_DPT * dg + 2);
-                const float2 ev[FF_DPT] = {make_float2(e01.x, e01.y), make_float2(e01.z, e01.w),
-                                           make_float2(e23.x, e23.y), make_float2(e23.z, e23.w)};
-                const float2 pv[3] = {row[3 * l], row[3 * l + 1], row[3 * l + 2]};
-#pragma unroll
-                for (int u = 0; u < FF_DPT; u++)
-#pragma unroll
-                    for (int c = 0; c < 3; c++) t[u][c] = cfma(ev[u], pv[c], t[u][c]);
-            }
-            const float2 *eyr = ey + (size_t)(j0 + rr) * D + FF_DPT * dg;
-#pragma unroll
-            for (int u = 0; u < FF_DPT; u++) {
-                const float2 f = cmul(eyr[u], exv[u]);
-#pragma unroll
-                for (int c = 0; c < 3; c++) acc[u][c] = cfma(f, t[u][c], acc[u][c]);
+            for (int r = 0; r < NR; r++) {
+                const float2 al = a.alpha[(size_t)(rhs + r) * nmat1 + e];
+                const bool nz = !(al.x == 0.f && al.y == 0.f);
+                const int mode = nz ? (mv ? 1 : 2) : 0;
+                ccm[r * nmat1 + e] = mode;
+                if (mode == 2) misc[0] = 1;
+                const double ar = al.x, ai = al.y;
+                cwt[r * nmat1 + e] = nz ? ai / (ar * ar + ai * ai) : 0.0;
             }
         }
     }
-    }   // planes of this CTA
-    // the sum over row and column groups in FP64
-    __syncthreads();
-    float2 *red = P;   // [threads][FF_DPT][3]
+    // the incident direction is the pair's (both polarisations of one orientation)
+    const double *ki = a.kinc + 3 * rhs;
+    if (cc) {
+        // CabsCext's phase -k.(r - c') with the centre c' = n d0 / 2 (dda_func.cpp:1685)
+        const double ccx = a.ni * a.d0 / 2, ccy = nj * a.d0 / 2, ccz = nl * a.d0 / 2;
+        for (int e = threadIdx.x; e < nj + nl + np; e += T) {
+            const double ph = e < nj ? -ki[1] * (e * a.d0 - ccy)
+                            : e < nj + nl ? -ki[2] * ((e - nj) * a.d0 - ccz)
+                                          : -ki[0] * ((i0 + e - nj - nl) * a.d0 - ccx);
+            cy[e] = expi_reduced(ph);   // cy, cz, cx are consecutive
+        }
+    }
+    double Ec[NR][6];   // CC: conj(E_inc) of each right-hand side
 #pragma unroll
-    for (int u = 0; u < FF_DPT; u++)
+    for (int r = 0; r < NR; r++)
 #pragma unroll
-        for (int c = 0; c < 3; c++) red[((size_t)threadIdx.x * FF_DPT + u) * 3 + c] = acc[u][c];
+        for (int k = 0; k < 6; k++) {
+            const double e = CC ? a.einc[6 * (rhs + r) + k] : 0.0;
+            Ec[r][k] = (k & 1) ? -e : e;
+        }
     __syncthreads();
-    for (int o = threadIdx.x; o < D * 6; o += blockDim.x) {
-        const int dl = o / 6, k = o % 6, u = dl % FF_DPT, g = dl / FF_DPT, c = k >> 1;
+    const bool slow_cc = cc && misc[0] != 0;
+
+    const size_t N = a.N, plane = (size_t)nj * nl;
+    const float2 *pr = a.p + (size_t)rhs * 3 * N;   // the NR right-hand sides follow each other
+    const signed char *occr = a.occ + (size_t)rhs * a.occ_stride;
+    const bool vec_occ = plane % 16 == 0 && (reinterpret_cast<size_t>(occr) & 15) == 0;
+    float2 acc[NR][DPT][3];
+#pragma unroll
+    for (int r = 0; r < NR; r++)
+#pragma unroll
+        for (int u = 0; u < DPT; u++)
+#pragma unroll
+            for (int c = 0; c < 3; c++) acc[r][u][c] = czero();
+    double v[NR][2];   // CC: Cext and Cabs sums
+#pragma unroll
+    for (int r = 0; r < NR; r++) v[r][0] = v[r][1] = 0.0;
+
+#pragma unroll 1
+    for (int ip = 0; ip < np; ip++) {
+        const size_t q0 = (size_t)(i0 + ip) * plane;
+        // ---- occupancy of the plane into shared memory
+        if (vec_occ) {
+            const int4 *src = reinterpret_cast<const int4 *>(occr + q0);
+            int4 *dst = reinterpret_cast<int4 *>(occs);
+            for (int e = threadIdx.x; e < (int)(plane / 16); e += T) dst[e] = src[e];
+        } else {
+            for (int e = threadIdx.x; e < (int)plane; e += T) occs[e] = occr[q0 + e];
+        }
+        // row factors exp(i (kx x + ky y)) of this plane
+        for (int e = threadIdx.x; e < nj * D; e += T) eyx[e] = cmul(ey[e], ex[ip * D + e % D]);
+        __syncthreads();
+        // ---- spans: first and last active column of every row (warp per row)
+        for (int r = warp; r < nj; r += nwarps) {
+            int first = nl, last = -1;
+            for (int c0 = 0; c0 < nl; c0 += 32) {
+                const int l = c0 + lane;
+                bool act = false;
+                if (l < nl) {
+                    const int m = occs[r * nl + l];
+                    // nmat1 == 0: the activity list's length is not known (allocation-free
+                    // entry point), so it is read from global memory at the occupancy's indices
+                    act = nmat1 ? ((unsigned)m < (unsigned)nmat1 && mvs[m] != 0) : (m >= 0 && a.mv[m] != 0);
+                }
+                const unsigned bal = __ballot_sync(0xffffffffu, act);
+                if (bal) {
+                    if (first == nl) first = c0 + __ffs(bal) - 1;
+                    last = c0 + 31 - __clz(bal);
+                }
+            }
+            if (lane == 0) {
+                sb[r] = first;
+                ln[r] = last >= first ? last - first + 1 : 0;
+            }
+        }
+        __syncthreads();
+        // ---- list positions of the spans (exclusive prefix sum, warp 0)
+        if (warp == 0) {
+            int carry = 0;
+            for (int r0 = 0; r0 < nj; r0 += 32) {
+                const int r = r0 + lane;
+                const int x = r < nj ? ln[r] : 0;
+                int inc = x;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int y = __shfl_up_sync(0xffffffffu, inc, o);
+                    if (lane >= o) inc += y;
+                }
+                if (r < nj) off[r] = carry + inc - x;
+                carry += __shfl_sync(0xffffffffu, inc, 31);
+            }
+            if (lane == 0) off[nj] = carry;
+        }
+        __syncthreads();
+        const int total = off[nj];
+        // ---- chunks of the list
+#pragma unroll 1
+        for (int v0 = 0; v0 < total; v0 += CAP) {
+            const int v1 = v0 + CAP < total ? v0 + CAP : total, len = v1 - v0;
+            // copies: warp per row, the row's span cells that fall in [v0, v1)
+            for (int r = warp; r < nj; r += nwarps) {
+                const int o = off[r], n = ln[r];
+                if (o + n <= v0 || o >= v1) continue;   // uniform over the warp
+                const int c0 = sb[r];
+                for (int x = lane; x < n; x += 32) {
+                    const int vv = o + x;
+                    if (vv < v0 || vv >= v1) continue;
+                    const int l = c0 + x, m = occs[r * nl + l];
+                    const bool act = nmat1 ? ((unsigned)m < (unsigned)nmat1 && mvs[m] != 0) : (m >= 0 && a.mv[m] != 0);
+                    float2 *dst = P + 3 * NR * (size_t)(vv - v0);
+#pragma unroll
+                    for (int k = 0; k < NR; k++) {
+                        if (act) {
+                            const float2 *src = pr + (size_t)k * 3 * N + q0 + (size_t)r * nl + l;
+                            cp_async8(dst + 3 * k, src);
+                            cp_async8(dst + 3 * k + 1, src + N);
+                            cp_async8(dst + 3 * k + 2, src + 2 * N);
+                        } else {
+                            dst[3 * k] = czero();
+                            dst[3 * k + 1] = czero();
+                            dst[3 * k + 2] = czero();
+                        }
+                    }
+                    idx[vv - v0] = (unsigned)l | ((unsigned)r << 12) | ((unsigned)(m & 0xff) << 24);
+                }
+            }
+            cp_async_commit();
+            cp_async_wait_all();
+            __syncthreads();
+            // far field: worker w's share of the chunk
+            const int p0 = (int)(((long long)w * len) / s.RW), p1 = (int)(((long long)(w + 1) * len) / s.RW);
+            if (p0 < p1) {
+                float2 tt[NR][DPT][3];
+#pragma unroll
+                for (int r = 0; r < NR; r++)
+#pragma unroll
+                    for (int u = 0; u < DPT; u++)
+#pragma unroll
+                        for (int c = 0; c < 3; c++) tt[r][u][c] = czero();
+                int cur = (int)((idx[p0] >> 12) & 0xfff);
+#pragma unroll 2
+                for (int p = p0; p < p1; p++) {
+                    const unsigned id = idx[p];
+                    const int row = (int)((id >> 12) & 0xfff), l = (int)(id & 0xfff);
+                    if (row != cur) {
+                        // row end: acc += exp(i (kx x + ky y)) t
+                        float2 f[DPT];
+                        ld_dirs<DPT>(eyx + (size_t)cur * D + DPT * dg, f);
+#pragma unroll
+                        for (int r = 0; r < NR; r++)
+#pragma unroll
+                            for (int u = 0; u < DPT; u++)
+#pragma unroll
+                                for (int c = 0; c < 3; c++) {
+                                    acc[r][u][c] = cfma(f[u], tt[r][u][c], acc[r][u][c]);
+                                    tt[r][u][c] = czero();
+                                }
+                        cur = row;
+                    }
+                    float2 ev[DPT];
+                    ld_dirs<DPT>(ez + (size_t)l * D + DPT * dg, ev);
+#pragma unroll
+                    for (int r = 0; r < NR; r++) {
+                        const float2 *pp = P + 3 * (NR * p + r);
+                        const float2 pv[3] = {pp[0], pp[1], pp[2]};
+#pragma unroll
+                        for (int u = 0; u < DPT; u++)
+#pragma unroll
+                            for (int c = 0; c < 3; c++) tt[r][u][c] = cfma(ev[u], pv[c], tt[r][u][c]);
+                    }
+                }
+                float2 f[DPT];
+                ld_dirs<DPT>(eyx + (size_t)cur * D + DPT * dg, f);
+#pragma unroll
+                for (int r = 0; r < NR; r++)
+#pragma unroll
+                    for (int u = 0; u < DPT; u++)
+#pragma unroll
+                        for (int c = 0; c < 3; c++) acc[r][u][c] = cfma(f[u], tt[r][u][c], acc[r][u][c]);
+            }
+            if (cc) {
+                // CabsCext (dda_func.cpp:1688-1723) over the staged cells whose material has a
+                // nonzero polarisability and is active (mode 1)
+                for (int p = threadIdx.x; p < len; p += T) {
+                    const unsigned id = idx[p];
+                    const int m = (int)(id >> 24);
+                    if (m >= nmat1) continue;
+                    const int row = (int)((id >> 12) & 0xfff), l = (int)(id & 0xfff);
+                    const float2 ph = cmul(cmul(cx[ip], cy[row]), cz[l]);
+#pragma unroll
+                    for (int r = 0; r < NR; r++) {
+                        if (ccm[r * nmat1 + m] != 1) continue;
+                        double per = 0.0, pei = 0.0, pp = 0.0;
+#pragma unroll
+                        for (int c = 0; c < 3; c++) {
+                            const float2 Pc = P[3 * (NR * p + r) + c];
+                            const double er = Ec[r][2 * c], ei = Ec[r][2 * c + 1];   // conj(E)
+                            per += Pc.x * er - Pc.y * ei;
+                            pei += Pc.x * ei + Pc.y * er;
+                            pp += (double)Pc.x * Pc.x + (double)Pc.y * Pc.y;
+                        }
+                        v[r][0] += (double)ph.x * pei + (double)ph.y * per;   // Im(ph * (P . conj E))
+                        v[r][1] += pp * cwt[r * nmat1 + m] - (2.0 / 3.0) * pp;   // Im(pp / conj(alpha)) - 2/3 pp
+                    }
+                }
+            }
+            __syncthreads();   // the chunk buffers are refilled next
+        }
+        if (slow_cc) {
+            // materials with a polarisability but switched off in the activity list: their
+            // dipoles were not staged and are read from global memory
+            for (int e = threadIdx.x; e < (int)plane; e += T) {
+                const int m = occs[e];
+                if ((unsigned)m >= (unsigned)nmat1) continue;
+                const int row = e / nl, l = e - row * nl;
+                const float2 ph = cmul(cmul(cx[ip], cy[row]), cz[l]);
+#pragma unroll
+                for (int r = 0; r < NR; r++) {
+                    if (ccm[r * nmat1 + m] != 2) continue;
+                    double per = 0.0, pei = 0.0, pp = 0.0;
+#pragma unroll
+                    for (int c = 0; c < 3; c++) {
+                        const float2 Pc = pr[(size_t)r * 3 * N + c * N + q0 + e];
+                        const double er = Ec[r][2 * c], ei = Ec[r][2 * c + 1];
+                        per += Pc.x * er - Pc.y * ei;
+                        pei += Pc.x * ei + Pc.y * er;
+                        pp += (double)Pc.x * Pc.x + (double)Pc.y * Pc.y;
+                    }
+                    v[r][0] += (double)ph.x * pei + (double)ph.y * per;
+                    v[r][1] += pp * cwt[r * nmat1 + m] - (2.0 / 3.0) * pp;
+                }
+            }
+        }
+        __syncthreads();   // the plane's occupancy and spans are replaced next
+    }
+    // the sum over workers in FP64
+    float2 *red = P;   // [threads][NR][DPT][3]
+#pragma unroll
+    for (int r = 0; r < NR; r++)
+#pragma unroll
+        for (int u = 0; u < DPT; u++)
+#pragma unroll
+            for (int c = 0; c < 3; c++)
+                red[(((size_t)threadIdx.x * NR + r) * DPT + u) * 3 + c] = acc[r][u][c];
+    __syncthreads();
+    for (int o = threadIdx.x; o < NR * D * 6; o += T) {
+        const int r = o / (D * 6), dl = (o / 6) % D, k = o % 6, u = dl % DPT, g = dl / DPT, c = k >> 1;
         const int dd = dbase + dl;
         if (dd >= a.ndir) continue;
         double sum = 0.0;
-        for (int r = 0; r < s.RG * s.LG; r++) {
-            const float2 v = red[((size_t)(g + s.DG * r) * FF_DPT + u) * 3 + c];
-            sum += (k & 1) ? v.y : v.x;
+        for (int q = 0; q < s.RW; q++) {
+            const float2 x = red[(((size_t)(g + s.DG * q) * NR + r) * DPT + u) * 3 + c];
+            sum += (k & 1) ? x.y : x.x;
         }
-        if (sum != 0.0) atomicAdd(a.esc_acc + ((size_t)rhs * a.ndir + dd) * 6 + k, sum);
+        if (sum != 0.0) atomicAdd(a.esc_acc + ((size_t)(rhs + r) * a.ndir + dd) * 6 + k, sum);
+    }
+    if (cc) {
+#pragma unroll
+        for (int r = 0; r < NR; r++) {
+            __syncthreads();   // the reduction buffer is read above; block_sum_atomic reuses it
+            block_sum_atomic<2>(v[r], reinterpret_cast<double *>(red), a.cc_acc + 2 * (rhs + r));
+        }
     }
 }
 
@@ -337,19 +602,26 @@ inline unsigned nblk(size_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
 size_t farfield_smem(int nj, int nl)
 {
-    // the largest shape any direction count gives on this lattice
+    // the largest shape any direction count gives on this lattice, cross sections fused,
+    // every material slot in use
     size_t m = 0;
-    for (int nd = FF_DPT; nd <= FF_DMAX; nd += FF_DPT) {
-        const size_t b = ff_smem(ff_shape(nd, nj, nl), nj, nl);
-        m = b > m ? b : m;
+    for (int nd = FF_DQ; nd <= FF_DMAX; nd += FF_DQ) {
+        const size_t b1 = ff_layout(ff_shape(nd, 4), nj, nl, kMaxMaterials + 1, true, 1).total;
+        const size_t b2 = ff_layout(ff_shape(nd, 2), nj, nl, kMaxMaterials + 1, true, 2).total;
+        m = b1 > m ? b1 : m;
+        m = b2 > m ? b2 : m;
     }
     return m;
 }
 
 cudaError_t post_prepare(int nj, int nl)
 {
-    return cudaFuncSetAttribute(farfield_sum, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)farfield_smem(nj, nl));
+    const int bytes = (int)farfield_smem(nj, nl);
+    const cudaFuncAttribute at = cudaFuncAttributeMaxDynamicSharedMemorySize;
+    cudaError_t e = cudaFuncSetAttribute(farfield_sum<true, 1, 4>, at, bytes);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(farfield_sum<true, 2, 2>, at, bytes);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(farfield_sum<false, 1, 4>, at, bytes);
+    return e;
 }
 
 cudaError_t launch_post(const PostArgs &a, float2 *esc, float *cabs, float *cext, cudaStream_t st)
@@ -357,13 +629,21 @@ cudaError_t launch_post(const PostArgs &a, float2 *esc, float *cabs, float *cext
     cudaError_t e;
     if ((e = cudaMemsetAsync(a.esc_acc, 0, (size_t)a.nrhs * a.ndir * 6 * sizeof(double), st))) return e;
     if ((e = cudaMemsetAsync(a.cc_acc, 0, (size_t)a.nrhs * 2 * sizeof(double), st))) return e;
-    if (a.ndir > 0)
-    {
-        const FFShape s = ff_shape(a.ndir, a.nj, a.nl);
-        farfield_sum<<<dim3(nblk(a.ndir, s.D), nblk(a.ni, FF_PLANES), a.nrhs), s.threads,
-                       ff_smem(s, a.nj, a.nl), st>>>(a, s);
+    if (a.ndir > 0) {
+        // far field with the cross sections summed by the first direction chunk
+        if (a.nj >= 4096 || a.nl >= 4096) return cudaErrorInvalidValue;   // packed list words
+        if (a.pairs && a.nrhs % 2 == 0) {
+            const FFShape s = ff_shape(a.ndir, 2);
+            farfield_sum<true, 2, 2><<<dim3(nblk(a.ndir, s.D), nblk(a.ni, FF_PLANES), a.nrhs / 2), s.threads,
+                                       ff_layout(s, a.nj, a.nl, a.nmat1, true, 2).total, st>>>(a, s);
+        } else {
+            const FFShape s = ff_shape(a.ndir, 4);
+            farfield_sum<true, 1, 4><<<dim3(nblk(a.ndir, s.D), nblk(a.ni, FF_PLANES), a.nrhs), s.threads,
+                                       ff_layout(s, a.nj, a.nl, a.nmat1, true, 1).total, st>>>(a, s);
+        }
+    } else {
+        cabs_cext_sum<<<dim3(a.ni, a.nrhs), 256, (a.nj + a.nl) * sizeof(float2), st>>>(a);
     }
-    cabs_cext_sum<<<dim3(a.ni, a.nrhs), 256, (a.nj + a.nl) * sizeof(float2), st>>>(a);
     const size_t nd = (size_t)a.nrhs * a.ndir;
     const size_t nt = nd > (size_t)a.nrhs ? nd : (size_t)a.nrhs;
     post_finalize<<<nblk(nt, 256), 256, 0, st>>>(a, esc, cabs, cext);
@@ -435,9 +715,10 @@ cudaError_t farfield_noalloc(const PostArgs &in, const float *ksc_dev, float2 *e
     if ((e = cudaMemsetAsync(a.esc_acc, 0, (size_t)a.ndir * 6 * sizeof(double), st))) return e;
     const int n3 = 3 * a.ndir;
     ksc_to_double<<<nblk((size_t)n3, 256), 256, 0, st>>>(ksc_dev, kscd, n3);
-    const FFShape s = ff_shape(a.ndir, a.nj, a.nl);
-    farfield_sum<<<dim3(nblk(a.ndir, s.D), nblk(a.ni, FF_PLANES), 1), s.threads, ff_smem(s, a.nj, a.nl),
-                   st>>>(a, s);
+    if (a.nj >= 4096 || a.nl >= 4096) return cudaErrorInvalidValue;   // packed list words
+    const FFShape s = ff_shape(a.ndir, 4);
+    farfield_sum<false, 1, 4><<<dim3(nblk(a.ndir, s.D), nblk(a.ni, FF_PLANES), 1), s.threads,
+                                ff_layout(s, a.nj, a.nl, a.nmat1, false, 1).total, st>>>(a, s);
     post_finalize<<<nblk((size_t)a.ndir, 256), 256, 0, st>>>(a, esc_dev, nullptr, nullptr);
     return cudaGetLastError();
 }

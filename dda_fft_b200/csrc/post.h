@@ -20,6 +20,8 @@ struct PostArgs {
     const double *ksc;        // [nrhs][ndir][3]
     double *esc_acc;          // [nrhs][ndir][6] scratch
     double *cc_acc;           // [nrhs][2] scratch (Cext sum, Cabs sum)
+    int pairs;                // right-hand sides 2k, 2k+1 share directions, incident
+                              // direction and occupancy (both polarisations of one orientation)
 };
 
 struct MuellerArgs {
