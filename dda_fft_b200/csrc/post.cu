@@ -18,7 +18,7 @@ namespace ddagpu {
 
 namespace {
 
-// Far-field tiling.  A CTA takes FF_PLANES lattice planes i of one right-hand side and up to
+// Far-field tiling.  A CTA takes s.planes (<= FF_PLANES) lattice planes i of one right-hand side and up to
 // FF_DMAX directions, whose phase tables (one per axis) it builds once.  Thread (dg, w)
 // accumulates DPT directions x 3 components; the RW threads w of one direction group are
 // workers that split the plane's dipoles evenly:
@@ -39,18 +39,24 @@ namespace {
 // read from HBM once for both.
 constexpr int FF_DMAX = 32;
 constexpr int FF_DQ = 4;         // directions per CTA are padded to a multiple of this
-constexpr int FF_PLANES = 8;     // lattice planes per CTA
+constexpr int FF_PLANES = 8;     // lattice planes per CTA at most
 
 // list cells per chunk
 __host__ __device__ constexpr int ff_cap(int nr) { return nr == 2 ? 512 : 1024; }
 
 struct FFShape {
-    int D, dpt, DG, RW, threads;
+    int D, dpt, DG, RW, threads, planes;
 };
 
-FFShape ff_shape(int ndir, int dpt)
+// blocks: right-hand-side blocks of the grid (nrhs / NR); the planes per CTA are the most
+// that still give the grid eight CTAs per SM (148 SMs), two at least, so that the plane
+// groups' unequal work (a target's middle planes hold more dipoles) is spread
+FFShape ff_shape(int ndir, int dpt, int ni = 1, int blocks = 1)
 {
     FFShape s;
+    const int chunks = (ndir + FF_DMAX - 1) / FF_DMAX;
+    s.planes = FF_PLANES;
+    while (s.planes > 2 && (long long)((ni + s.planes - 1) / s.planes) * chunks * blocks < 8 * 148) s.planes /= 2;
     s.D = ndir >= FF_DMAX ? FF_DMAX : ((ndir + FF_DQ - 1) / FF_DQ) * FF_DQ;
     if (s.D < FF_DQ) s.D = FF_DQ;
     s.dpt = dpt;
@@ -111,7 +117,7 @@ DDA_DEV void cp_async8(void *dst, const void *src)
 DDA_DEV void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 DDA_DEV void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
-// grid (direction chunks of D, plane groups of FF_PLANES, nrhs / NR); the lattice has
+// grid (direction chunks of D, plane groups of s.planes, nrhs / NR); the lattice has
 // nj, nl < 4096
 template <bool CC, int NR, int DPT>
 __global__ void __launch_bounds__(256) farfield_sum(PostArgs a, FFShape s)
@@ -119,8 +125,8 @@ __global__ void __launch_bounds__(256) farfield_sum(PostArgs a, FFShape s)
     constexpr int CAP = ff_cap(NR);
     extern __shared__ __align__(16) unsigned char smraw[];
     const int nj = a.nj, nl = a.nl, D = s.D, T = blockDim.x, nmat1 = a.nmat1;
-    const int dbase = blockIdx.x * D, i0 = blockIdx.y * FF_PLANES, rhs = NR * blockIdx.z;
-    const int np = a.ni - i0 < FF_PLANES ? a.ni - i0 : FF_PLANES;
+    const int dbase = blockIdx.x * D, i0 = blockIdx.y * s.planes, rhs = NR * blockIdx.z;
+    const int np = a.ni - i0 < s.planes ? a.ni - i0 : s.planes;
     const bool cc = CC && blockIdx.x == 0;
     const int dg = threadIdx.x % s.DG, w = threadIdx.x / s.DG;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = T >> 5;
@@ -633,12 +639,12 @@ cudaError_t launch_post(const PostArgs &a, float2 *esc, float *cabs, float *cext
         // far field with the cross sections summed by the first direction chunk
         if (a.nj >= 4096 || a.nl >= 4096) return cudaErrorInvalidValue;   // packed list words
         if (a.pairs && a.nrhs % 2 == 0) {
-            const FFShape s = ff_shape(a.ndir, 2);
-            farfield_sum<true, 2, 2><<<dim3(nblk(a.ndir, s.D), nblk(a.ni, FF_PLANES), a.nrhs / 2), s.threads,
+            const FFShape s = ff_shape(a.ndir, 2, a.ni, a.nrhs / 2);
+            farfield_sum<true, 2, 2><<<dim3(nblk(a.ndir, s.D), nblk(a.ni, s.planes), a.nrhs / 2), s.threads,
                                        ff_layout(s, a.nj, a.nl, a.nmat1, true, 2).total, st>>>(a, s);
         } else {
-            const FFShape s = ff_shape(a.ndir, 4);
-            farfield_sum<true, 1, 4><<<dim3(nblk(a.ndir, s.D), nblk(a.ni, FF_PLANES), a.nrhs), s.threads,
+            const FFShape s = ff_shape(a.ndir, 4, a.ni, a.nrhs);
+            farfield_sum<true, 1, 4><<<dim3(nblk(a.ndir, s.D), nblk(a.ni, s.planes), a.nrhs), s.threads,
                                        ff_layout(s, a.nj, a.nl, a.nmat1, true, 1).total, st>>>(a, s);
         }
     } else {
@@ -716,8 +722,8 @@ cudaError_t farfield_noalloc(const PostArgs &in, const float *ksc_dev, float2 *e
     const int n3 = 3 * a.ndir;
     ksc_to_double<<<nblk((size_t)n3, 256), 256, 0, st>>>(ksc_dev, kscd, n3);
     if (a.nj >= 4096 || a.nl >= 4096) return cudaErrorInvalidValue;   // packed list words
-    const FFShape s = ff_shape(a.ndir, 4);
-    farfield_sum<false, 1, 4><<<dim3(nblk(a.ndir, s.D), nblk(a.ni, FF_PLANES), 1), s.threads,
+    const FFShape s = ff_shape(a.ndir, 4, a.ni, 1);
+    farfield_sum<false, 1, 4><<<dim3(nblk(a.ndir, s.D), nblk(a.ni, s.planes), 1), s.threads,
                                 ff_layout(s, a.nj, a.nl, a.nmat1, false, 1).total, st>>>(a, s);
     post_finalize<<<nblk((size_t)a.ndir, 256), 256, 0, st>>>(a, esc_dev, nullptr, nullptr);
     return cudaGetLastError();
