@@ -68,6 +68,23 @@ DDA_DEV void axpy3(float2 (&y)[3], float2 a, const float2 (&x)[3])
     for (int c = 0; c < 3; c++) y[c] = cadd(y[c], cmul(a, x[c]));
 }
 
+// A warp takes FB x 32 consecutive cells per pass: lane t has cells q0 + t + 32 k, k < FB,
+// so every access of the warp stays one contiguous run and a thread has the loads of its
+// FB cells in flight together.
+constexpr int FB = 4;
+DDA_DEV void occ_batch(const signed char *occ, size_t N, size_t q0, int (&m)[FB])
+{
+#pragma unroll
+    for (int k = 0; k < FB; k++) m[k] = q0 + 32 * k < N ? (int)occ[q0 + 32 * k] : 0;
+}
+// first cell of this thread and the stride between passes
+DDA_DEV size_t fb_first()
+{
+    const size_t gt = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    return (gt >> 5) * (32 * FB) + (gt & 31);
+}
+DDA_DEV size_t fb_stride() { return (size_t)gridDim.x * blockDim.x * FB; }
+
 // ------------------------------------------------------------------ field pass
 template <int OP>
 __global__ void __launch_bounds__(256) field_op(FieldArgs a)
@@ -256,21 +273,37 @@ __global__ void __launch_bounds__(256) first_approx(FieldArgs a)
     const size_t N = a.N, off = (size_t)rhs * 3 * N;
     const float2 *al = a.alpha + (size_t)rhs * a.nmat1;
     const signed char *occ = a.occ + (size_t)rhs * a.occ_stride;
-    for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < N;
-         q += (size_t)gridDim.x * blockDim.x) {
-        const int l = (int)(q % nl), j = (int)((q / nl) % nj), i = (int)(q / ((size_t)nl * nj));
-        const int m = occ[q];
-        float2 out[3];
-        if (a.mv[m]) {
-            const float2 ph = cmul(cmul(tab[nj + nl + i], tab[j]), tab[nj + l]);
-            const float2 c1 = cmul(ph, al[m]);
+    const float2 Ef[3] = {make_float2((float)E[0], (float)E[1]), make_float2((float)E[2], (float)E[3]),
+                          make_float2((float)E[4], (float)E[5])};
+    for (size_t q0 = fb_first(); q0 < N; q0 += fb_stride()) {
+        int mk[FB];
+        occ_batch(occ, N, q0, mk);
+        // lattice position of the first cell; the others are 32 cells further along l
+        // (wrapping rows)
+        const unsigned q0u = (unsigned)q0, row = q0u / (unsigned)nl;   // lattices below 2^32 cells
+        int l = (int)(q0u - row * (unsigned)nl), j = (int)(row % (unsigned)nj), i = (int)(row / (unsigned)nj);
 #pragma unroll
-            for (int c = 0; c < 3; c++)
-                out[c] = cmul(c1, make_float2((float)E[2 * c], (float)E[2 * c + 1]));
-        } else {
-            z3(out);
+        for (int k = 0; k < FB; k++) {
+            const size_t q = q0 + 32 * k;
+            if (q >= N) break;
+            const int m = mk[k];
+            float2 out[3];
+            if (a.mv[m]) {
+                const float2 ph = cmul(cmul(tab[nj + nl + i], tab[j]), tab[nj + l]);
+                const float2 c1 = cmul(ph, al[m]);
+#pragma unroll
+                for (int c = 0; c < 3; c++) out[c] = cmul(c1, Ef[c]);
+            } else {
+                z3(out);
+            }
+            st3(a.p + off, N, q, out);
+            for (l += 32; l >= nl; l -= nl) {
+                if (++j == nj) {
+                    j = 0;
+                    ++i;
+                }
+            }
         }
-        st3(a.p + off, N, q, out);
     }
 }
 
@@ -497,7 +530,7 @@ cudaError_t launch_field_op(int op, const FieldArgs &a, cudaStream_t st)
 
 cudaError_t launch_first_approx(const FieldArgs &a, cudaStream_t st)
 {
-    const unsigned bx = (unsigned)((a.N + 1023) / 1024);
+    const unsigned bx = (unsigned)((a.N + 256 * FB - 1) / (256 * FB));
     first_approx<<<dim3(bx < 1 ? 1 : bx, a.nrhs), 256, (a.ni + a.nj + a.nl) * sizeof(float2), st>>>(a);
     return cudaGetLastError();
 }
@@ -576,7 +609,11 @@ cudaError_t launch_loop_control(const int *active, int nrhs, const int *step_dev
 
 cudaError_t launch_gated_copy(const FieldArgs &a, int dir, cudaStream_t st)
 {
-    const unsigned bx = (unsigned)((3 * a.N / 2 + 1023) / 1024);
+    // most right-hand sides copy nothing at a given step: a capped grid (grid-stride loop)
+    // keeps the launch of the idle blocks cheap
+    unsigned bx = (unsigned)((3 * a.N / 2 + 1023) / 1024);
+    const unsigned cap = (unsigned)(4096 / (a.nrhs > 0 ? a.nrhs : 1));
+    if (bx > (cap < 8 ? 8 : cap)) bx = cap < 8 ? 8 : cap;
     gated_copy<<<dim3(bx < 1 ? 1 : bx, a.nrhs), 256, 0, st>>>(a, dir);
     return cudaGetLastError();
 }
