@@ -89,6 +89,7 @@ struct ddagpu_ctx {
     float2 *alpha = nullptr;
     int nmat_cap = kMaxMaterials + 1;
     double *kinc = nullptr, *einc = nullptr;
+    float2 *inc_tab = nullptr;   // [max_rhs][nj + nl + ni] incident phase tables
     // post-processing buffers, grown on demand
     int ndir_cap = 0;
     double *ksc = nullptr, *esc_acc = nullptr, *cc_acc = nullptr, *normals = nullptr,
@@ -480,10 +481,22 @@ int run_solver(ddagpu_ctx *c, int nrhs, int solver, float tau, int max_step, flo
 
     // ---- step 0 (dda_func.cpp:1102-1293): p = p_inc, or the given right-hand side
     auto step0 = [&]() -> int {
-    if (rhs_in) CK(launch_refine(4, F, st));
-    else CK(launch_first_approx(F, st));
-    c->launches += 1;
-    CK(matvec(c->p, c->r, 0.f, nullptr, 0));   // r = -alpha (G * p_inc)
+    if (!rhs_in && c->fast) {
+        // the forward pass computes p_inc itself (from the phase tables) and stores it
+        CK(launch_inc_tables(F, c->inc_tab, st));
+        MatvecArgs m = mv_args(c, nrhs, c->p, c->r, 1, 0.f, nullptr, 0, nmat1, true);
+        m.inc = 1;
+        m.inc_tab = c->inc_tab;
+        m.einc = c->einc;
+        m.inc_out = c->p;
+        c->launches += 4;
+        CK(launch_matvec(m, st));   // p = p_inc, r = -alpha (G * p_inc)
+    } else {
+        if (rhs_in) CK(launch_refine(4, F, st));
+        else CK(launch_first_approx(F, st));
+        c->launches += 1;
+        CK(matvec(c->p, c->r, 0.f, nullptr, 0));   // r = -alpha (G * p_inc)
+    }
     res.matvec0 = 1;
     switch (solver) {
     case 0:   // s = r is deferred to the first iteration (an RHS converged at step 0 never needs it)
@@ -834,6 +847,7 @@ int ddagpu_create(ddagpu_ctx **out, int device, int i_max, int j_max, int l_max,
     A(dalloc(&c->alpha, (size_t)c->nmat_cap * max_rhs));
     A(dalloc(&c->kinc, (size_t)3 * max_rhs));
     A(dalloc(&c->einc, (size_t)6 * max_rhs));
+    A(dalloc(&c->inc_tab, (size_t)(i_max + j_max + l_max) * max_rhs));
     A(dalloc(&c->cc_acc, (size_t)2 * max_rhs));
     A(dalloc(&c->cabs, (size_t)max_rhs));
     A(dalloc(&c->cext, (size_t)max_rhs));
@@ -882,7 +896,8 @@ int ddagpu_destroy(ddagpu_ctx *c)
                     c->w,    c->g,      c->h,      c->state,   c->active, c->trace, c->occ,
                     c->mv,   c->alpha,  c->kinc,   c->einc,    c->ksc,    c->esc_acc,
                     c->cc_acc, c->normals, c->mueller, c->esc, c->cabs,   c->cext,
-                    c->occ_b, c->ndip, c->step_dev, c->nact_dev, c->err_dev, c->worm_buf};
+                    c->occ_b, c->ndip, c->step_dev, c->nact_dev, c->err_dev, c->worm_buf,
+                    c->inc_tab};
     for (void *q : ptrs)
         if (q) cudaFree(q);
     if (c->st) cudaStreamDestroy(c->st);

@@ -71,6 +71,13 @@ struct MatvecArgs {
     int fx, fyz;            // launch variants of the fast x pass (0..5) and y/z passes (0..2)
     int *err;               // device flag set by a kernel whose bounded wait gave up (or null)
     int wait_selftest;      // 1: the bulk-copy wait waits (briefly) for a phase that never completes
+    // step 0 from the incident field (compile-time-sized passes only): the forward y/z pass
+    // computes its input p = alpha_m exp(i k.(r - c)) E_inc on active cells (0 elsewhere)
+    // from the occupancy and materials of ep instead of reading src, and writes it to inc_out
+    int inc;
+    const float2 *inc_tab;  // [nrhs][nj + nl + ni] phase tables (y, z, x)
+    const double *einc;     // [nrhs][6] incident field
+    float2 *inc_out;        // [nrhs][3][N]
 };
 
 // kernels (matvec.cu)

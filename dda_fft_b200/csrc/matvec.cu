@@ -221,6 +221,7 @@ cudaError_t matvec_prepare(const Lat &L, int tile_x, int rows_g)
 cudaError_t launch_matvec(const MatvecArgs &a, cudaStream_t st)
 {
     if (a.fast) return launch_matvec_fast(a, st);
+    if (a.inc) return cudaErrorInvalidValue;   // the incident-field input needs the sized passes
     const Lat &L = a.L;
     const size_t syz = matvec_smem_yz(L, a.rows_g), sx = matvec_smem_x(L, a.tile_x);
     k1_forward_yz<<<dim3(2 * L.ni, 3, a.nrhs), 512, syz, st>>>(a);

@@ -84,7 +84,8 @@ DDA_DEV void row_fft_from_regs(float2 *row, int lane_sub, bool valid, float2 (&v
 // ------------------------------------------------------------------------------ K1
 // CTA (i, component, z half hl): z-forward of the NJ rows of plane i (half hl only), then
 // y-forward of the NL columns for both y halves; writes work rows in split order.
-template <int NJ, int NL, int NT>
+// INC: the input is the incident field, computed here (and written by the hl = 0 CTAs).
+template <int NJ, int NL, int NT, bool INC>
 __global__ void __launch_bounds__(NT) k1f(MatvecArgs a)
 {
     using SJ = Sp<NJ>;
@@ -98,7 +99,61 @@ __global__ void __launch_bounds__(NT) k1f(MatvecArgs a)
     const float2 *twl = a.L.tw_l, *hwl = a.L.tw_l + NL, *twj = a.L.tw_j, *hwj = a.L.tw_j + NJ;
 
     // ---- z: rows, row role
-    {
+    if constexpr (INC) {
+        // incident dipoles of this plane and component (FirstApproximation,
+        // dda_func.cpp:654-689) with the products of the separate pass, in its order:
+        // ((x phase * y phase) * z phase) * alpha_m * E_c
+        constexpr int RM = SL::RM, RPP = NT / RM, R1 = SL::R1, R2 = SL::R2;
+        const int sub = threadIdx.x % RM, rr = threadIdx.x / RM;
+        const Epilogue &ep = a.ep;
+        const float2 *tab = a.inc_tab + (size_t)rhs * (NJ + NL + ni);
+        const float2 tx = tab[NJ + NL + i];
+        float2 tz[R1];
+#pragma unroll
+        for (int r = 0; r < R1; r++) tz[r] = sub < R2 ? tab[NJ + sub + R2 * r] : czero();
+        const double *E = a.einc + 6 * rhs;
+        const float2 Ef = make_float2((float)E[2 * c], (float)E[2 * c + 1]);
+        const signed char *ob = ep.occ + (size_t)rhs * ep.occ_stride + (size_t)i * NJ * NL;
+        const float2 *al = ep.alpha + (size_t)rhs * ep.nmat1;
+        // up to two materials from registers
+        const bool rt = ep.nmat1 <= 2;
+        const bool mv0 = ep.mv[0] != 0, mv1 = ep.nmat1 > 1 && ep.mv[1] != 0;
+        const float2 al0 = al[0], al1 = ep.nmat1 > 1 ? al[1] : czero();
+        float2 *pout = a.inc_out + (size_t)rhs * a.fstride + ((size_t)c * ni + i) * (NJ * NL);
+        // the occupancy of the next pass's row is loaded while this pass's row is transformed
+        auto load = [&](int row, int (&o)[R1], float2 &ty) {
+            if (row < NJ && sub < R2) {
+#pragma unroll
+                for (int r = 0; r < R1; r++) o[r] = ob[row * NL + sub + R2 * r];
+                ty = tab[row];
+            }
+        };
+        int o[R1], on[R1];
+        float2 ty = czero(), tyn = czero();
+        load(rr, o, ty);
+#pragma unroll 1
+        for (int r0 = 0; r0 < NJ; r0 += RPP) {
+            const int row = r0 + rr;
+            if (r0 + RPP < NJ) load(row + RPP, on, tyn);
+            float2 v[R1];
+            if (row < NJ && sub < R2) {
+                const float2 txy = cmul(tx, ty);
+#pragma unroll
+                for (int r = 0; r < R1; r++) {
+                    const int m = o[r];
+                    const bool act = rt ? ((m & 1) ? mv1 : mv0) : ep.mv[m] != 0;
+                    float2 val = czero();
+                    if (act) val = cmul(cmul(cmul(txy, tz[r]), rt ? ((m & 1) ? al1 : al0) : al[m]), Ef);
+                    if (hl == 0) pout[row * NL + sub + R2 * r] = val;
+                    v[r] = hl ? cmul(val, __ldg(&hwl[sub + R2 * r])) : val;
+                }
+            }
+            row_fft_from_regs<NL, false>(Z + (row < NJ ? row : 0) * PS, sub, row < NJ, v, twl);
+#pragma unroll
+            for (int r = 0; r < R1; r++) o[r] = on[r];
+            ty = tyn;
+        }
+    } else {
         constexpr int RM = SL::RM, RPP = NT / RM;   // rows per pass
         const int sub = threadIdx.x % RM, rr = threadIdx.x / RM;
         // the next pass's row is loaded while this pass's row is transformed
@@ -613,7 +668,8 @@ void launch_yz_v(const MatvecArgs &a, int fwd, cudaStream_t st)
 {
     constexpr int NT = yz_threads<NJ, NL>(V);
     constexpr size_t S = yz_smem<NJ, NL>();
-    if (fwd) k1f<NJ, NL, NT><<<dim3(2 * a.L.ni, 3, a.nrhs), NT, S, st>>>(a);
+    if (fwd && a.inc) k1f<NJ, NL, NT, true><<<dim3(2 * a.L.ni, 3, a.nrhs), NT, S, st>>>(a);
+    else if (fwd) k1f<NJ, NL, NT, false><<<dim3(2 * a.L.ni, 3, a.nrhs), NT, S, st>>>(a);
     else k3f<NJ, NL, NT><<<dim3(2 * a.L.ni, 3, a.nrhs), NT, S, st>>>(a);
 }
 
@@ -630,7 +686,9 @@ cudaError_t prep_yz_v()
 {
     constexpr int NT = yz_threads<NJ, NL>(V);
     constexpr int S = (int)yz_smem<NJ, NL>();
-    cudaError_t e = cudaFuncSetAttribute(k1f<NJ, NL, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, S);
+    cudaError_t e = cudaFuncSetAttribute(k1f<NJ, NL, NT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, S);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k1f<NJ, NL, NT, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, S);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k3f<NJ, NL, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, S);
     return e;

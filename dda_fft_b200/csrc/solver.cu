@@ -254,7 +254,26 @@ __global__ void __launch_bounds__(256) field_op(FieldArgs a)
 
 // ------------------------------------------------------------ incident dipoles
 // p = alpha_m exp(i k.(r - c)) E_inc on active cells, c = (n-1) d0 / 2 per axis; the
-// phase is separable, so each block builds exp(i k_y y) and exp(i k_z z) tables.
+// phase is separable: entry e of the tables [nj] y, [nl] z, [ni] x is exp(i k_a (x_a - c_a)).
+DDA_DEV float2 inc_phase(const FieldArgs &a, const double *k, int e)
+{
+    const int ni = a.ni, nj = a.nj, nl = a.nl;
+    const double cx = (ni - 1) * a.d0 / 2, cy = (nj - 1) * a.d0 / 2, cz = (nl - 1) * a.d0 / 2;
+    const double ph = e < nj        ? k[1] * (e * a.d0 - cy)
+                    : e < nj + nl   ? k[2] * ((e - nj) * a.d0 - cz)
+                                    : k[0] * ((e - nj - nl) * a.d0 - cx);
+    return expi_reduced(ph);
+}
+
+// The phase tables of every right-hand side, [nrhs][nj + nl + ni], for the forward pass that
+// computes the incident dipoles itself (step 0 of a solve on the compile-time-sized passes).
+__global__ void __launch_bounds__(256) inc_tables(FieldArgs a, float2 *tab)
+{
+    const int rhs = blockIdx.x, n = a.nj + a.nl + a.ni;
+    if (a.rhs_active && !a.rhs_active[rhs]) return;
+    for (int e = threadIdx.x; e < n; e += blockDim.x) tab[(size_t)rhs * n + e] = inc_phase(a, a.kinc + 3 * rhs, e);
+}
+
 __global__ void __launch_bounds__(256) first_approx(FieldArgs a)
 {
     extern __shared__ float2 tab[];   // [nj] y, [nl] z, then [ni] x
@@ -262,13 +281,7 @@ __global__ void __launch_bounds__(256) first_approx(FieldArgs a)
     if (a.rhs_active && !a.rhs_active[rhs]) return;
     const int ni = a.ni, nj = a.nj, nl = a.nl;
     const double *k = a.kinc + 3 * rhs, *E = a.einc + 6 * rhs;
-    const double cx = (ni - 1) * a.d0 / 2, cy = (nj - 1) * a.d0 / 2, cz = (nl - 1) * a.d0 / 2;
-    for (int e = threadIdx.x; e < nj + nl + ni; e += blockDim.x) {
-        const double ph = e < nj        ? k[1] * (e * a.d0 - cy)
-                        : e < nj + nl   ? k[2] * ((e - nj) * a.d0 - cz)
-                                        : k[0] * ((e - nj - nl) * a.d0 - cx);
-        tab[e] = expi_reduced(ph);
-    }
+    for (int e = threadIdx.x; e < nj + nl + ni; e += blockDim.x) tab[e] = inc_phase(a, k, e);
     __syncthreads();
     const size_t N = a.N, off = (size_t)rhs * 3 * N;
     const float2 *al = a.alpha + (size_t)rhs * a.nmat1;
@@ -525,6 +538,12 @@ cudaError_t launch_field_op(int op, const FieldArgs &a, cudaStream_t st)
 #undef CASE
     default: return cudaErrorInvalidValue;
     }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_inc_tables(const FieldArgs &a, float2 *tab, cudaStream_t st)
+{
+    inc_tables<<<a.nrhs, 256, 0, st>>>(a, tab);
     return cudaGetLastError();
 }
 

@@ -44,6 +44,8 @@ struct FieldArgs {
 
 cudaError_t launch_field_op(int op, const FieldArgs &a, cudaStream_t st);
 cudaError_t launch_first_approx(const FieldArgs &a, cudaStream_t st);
+// phase tables [nrhs][nj + nl + ni] of the incident field (y, z, x), the values first_approx uses
+cudaError_t launch_inc_tables(const FieldArgs &a, float2 *tab, cudaStream_t st);
 // step_dev (may be null): read the step number from device memory; `step` then holds
 // Max_Step, past which SC_TOP only clears the copy flag
 cudaError_t launch_scalar(RhsState *st_, const int *act_in, int *act_out, int nrhs, int stage,
