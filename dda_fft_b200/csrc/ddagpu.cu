@@ -90,6 +90,10 @@ struct ddagpu_ctx {
     int nmat_cap = kMaxMaterials + 1;
     double *kinc = nullptr, *einc = nullptr;
     float2 *inc_tab = nullptr;   // [max_rhs][nj + nl + ni] incident phase tables
+    // pinned host staging of the batched calls' inputs and outputs, grown on demand (the
+    // copies from and to it are asynchronous, unlike those of pageable memory)
+    unsigned char *pin = nullptr;
+    size_t pin_bytes = 0;
     // post-processing buffers, grown on demand
     int ndir_cap = 0;
     double *ksc = nullptr, *esc_acc = nullptr, *cc_acc = nullptr, *normals = nullptr,
@@ -900,6 +904,7 @@ int ddagpu_destroy(ddagpu_ctx *c)
                     c->inc_tab};
     for (void *q : ptrs)
         if (q) cudaFree(q);
+    if (c->pin) cudaFreeHost(c->pin);
     if (c->st) cudaStreamDestroy(c->st);
     delete c;
     return DDAGPU_OK;
@@ -1200,6 +1205,19 @@ struct OccBatch {
     ~OccBatch() { c->occ_stride = 0; }
 };
 
+// Pinned staging of at least `bytes` (the stream is idle: every batched chunk ends with a
+// synchronisation).
+int ensure_pin(ddagpu_ctx *c, size_t bytes)
+{
+    if (bytes <= c->pin_bytes) return DDAGPU_OK;
+    if (c->pin) cudaFreeHost(c->pin);
+    c->pin = nullptr;
+    c->pin_bytes = 0;
+    CK(cudaHostAlloc((void **)&c->pin, bytes, cudaHostAllocDefault));
+    c->pin_bytes = bytes;
+    return DDAGPU_OK;
+}
+
 // Solves no orientations (rotation matrices rot[no][9]) as 2 no right-hand sides -- both
 // incident polarisations, x and y before rotation (main.cpp:153-154) -- whose occupancy is
 // on the device, then far fields, cross sections and the Mueller matrices averaged over the
@@ -1210,9 +1228,21 @@ int batch_chunk(ddagpu_ctx *c, const ddagpu_batch_cfg *cfg, const BatchGeom &g, 
 {
     const int nr = 2 * no, ndir = g.ndir, nP = g.nP, nA = g.nA, nmat1 = g.nmat1;
     const double d0 = c->kd;
-    std::vector<double> kin((size_t)nr * 3, 0.0), ein((size_t)nr * 6, 0.0),
-        ks((size_t)nr * ndir * 3, 0.0), nv((size_t)no * nP * 3, 0.0);
-    std::vector<float2> al((size_t)nr * nmat1, make_float2(0.f, 0.f));
+    // pinned layout: inputs kin, ein, ks, nv (double), al (float2); outputs ca, ce (float),
+    // mo (double); every block 16-byte aligned
+    auto al16 = [](size_t b) { return (b + 15) & ~(size_t)15; };
+    const size_t n_kin = (size_t)nr * 3, n_ein = (size_t)nr * 6, n_ks = (size_t)nr * ndir * 3,
+                 n_nv = (size_t)no * nP * 3, n_al = (size_t)nr * nmat1, n_mo = (size_t)no * nA * 16;
+    const size_t o_ein = al16(n_kin * 8), o_ks = o_ein + al16(n_ein * 8), o_nv = o_ks + al16(n_ks * 8),
+                 o_al = o_nv + al16(n_nv * 8), o_ca = o_al + al16(n_al * 8), o_ce = o_ca + al16((size_t)nr * 4),
+                 o_mo = o_ce + al16((size_t)nr * 4), total = o_mo + al16(n_mo * 8);
+    RET(ensure_pin(c, total));
+    double *kin = (double *)c->pin, *ein = (double *)(c->pin + o_ein), *ks = (double *)(c->pin + o_ks),
+           *nv = (double *)(c->pin + o_nv);
+    float2 *al = (float2 *)(c->pin + o_al);
+    float *ca = (float *)(c->pin + o_ca), *ce = (float *)(c->pin + o_ce);
+    double *mo = (double *)(c->pin + o_mo);
+    std::memset(c->pin, 0, o_ca);
     for (int o = 0; o < no; o++) {
         const double *T = rot + 9 * (size_t)o;
         auto R = [&](const double *v, double *out) {
@@ -1232,20 +1262,20 @@ int batch_chunk(ddagpu_ctx *c, const ddagpu_batch_cfg *cfg, const BatchGeom &g, 
                 ein[6 * rr + 2 * i + 1] = 0.0;
             }
             for (int dd = 0; dd < ndir; dd++)
-                R(g.ksc0.data() + 3 * dd, ks.data() + ((size_t)rr * ndir + dd) * 3);
+                R(g.ksc0.data() + 3 * dd, ks + ((size_t)rr * ndir + dd) * 3);
             for (int mm = 0; mm < cfg->n_mat; mm++) {
                 const cd a = polarizability(cfg->polarizability, d0, {cfg->m[2 * mm], cfg->m[2 * mm + 1]},
-                                            kin.data() + 3 * rr, ein.data() + 6 * rr);
+                                            kin + 3 * rr, ein + 6 * rr);
                 al[(size_t)rr * nmat1 + mm + 1] = make_float2((float)a.r, (float)a.i);
             }
         }
-        for (int pl = 0; pl < nP; pl++) R(g.nrm0.data() + 3 * pl, nv.data() + ((size_t)o * nP + pl) * 3);
+        for (int pl = 0; pl < nP; pl++) R(g.nrm0.data() + 3 * pl, nv + ((size_t)o * nP + pl) * 3);
     }
-    CK(cudaMemcpyAsync(c->kinc, kin.data(), kin.size() * sizeof(double), cudaMemcpyHostToDevice, c->st));
-    CK(cudaMemcpyAsync(c->einc, ein.data(), ein.size() * sizeof(double), cudaMemcpyHostToDevice, c->st));
-    CK(cudaMemcpyAsync(c->ksc, ks.data(), ks.size() * sizeof(double), cudaMemcpyHostToDevice, c->st));
-    CK(cudaMemcpyAsync(c->normals, nv.data(), nv.size() * sizeof(double), cudaMemcpyHostToDevice, c->st));
-    CK(cudaMemcpyAsync(c->alpha, al.data(), al.size() * sizeof(float2), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->kinc, kin, n_kin * sizeof(double), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->einc, ein, n_ein * sizeof(double), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->ksc, ks, n_ks * sizeof(double), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->normals, nv, n_nv * sizeof(double), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->alpha, al, n_al * sizeof(float2), cudaMemcpyHostToDevice, c->st));
     SolveResult res;
     // far field, cross sections and the plane-averaged Mueller matrices, after the solve
     // (recorded with it when the solve is one graph launch)
@@ -1259,18 +1289,15 @@ int batch_chunk(ddagpu_ctx *c, const ddagpu_batch_cfg *cfg, const BatchGeom &g, 
     c->post_key = ((long long)ndir << 40) | ((long long)no << 24) | ((long long)nP << 12) | nA;
     RET(run_solver(c, nr, cfg->solver, cfg->tau, cfg->max_step, cfg->err_max, nmat1, d0, nact, res,
                    false, nullptr, nact_per, &post));
-    std::vector<float> ca((size_t)nr), ce((size_t)nr);
-    std::vector<double> mo((size_t)no * nA * 16);
-    CK(cudaMemcpyAsync(ca.data(), c->cabs, nr * sizeof(float), cudaMemcpyDeviceToHost, c->st));
-    CK(cudaMemcpyAsync(ce.data(), c->cext, nr * sizeof(float), cudaMemcpyDeviceToHost, c->st));
-    if (mueller)
-        CK(cudaMemcpyAsync(mo.data(), c->mueller, mo.size() * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaMemcpyAsync(ca, c->cabs, nr * sizeof(float), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaMemcpyAsync(ce, c->cext, nr * sizeof(float), cudaMemcpyDeviceToHost, c->st));
+    if (mueller) CK(cudaMemcpyAsync(mo, c->mueller, n_mo * sizeof(double), cudaMemcpyDeviceToHost, c->st));
     CK(cudaStreamSynchronize(c->st));
     for (int o = 0; o < no; o++) {
         if (cabs) cabs[o] = 0.5 * ca[(size_t)2 * o] + 0.5 * ca[(size_t)2 * o + 1];
         if (cext) cext[o] = 0.5 * ce[(size_t)2 * o] + 0.5 * ce[(size_t)2 * o + 1];
     }
-    if (mueller) std::memcpy(mueller, mo.data(), mo.size() * sizeof(double));
+    if (mueller) std::memcpy(mueller, mo, n_mo * sizeof(double));
     bi.n_rhs += nr;
     for (const RhsState &S : res.st) {
         bi.max_steps = std::max(bi.max_steps, S.steps);
