@@ -359,3 +359,28 @@ def test_occupancy_changes_between_calls(D, oracle):
         got.append(run(ctx, buf))
     for g, r in zip(got, (ref_a, ref_a, ref_b, ref_a, ref_a)):
         assert abs(g - r) <= 1e-6 * abs(r)
+
+
+def test_material_switched_off_with_polarisability(D, oracle):
+    """A material listed inactive (iListMV = 0) but given a nonzero polarisability: its
+    cells carry no dipoles, the far field skips them, and CabsCext still visits them (it
+    tests the polarisability, dda_func.cpp:1696) -- the fused far-field pass reads such
+    cells from global memory.  Results equal the FP64 oracle's."""
+    rng = np.random.default_rng(21)
+    n, kd = 16, 0.4
+    occ, _ = oracle.gen_ellipsoid(n, n, n, 0.8, 0.6)
+    occ[occ == 1] = rng.integers(1, 3, size=int((occ == 1).sum()))
+    alpha = np.array([0, 0.02 + 0.001j, 0.015 + 0.002j], np.complex64)
+    mv = np.array([0, 1, 0])
+    ksc = oracle.scattering_geometry(2, 19, 0.0, 10.0)[1]
+    einc = (1.0, 0.0, 0.0)
+    with D.Context(n, kd) as ctx:
+        # the residual crosses 1.5e-2 at step 3 (1.23e-2; 1.73e-2 at step 2)
+        r = ctx.dda_fft(occ, alpha, mv, kd, (0, 0, 1), einc, ksc, max_step=30, err_max=1.5e-2)
+    o = oracle.dda_fft(occ, alpha.astype(np.complex128), mv, kd, (0, 0, 1), einc,
+                       oracle.green_hat(n, n, n, kd), ksc.astype(np.float64), solver=0, tau=1.0,
+                       max_step=30, err_max=1.5e-2)
+    assert r["steps"] == 3
+    for q in ("cext", "cabs"):
+        assert abs(r[q] - o[q]) <= 1e-4 * abs(o[q]), (q, r[q], o[q])
+    assert rel(r["esc"], o["esc"]) < 1e-3
