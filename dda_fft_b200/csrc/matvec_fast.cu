@@ -314,7 +314,27 @@ __global__ void __launch_bounds__(Sp<NI>::RM * TL, k2_min_blocks(NI, Sp<NI>::RM 
             mbar_wait(&bar, 0);           // one more bounded wait for the copies in flight
             return;
         }
-        if (sub < R2) {
+        if constexpr (R1 == 2 * R2) {
+            // R1 = 2 R2 (edges 32, 128): every lane works -- lane (t2, hb) transforms half hb
+            // (hb = 1: the input times W_2NI^m) of the lines t2 + R2 r
+            const int t2 = sub % R2, hb = sub / R2;
+#pragma unroll 1
+            for (int c = 0; c < 3; c++) {
+                float2 v[R1];
+#pragma unroll
+                for (int r = 0; r < R1; r++) {
+                    v[r] = Bat(c, 0, t2 + R2 * r);
+                    if (hb) v[r] = cmul(v[r], __ldg(&hw[t2 + R2 * r]));
+                }
+                __syncthreads();   // half 0 of component c is read by both lane halves before it is rewritten
+                dft_reg<R1, false>(v);
+#pragma unroll
+                for (int k1 = 0; k1 < R1; k1++) {
+                    const float2 tk = k1 ? twid<false>(tw, t2 * k1) : make_float2(1.f, 0.f);
+                    Bat(c, hb, t2 + R2 * k1) = k1 ? cmul(v[k1], tk) : v[k1];
+                }
+            }
+        } else if (sub < R2) {
             auto step_a_smem = [&](int c) {
                 float2 v[R1], w[R1];
 #pragma unroll
@@ -498,6 +518,35 @@ __global__ void __launch_bounds__(Sp<NI>::RM * TL, k2_min_blocks(NI, Sp<NI>::RM 
 #pragma unroll
                 for (int k = 0; k < R1; k++)
                     base[c * cstr + k * plane] = cadd(e[k], cmulc(o[k], __ldg(&hw[k])));
+            }
+        }
+    } else if constexpr (R1 == 2 * R2) {
+        // every lane works: lane (k1p, hb) produces the outputs k2 = 2 m + hb of its lines,
+        // an R1/2-point inverse DFT of y[n] = (x[n] + (-1)^hb x[n + R1/2]) exp(2 pi i n hb / R1)
+        const int k1p = sub % R2, hb = sub / R2;
+        constexpr int H = R1 / 2;
+#pragma unroll 1
+        for (int c = 0; c < 3; c++) {
+            float2 e[H], o[H];
+#pragma unroll
+            for (int n = 0; n < H; n++) {
+                const float2 e0 = Bat(c, 0, R1 * k1p + n), e1 = Bat(c, 0, R1 * k1p + n + H);
+                const float2 o0 = Bat(c, 1, R1 * k1p + n), o1 = Bat(c, 1, R1 * k1p + n + H);
+                if (hb) {
+                    const float2 wn = cconj(w16(n * (16 / R1)));
+                    e[n] = n ? cmul(csub(e0, e1), wn) : csub(e0, e1);
+                    o[n] = n ? cmul(csub(o0, o1), wn) : csub(o0, o1);
+                } else {
+                    e[n] = cadd(e0, e1);
+                    o[n] = cadd(o0, o1);
+                }
+            }
+            dft_reg<H, true>(e);
+            dft_reg<H, true>(o);
+#pragma unroll
+            for (int m = 0; m < H; m++) {
+                const int i = k1p + R2 * (2 * m + hb);
+                base[c * cstr + i * plane] = cadd(e[m], cmulc(o[m], __ldg(&hw[i])));
             }
         }
     } else if (sub < R2) {
