@@ -229,6 +229,9 @@ __global__ void __launch_bounds__(NT) k1f(MatvecArgs a)
 // ------------------------------------------------------------------------------ K2
 // CTA (spectral row js, TL spectral columns): forward x (both halves), 3x3 product,
 // inverse x, in place.  Shared B[c][h][pos][t].
+// grid order of the x pass: right-hand side fastest where the Green octant outgrows L2
+__host__ __device__ constexpr bool k2_rhs_fastest(int NI) { return NI >= 128; }
+
 // at least this many CTAs per SM: about 128 registers a thread (80 for the 16-point lines)
 constexpr int k2_min_blocks(int NI, int threads)
 {
@@ -280,7 +283,13 @@ __global__ void __launch_bounds__(Sp<NI>::RM * TL, k2_min_blocks(NI, Sp<NI>::RM 
     using S = Sp<NI>;
     constexpr int R1 = S::R1, R2 = S::R2, RM = S::RM;
     extern __shared__ __align__(128) float2 B[];   // [6][NI][TL]
-    const int js = blockIdx.x, rhs = blockIdx.z;
+    // at edge 128 the right-hand side is the fastest grid index: CTAs that run together
+    // read the same Green-tensor columns, which then come from L2 (that octant, 103 MB,
+    // does not stay resident while a whole right-hand side streams through; 18.8 -> 18.4 ms
+    // per 42-RHS matvec).  Smaller octants stay in L2, and there the spectral row first
+    // is faster (64^3, 128 RHS: 2.42 vs 2.63 ms for this pass)
+    constexpr bool rhs_fast = k2_rhs_fastest(NI);
+    const int js = rhs_fast ? blockIdx.z : blockIdx.x, rhs = rhs_fast ? blockIdx.x : blockIdx.z;
     if (a.rhs_active && !a.rhs_active[rhs]) return;
     const int nj = a.L.nj, nl = a.L.nl;
     const int l0 = blockIdx.y * TL;
@@ -767,7 +776,9 @@ void launch_x_v(const MatvecArgs &a, cudaStream_t st)
     constexpr int TL = x_tile<NI>(V % 3);
     const int ncol = 2 * a.L.nl;
     const size_t smem = (size_t)6 * NI * TL * sizeof(float2);
-    k2f<NI, TL, (V >= 3)><<<dim3(2 * a.L.nj, ncol / TL, a.nrhs), Sp<NI>::RM * TL, smem, st>>>(a);
+    const dim3 grid = k2_rhs_fastest(NI) ? dim3(a.nrhs, ncol / TL, 2 * a.L.nj)
+                                         : dim3(2 * a.L.nj, ncol / TL, a.nrhs);
+    k2f<NI, TL, (V >= 3)><<<grid, Sp<NI>::RM * TL, smem, st>>>(a);
 }
 
 template <int NI>
