@@ -372,7 +372,7 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         threads = os.cpu_count() or 1
-        ns = args.cpu_samples or max(threads, 8)
+        ns = args.cpu_samples or max(24 * threads, 64)   # about 10 s of the host's threads
         v, kind, secs, used = cpu_reference(ns, threads)
         cpu = {"value": v, "unit": "orientation-solves/s", "cores": used, "kind": kind,
                "sample": f"{ns} orientation-solves of the same workload, {secs:.1f} s wall "
