@@ -679,23 +679,59 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(NT) k3f(MatvecArgs a
 
     // ---- sum of the two halves, epilogue, rows of this rank
     const float2 *R = cl.map_shared_rank(Q, hl ^ 1);
-    constexpr int HR = NJ / 2;
+    constexpr int HR = NJ / 2, EPK = (HR * NL + NT - 1) / NT;   // output cells per thread
     const size_t N = a.L.N;
     const size_t obase = (size_t)rhs * a.fstride + (size_t)c * N + (size_t)i * NJ * NL;
     const Epilogue &ep = a.ep;
-    for (int e = threadIdx.x; e < HR * NL; e += NT) {
+    // the solver form's materials: all of this thread's occupancy bytes are loaded before
+    // the first is used (one latency instead of one per cell), and with at most two
+    // materials the activity flags and polarisabilities come from registers
+    int mk[EPK];
+    bool act0 = false, act1 = false;
+    float2 al0 = czero(), al1 = czero();
+    const bool regtab = ep.mode == 1 && ep.nmat1 <= 2;
+    if (ep.mode == 1) {
+        const signed char *ob = ep.occ + (size_t)rhs * ep.occ_stride + ((size_t)i * NJ + (size_t)hl * HR) * NL;
+#pragma unroll
+        for (int k = 0; k < EPK; k++) {
+            const int e = threadIdx.x + NT * k;
+            mk[k] = e < HR * NL ? (int)ob[e] : 0;
+        }
+        if (regtab) {
+            act0 = ep.mv[0] != 0;
+            al0 = ep.alpha[(size_t)rhs * ep.nmat1];
+            if (ep.nmat1 > 1) {
+                act1 = ep.mv[1] != 0;
+                al1 = ep.alpha[(size_t)rhs * ep.nmat1 + 1];
+            }
+            if (ep.conj) {
+                al0 = cconj(al0);
+                al1 = cconj(al1);
+            }
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < EPK; k++) {
+        const int e = threadIdx.x + NT * k;
+        if (e >= HR * NL) break;
         const int jj = e / NL, l = e % NL, j = hl * HR + jj;
         const int q = j * PS + spos(l);
         const float2 conv = cadd(Q[q], R[q]);
         const size_t o = obase + (size_t)j * NL + l;
         float2 res = conv;
         if (ep.mode == 1) {
-            const int m = ep.occ[(size_t)rhs * ep.occ_stride + (size_t)i * NJ * NL + (size_t)j * NL + l];
-            if (!ep.mv[m]) {
+            const int m = mk[k];
+            const bool act = regtab ? ((m & 1) ? act1 : act0) : ep.mv[m] != 0;
+            if (!act) {
                 res = czero();
             } else {
-                float2 al = ep.alpha[(size_t)rhs * ep.nmat1 + m];
-                if (ep.conj) al = cconj(al);
+                float2 al;
+                if (regtab) {
+                    al = (m & 1) ? al1 : al0;
+                } else {
+                    al = ep.alpha[(size_t)rhs * ep.nmat1 + m];
+                    if (ep.conj) al = cconj(al);
+                }
                 res = csub(ep.sv != 0.f ? cscale(ep.v[o], ep.sv) : czero(), cmul(al, conv));
             }
         }
