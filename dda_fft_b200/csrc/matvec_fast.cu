@@ -108,9 +108,12 @@ __global__ void __launch_bounds__(NT) k1f(MatvecArgs a)
         const Epilogue &ep = a.ep;
         const float2 *tab = a.inc_tab + (size_t)rhs * (NJ + NL + ni);
         const float2 tx = tab[NJ + NL + i];
-        float2 tz[R1];
+        // this lane's z phases: held in registers up to 64-point rows; at 128 points they
+        // are re-read from the (L1-resident) table, which keeps the pass from spilling
+        constexpr bool tz_reg = NL <= 64;
+        float2 tz[tz_reg ? R1 : 1];
 #pragma unroll
-        for (int r = 0; r < R1; r++) tz[r] = sub < R2 ? tab[NJ + sub + R2 * r] : czero();
+        for (int r = 0; r < (tz_reg ? R1 : 1); r++) tz[r] = sub < R2 ? tab[NJ + sub + R2 * r] : czero();
         const double *E = a.einc + 6 * rhs;
         const float2 Ef = make_float2((float)E[2 * c], (float)E[2 * c + 1]);
         const signed char *ob = ep.occ + (size_t)rhs * ep.occ_stride + (size_t)i * NJ * NL;
@@ -143,7 +146,8 @@ __global__ void __launch_bounds__(NT) k1f(MatvecArgs a)
                     const int m = o[r];
                     const bool act = rt ? ((m & 1) ? mv1 : mv0) : ep.mv[m] != 0;
                     float2 val = czero();
-                    if (act) val = cmul(cmul(cmul(txy, tz[r]), rt ? ((m & 1) ? al1 : al0) : al[m]), Ef);
+                    const float2 tzr = tz_reg ? tz[tz_reg ? r : 0] : __ldg(&tab[NJ + sub + R2 * r]);
+                    if (act) val = cmul(cmul(cmul(txy, tzr), rt ? ((m & 1) ? al1 : al0) : al[m]), Ef);
                     if (hl == 0) pout[row * NL + sub + R2 * r] = val;
                     v[r] = hl ? cmul(val, __ldg(&hwl[sub + R2 * r])) : val;
                 }
