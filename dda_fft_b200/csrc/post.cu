@@ -22,10 +22,10 @@ namespace {
 // FF_DMAX directions, whose phase tables (one per axis) it builds once.  Thread (dg, w)
 // accumulates DPT directions x 3 components; the RW threads w of one direction group are
 // workers that split the plane's dipoles evenly:
-//   1. the plane's occupancy is staged in shared memory and each row's span -- first to
-//      last active column -- found with warp ballots; a prefix sum over the rows gives
-//      every span cell a position in one list (inactive cells inside a span stay in it,
-//      with zero dipoles);
+//   1. the plane's occupancy is staged in shared memory and each row's active cells
+//      counted with warp ballots; a prefix sum over the rows gives every active cell a
+//      position in one list (row by row, columns in order), so a porous target's holes
+//      cost nothing;
 //   2. the list is taken in chunks of ff_cap cells: the dipoles of a chunk are copied into
 //      shared memory (cp.async) with their row, column and material packed in one word,
 //      and worker w sums positions [w len / RW, (w + 1) len / RW) of the chunk:
@@ -102,8 +102,8 @@ __host__ __device__ inline FFLayout ff_layout(FFShape s, int nj, int nl, int nma
     L.P = ff_al16(L.eyx + (size_t)nj * s.D * f2);                       // [cap][nr][3]
     L.cc = ff_al16(L.P + pz * f2);                                      // CC: cy [nj], cz [nl], cx [8], weights
     L.idx = ff_al16(L.cc + (cc ? (size_t)(nj + nl + FF_PLANES) * f2 + (size_t)nr * nmat1 * sizeof(double) : 0));
-    L.ints = ff_al16(L.idx + (size_t)ff_cap(nr) * sizeof(unsigned));    // sb, len [nj], off [nj+1], mv, modes, misc
-    L.occ = ff_al16(L.ints + (size_t)(3 * nj + 1 + (1 + nr) * nmat1 + 4) * sizeof(int));
+    L.ints = ff_al16(L.idx + (size_t)ff_cap(nr) * sizeof(unsigned));    // count [nj], off [nj+1], mv, modes, misc
+    L.occ = ff_al16(L.ints + (size_t)(2 * nj + 1 + (1 + nr) * nmat1 + 4) * sizeof(int));
     L.total = ff_al16(L.occ + (size_t)nj * nl);
     return L;
 }
@@ -140,9 +140,8 @@ __global__ void __launch_bounds__(256) farfield_sum(PostArgs a, FFShape s)
     float2 *cz = cy + nj, *cx = cz + nl;
     double *cwt = reinterpret_cast<double *>(cx + FF_PLANES);  // CC: [NR][nmat1]
     unsigned *idx = reinterpret_cast<unsigned *>(smraw + L.idx);   // [CAP] l | row << 12 | m << 24
-    int *sb = reinterpret_cast<int *>(smraw + L.ints);         // [nj] first column of each row's span
-    int *ln = sb + nj;                                         // [nj] span length (0: no dipole)
-    int *off = ln + nj;                                        // [nj + 1] list position of each span
+    int *ln = reinterpret_cast<int *>(smraw + L.ints);         // [nj] active cells of each row
+    int *off = ln + nj;                                        // [nj + 1] list position of each row
     int *mvs = off + nj + 1;                                   // [nmat1]
     int *ccm = mvs + nmat1;                                    // [NR][nmat1]
     int *misc = ccm + NR * nmat1;                              // [0]: some material in mode 2
@@ -235,31 +234,24 @@ __global__ void __launch_bounds__(256) farfield_sum(PostArgs a, FFShape s)
         // row factors exp(i (kx x + ky y)) of this plane
         for (int e = threadIdx.x; e < nj * D; e += T) eyx[e] = cmul(ey[e], ex[ip * D + e % D]);
         __syncthreads();
-        // ---- spans: first and last active column of every row (warp per row)
+        // activity of a staged cell; nmat1 == 0: the activity list's length is not known
+        // (allocation-free entry point), so it is read from global memory at the
+        // occupancy's indices
+        auto active = [&](int m) {
+            return nmat1 ? ((unsigned)m < (unsigned)nmat1 && mvs[m] != 0) : (m >= 0 && a.mv[m] != 0);
+        };
+        // ---- active cells of every row (warp per row)
         for (int r = warp; r < nj; r += nwarps) {
-            int first = nl, last = -1;
+            int cnt = 0;
             for (int c0 = 0; c0 < nl; c0 += 32) {
                 const int l = c0 + lane;
-                bool act = false;
-                if (l < nl) {
-                    const int m = occs[r * nl + l];
-                    // nmat1 == 0: the activity list's length is not known (allocation-free
-                    // entry point), so it is read from global memory at the occupancy's indices
-                    act = nmat1 ? ((unsigned)m < (unsigned)nmat1 && mvs[m] != 0) : (m >= 0 && a.mv[m] != 0);
-                }
-                const unsigned bal = __ballot_sync(0xffffffffu, act);
-                if (bal) {
-                    if (first == nl) first = c0 + __ffs(bal) - 1;
-                    last = c0 + 31 - __clz(bal);
-                }
+                const bool act = l < nl && active(occs[r * nl + l]);
+                cnt += __popc(__ballot_sync(0xffffffffu, act));
             }
-            if (lane == 0) {
-                sb[r] = first;
-                ln[r] = last >= first ? last - first + 1 : 0;
-            }
+            if (lane == 0) ln[r] = cnt;
         }
         __syncthreads();
-        // ---- list positions of the spans (exclusive prefix sum, warp 0)
+        // ---- list positions of the rows (exclusive prefix sum, warp 0)
         if (warp == 0) {
             int carry = 0;
             for (int r0 = 0; r0 < nj; r0 += 32) {
@@ -282,31 +274,30 @@ __global__ void __launch_bounds__(256) farfield_sum(PostArgs a, FFShape s)
 #pragma unroll 1
         for (int v0 = 0; v0 < total; v0 += CAP) {
             const int v1 = v0 + CAP < total ? v0 + CAP : total, len = v1 - v0;
-            // copies: warp per row, the row's span cells that fall in [v0, v1)
+            // copies: warp per row, the row's active cells that fall in [v0, v1), each at
+            // its row's list position plus the active cells before it (ballot ranks)
             for (int r = warp; r < nj; r += nwarps) {
                 const int o = off[r], n = ln[r];
                 if (o + n <= v0 || o >= v1) continue;   // uniform over the warp
-                const int c0 = sb[r];
-                for (int x = lane; x < n; x += 32) {
-                    const int vv = o + x;
-                    if (vv < v0 || vv >= v1) continue;
-                    const int l = c0 + x, m = occs[r * nl + l];
-                    const bool act = nmat1 ? ((unsigned)m < (unsigned)nmat1 && mvs[m] != 0) : (m >= 0 && a.mv[m] != 0);
-                    float2 *dst = P + 3 * NR * (size_t)(vv - v0);
+                int base = o;
+                for (int c0 = 0; c0 < nl && base < v1; c0 += 32) {   // uniform over the warp
+                    const int l = c0 + lane;
+                    const int m = l < nl ? (int)occs[r * nl + l] : 0;
+                    const bool act = l < nl && active(m);
+                    const unsigned bal = __ballot_sync(0xffffffffu, act);
+                    const int vv = base + __popc(bal & ((1u << lane) - 1u));
+                    if (act && vv >= v0 && vv < v1) {
+                        float2 *dst = P + 3 * NR * (size_t)(vv - v0);
 #pragma unroll
-                    for (int k = 0; k < NR; k++) {
-                        if (act) {
+                        for (int k = 0; k < NR; k++) {
                             const float2 *src = pr + (size_t)k * 3 * N + q0 + (size_t)r * nl + l;
                             cp_async8(dst + 3 * k, src);
                             cp_async8(dst + 3 * k + 1, src + N);
                             cp_async8(dst + 3 * k + 2, src + 2 * N);
-                        } else {
-                            dst[3 * k] = czero();
-                            dst[3 * k + 1] = czero();
-                            dst[3 * k + 2] = czero();
                         }
+                        idx[vv - v0] = (unsigned)l | ((unsigned)r << 12) | ((unsigned)(m & 0xff) << 24);
                     }
-                    idx[vv - v0] = (unsigned)l | ((unsigned)r << 12) | ((unsigned)(m & 0xff) << 24);
+                    base += __popc(bal);
                 }
             }
             cp_async_commit();
