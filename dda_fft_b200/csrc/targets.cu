@@ -416,6 +416,45 @@ long long anthrax_count(int ni, int nj, int nl, float packing, float radius, flo
     return (long long)v + 1;
 }
 
+// CrossTwoWorms (particle.cpp:233-300) of a candidate c against n placed monomers, up to its
+// point tests, as one branch-free loop over distinct arrays that the compiler vectorises:
+// flag 1 -- crossing (parallel axes, or the "nearest points inside both segments" rule
+// with the reference's signs), 0 -- no crossing (line distance beyond r_a + r_b, or the
+// point tests cannot accept: the segments lie farther apart than r_a + r_b + 1 cell, so
+// each point test measures a distance beyond its threshold by more than a cell), 2 -- the
+// point tests decide.  Every lane performs cross_head's float operations in its order
+// (correctly rounded vector square root and division, no contraction), so the flags are
+// those of the scalar test.
+__attribute__((target_clones("avx2", "default"))) void cross_flags(const float *__restrict__ nx, const float *__restrict__ ny, const float *__restrict__ nz,
+                 const float *__restrict__ bx, const float *__restrict__ by, const float *__restrict__ bz,
+                 const float *__restrict__ r, const float *__restrict__ len, const double *__restrict__ mx,
+                 const double *__restrict__ my, const double *__restrict__ mz,
+                 const double *__restrict__ reach, unsigned char *__restrict__ flag, int n, const Worm &c,
+                 double cmx, double cmy, double cmz, double creach)
+{
+    const float cnx = c.n.x, cny = c.n.y, cnz = c.n.z, cbx = c.b.x, cby = c.b.y, cbz = c.b.z, cr = c.r,
+                cl = c.l;
+    for (int j = 0; j < n; j++) {
+        // v0 = a.n x b.n, v1 = b.b - a.b with a = the candidate
+        const float vx = cny * nz[j] - cnz * ny[j], vy = cnz * nx[j] - cnx * nz[j], vz = cnx * ny[j] - cny * nx[j];
+        const float r0 = std::sqrt(vx * vx + vy * vy + vz * vz);
+        const float ux = bx[j] - cbx, uy = by[j] - cby, uz = bz[j] - cbz;
+        const float dd = std::fabs((ux * vx + uy * vy + uz * vz) / r0);
+        // decisions as 0 / 1 integers combined without branches
+        const int par = r0 <= 1.e-20f;   // (double)r0 <= 1e-20 for every float r0
+        const int near = !(dd > cr + r[j]);
+        const float b1 = ux * cnx + uy * cny + uz * cnz, b2 = ux * nx[j] + uy * ny[j] + uz * nz[j];
+        const float a11 = 1.f, a12 = nx[j] * cnx + ny[j] * cny + nz[j] * cnz, a21 = -a12, a22 = -a11;
+        const float det = a11 * a22 - a12 * a21;
+        const float q0 = (b1 * a22 - b2 * a12) / det, q1 = (b2 * a11 - b1 * a21) / det;
+        const int inside = (q0 >= 0.f) & (q0 <= cl) & (q1 >= 0.f) & (q1 <= len[j]);
+        const double dx = cmx - mx[j], dy = cmy - my[j], dz = cmz - mz[j], rr = creach + reach[j];
+        const int reachable = dx * dx + dy * dy + dz * dz <= rr * rr;
+        const int one = par | (near & inside), two = (par ^ 1) & near & (inside ^ 1) & reachable;
+        flag[j] = (unsigned char)(one | (two << 1));
+    }
+}
+
 int anthrax_place(unsigned long long *state, int ni, float radius, float length, int count,
                   float *cyl13, long long max_tries)
 {
@@ -424,7 +463,7 @@ int anthrax_place(unsigned long long *state, int ni, float radius, float length,
     std::vector<Worm> w;
     w.reserve((size_t)count);
     // placed monomers' axes, starts, radii, midpoints and reach (half length + radius)
-    std::vector<float> nx_, ny_, nz_, bx_, by_, bz_, r_;
+    std::vector<float> nx_, ny_, nz_, bx_, by_, bz_, r_, l_;
     std::vector<double> mx_, my_, mz_, reach_;
     std::vector<unsigned char> cand_;
     unsigned long long s = *state;
@@ -446,40 +485,23 @@ int anthrax_place(unsigned long long *state, int ni, float radius, float length,
             c = make_worm(r1, th1, ph1, r2, th2, ph2, length, radius, R2);
         }
         // The reference tests the candidate against every placed monomer with
-        // CrossTwoWorms and rejects it on the first crossing; only that yes / no matters.
-        // Here, chunk by chunk of placed monomers: (1) the parallel-axes rule and the
-        // line-distance exit of the test, with the same float operations, for the whole
-        // chunk (a branch-free loop); (2) for the pairs left, the rest of the test up to the
-        // "nearest points inside both segments" rule (cross_head); (3) the point tests only
-        // for pairs whose segments lie within r_a + r_b + 1 cell -- for every other pair
-        // each point test measures a distance beyond its threshold by more than a cell,
-        // far above float rounding, so it returns 0 and the pair's answer is cross_head's.
+        // CrossTwoWorms and rejects it on the first crossing; only that yes / no matters,
+        // so the pairs are decided chunk by chunk of placed monomers: cross_flags for the
+        // whole chunk, then the point tests only for the pairs it leaves to them.
         if (!w.empty()) {
             const size_t nw = w.size();
-            const float cnx = c.n.x, cny = c.n.y, cnz = c.n.z, cbx = c.b.x, cby = c.b.y, cbz = c.b.z;
             const double mx = 0.5 * ((double)c.b.x + c.e.x), my = 0.5 * ((double)c.b.y + c.e.y),
                          mz = 0.5 * ((double)c.b.z + c.e.z), reach = 0.5 * (double)c.l + c.r + 1.0;
             l = 0;
             for (size_t j0 = 0; j0 < nw && !l; j0 += 256) {
                 const size_t j1 = std::min(nw, j0 + 256);
-                for (size_t j = j0; j < j1; j++) {
-                    const float vx = cny * nz_[j] - cnz * ny_[j], vy = cnz * nx_[j] - cnx * nz_[j],
-                                vz = cnx * ny_[j] - cny * nx_[j];
-                    const float r0 = std::sqrt(vx * vx + vy * vy + vz * vz);
-                    const float ux = bx_[j] - cbx, uy = by_[j] - cby, uz = bz_[j] - cbz;
-                    const float dd = std::fabs((ux * vx + uy * vy + uz * vz) / r0);
-                    cand_[j] = ((double)r0 <= 1.e-20) | !(dd > c.r + r_[j]);
-                }
+                cross_flags(nx_.data() + j0, ny_.data() + j0, nz_.data() + j0, bx_.data() + j0, by_.data() + j0,
+                            bz_.data() + j0, r_.data() + j0, l_.data() + j0, mx_.data() + j0, my_.data() + j0,
+                            mz_.data() + j0, reach_.data() + j0, cand_.data() + j0, (int)(j1 - j0), c, mx, my,
+                            mz, reach);
                 for (size_t j = j0; j < j1 && !l; j++) {
-                    if (!cand_[j]) continue;
-                    const double dx = mx - mx_[j], dy = my - my_[j], dz = mz - mz_[j],
-                                 rr = reach + reach_[j];
-                    if (dx * dx + dy * dy + dz * dz <= rr * rr) {
-                        l = cross_two_worms(c, w[j]);
-                    } else {
-                        float q0, q1;
-                        l = cross_head(c, w[j], q0, q1) == 1;
-                    }
+                    if (cand_[j] == 1) l = 1;
+                    else if (cand_[j] == 2) l = cross_two_worms(c, w[j]);
                 }
             }
         }
@@ -492,6 +514,7 @@ int anthrax_place(unsigned long long *state, int ni, float radius, float length,
             by_.push_back(c.b.y);
             bz_.push_back(c.b.z);
             r_.push_back(c.r);
+            l_.push_back(c.l);
             mx_.push_back(0.5 * ((double)c.b.x + c.e.x));
             my_.push_back(0.5 * ((double)c.b.y + c.e.y));
             mz_.push_back(0.5 * ((double)c.b.z + c.e.z));
