@@ -466,6 +466,15 @@ int anthrax_place(unsigned long long *state, int ni, float radius, float length,
     std::vector<float> nx_, ny_, nz_, bx_, by_, bz_, r_, l_;
     std::vector<double> mx_, my_, mz_, reach_;
     std::vector<unsigned char> cand_;
+    // placed monomers bucketed by midpoint on a grid whose cell G exceeds every reach sum,
+    // so that a pair within reach of the point tests lies in neighbouring buckets
+    const double G = (double)length + 2.0 * (double)radius + 2.0, org = -(double)R - G;
+    const int nb = (int)std::ceil((2.0 * (double)R + 2.0 * G) / G) + 1;
+    std::vector<std::vector<int>> bucket((size_t)nb * nb * nb);
+    auto bidx = [&](double x) {
+        const int b = (int)std::floor((x - org) / G);
+        return b < 0 ? 0 : b >= nb ? nb - 1 : b;
+    };
     unsigned long long s = *state;
     long long tries = 0;
     int l = 0;
@@ -485,14 +494,29 @@ int anthrax_place(unsigned long long *state, int ni, float radius, float length,
             c = make_worm(r1, th1, ph1, r2, th2, ph2, length, radius, R2);
         }
         // The reference tests the candidate against every placed monomer with
-        // CrossTwoWorms and rejects it on the first crossing; only that yes / no matters,
-        // so the pairs are decided chunk by chunk of placed monomers: cross_flags for the
-        // whole chunk, then the point tests only for the pairs it leaves to them.
-        if (!w.empty()) {
+        // CrossTwoWorms and rejects it on the first crossing; only that yes / no matters.
+        // The monomers in the candidate's and the neighbouring buckets are tested first
+        // (most rejections come from them); if none crosses, all pairs are decided chunk by
+        // chunk of placed monomers: cross_flags for the whole chunk, then the point tests
+        // only for the pairs it leaves to them.
+        const double mx = 0.5 * ((double)c.b.x + c.e.x), my = 0.5 * ((double)c.b.y + c.e.y),
+                     mz = 0.5 * ((double)c.b.z + c.e.z);
+        const int bi = bidx(mx), bj = bidx(my), bk = bidx(mz);
+        l = 0;
+        for (int di = -1; di <= 1 && !l; di++)
+            for (int dj = -1; dj <= 1 && !l; dj++)
+                for (int dk = -1; dk <= 1 && !l; dk++) {
+                    const int a = bi + di, b = bj + dj, q = bk + dk;
+                    if (a < 0 || b < 0 || q < 0 || a >= nb || b >= nb || q >= nb) continue;
+                    for (const int j : bucket[((size_t)a * nb + b) * nb + q])
+                        if (cross_two_worms(c, w[(size_t)j])) {
+                            l = 1;
+                            break;
+                        }
+                }
+        if (!l && !w.empty()) {
             const size_t nw = w.size();
-            const double mx = 0.5 * ((double)c.b.x + c.e.x), my = 0.5 * ((double)c.b.y + c.e.y),
-                         mz = 0.5 * ((double)c.b.z + c.e.z), reach = 0.5 * (double)c.l + c.r + 1.0;
-            l = 0;
+            const double reach = 0.5 * (double)c.l + c.r + 1.0;
             for (size_t j0 = 0; j0 < nw && !l; j0 += 256) {
                 const size_t j1 = std::min(nw, j0 + 256);
                 cross_flags(nx_.data() + j0, ny_.data() + j0, nz_.data() + j0, bx_.data() + j0, by_.data() + j0,
@@ -520,6 +544,7 @@ int anthrax_place(unsigned long long *state, int ni, float radius, float length,
             mz_.push_back(0.5 * ((double)c.b.z + c.e.z));
             reach_.push_back(0.5 * (double)c.l + c.r);
             cand_.push_back(0);
+            bucket[((size_t)bidx(mx) * nb + bidx(my)) * nb + bidx(mz)].push_back((int)w.size() - 1);
         }
     }
     *state = s;
