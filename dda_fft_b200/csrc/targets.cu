@@ -503,17 +503,17 @@ int anthrax_place(unsigned long long *state, int ni, float radius, float length,
                      mz = 0.5 * ((double)c.b.z + c.e.z);
         const int bi = bidx(mx), bj = bidx(my), bk = bidx(mz);
         l = 0;
-        for (int di = -1; di <= 1 && !l; di++)
-            for (int dj = -1; dj <= 1 && !l; dj++)
-                for (int dk = -1; dk <= 1 && !l; dk++) {
-                    const int a = bi + di, b = bj + dj, q = bk + dk;
-                    if (a < 0 || b < 0 || q < 0 || a >= nb || b >= nb || q >= nb) continue;
-                    for (const int j : bucket[((size_t)a * nb + b) * nb + q])
-                        if (cross_two_worms(c, w[(size_t)j])) {
-                            l = 1;
-                            break;
-                        }
+        // the candidate's own bucket first (s = 0), then the 26 around it
+        for (int s = 0; s < 27 && !l; s++) {
+            const int o = s == 0 ? 13 : (s <= 13 ? s - 1 : s);   // offsets 0..26, 13 = (0, 0, 0)
+            const int a = bi + o / 9 - 1, b = bj + (o / 3) % 3 - 1, q = bk + o % 3 - 1;
+            if (a < 0 || b < 0 || q < 0 || a >= nb || b >= nb || q >= nb) continue;
+            for (const int j : bucket[((size_t)a * nb + b) * nb + q])
+                if (cross_two_worms(c, w[(size_t)j])) {
+                    l = 1;
+                    break;
                 }
+        }
         if (!l && !w.empty()) {
             const size_t nw = w.size();
             const double reach = 0.5 * (double)c.l + c.r + 1.0;
