@@ -159,3 +159,23 @@ def test_random_ellipsoid_matches_reference(fx, name):
     occ, count, _ = RandomEllipsoid(state=seed).generate(grid, ba, ca, sps)
     np.testing.assert_array_equal(occ, fx[f"{name}_occ"])
     assert count == int(fx[f"{name}_count_next"][0])
+
+
+@pytest.mark.parametrize("n,r,lr,seed", [(32, 3.0, 0.0, 5), (32, 2.0, 1.5, 17), (64, 3.0, 0.0, 23),
+                                         (64, 2.5, 2.0, 41), (32, 1.5, 3.0, 99)])
+def test_placement_matches_live_reference(n, r, lr, seed):
+    """The placement (grid-bucketed and vectorised crossing test) against the reference's
+    own iGenerateAnthrax compiled from its sources, on seeds and shapes beyond the fixtures:
+    the same monomers bit for bit and the same next draw."""
+    import sys
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as P
+    if not os.path.exists(P.REF_SO):
+        pytest.skip("reference library not built")
+    from dda_fft_b200 import Agglomerate
+    count = Agglomerate.count((n, n, n), 0.25, r, lr)
+    _, _, cyl, nxt = P.RefLib().gen_anthrax(seed, n, r, r * lr, count)
+    a = Agglomerate(state=seed)
+    mon = a.place(n, r, r * lr, count)
+    np.testing.assert_array_equal(mon, cyl.astype(np.float32))
+    assert next_draw(a.state) == nxt
