@@ -76,6 +76,7 @@ def lib():
         L = C.CDLL(path)
         L.ddagpu_version.restype = C.c_char_p
         L.ddagpu_last_error.restype = C.c_char_p
+        L.ddagpu_binary_version.argtypes = [_i, C.POINTER(_i)]
         L.ddagpu_create.argtypes = [C.POINTER(_p), _i, _i, _i, _i, _d, _i]
         L.ddagpu_destroy.argtypes = [_p]
         L.ddagpu_set_green.argtypes = [_p, _p]
@@ -113,7 +114,7 @@ def lib():
         L.ddagpu_get_tiling.argtypes = [_p, C.POINTER(_i), C.POINTER(_i)]
         L.ddagpu_autotune.argtypes = [_p, _i]
         L.ddagpu_set_kernels.argtypes = [_p, _i]
-        L.ddagpu_farfield_noalloc.argtypes = [_i, _i, _i, _i, _f, _p, _p, _p, _i, _p, _p, _p]
+        L.ddagpu_farfield_noalloc.argtypes = [_i, _i, _i, _i, _f, _p, _p, _i, _p, _i, _p, _p, _p]
         L.ddagpu_get_kernels.argtypes = [_p]
         L.ddagpu_set_fast_variant.argtypes = [_p, _i, _i]
         L.ddagpu_get_fast_variant.argtypes = [_p, C.POINTER(_i), C.POINTER(_i)]

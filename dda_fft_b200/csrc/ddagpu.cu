@@ -789,6 +789,18 @@ int rounding_ref(float r0)
 extern "C" {
 
 const char *ddagpu_version(void) { return "ddagpu 1.0 (sm_100a)"; }
+
+int ddagpu_binary_version(int device, int *version)
+{
+    if (!version) return fail(DDAGPU_EINVAL, "null argument");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return fail(DDAGPU_ENOTBUILT, "no CUDA device");
+    if (device < 0 || device >= ndev) return fail(DDAGPU_EINVAL, "bad device index");
+    DevGuard dg(device);
+    CK(kernel_binary_version(version));
+    return DDAGPU_OK;
+}
 const char *ddagpu_last_error(void) { return g_err.c_str(); }
 
 int ddagpu_num_angles(float theta_min, float theta_max, float theta_step)
@@ -952,7 +964,7 @@ int ddagpu_set_kernels(ddagpu_ctx *c, int fast)
 {
     if (!c) return fail(DDAGPU_EINVAL, "null context");
     if (fast && !matvec_fast_supported(c->L))
-        return fail(DDAGPU_EINVAL, "compile-time-sized passes need edges in {16, 32, 64}");
+        return fail(DDAGPU_EINVAL, "compile-time-sized passes need edges in {16, 32, 64, 128}");
     c->fast = fast ? 1 : 0;
     return DDAGPU_OK;
 }
@@ -1689,11 +1701,13 @@ int ddagpu_mueller(ddagpu_ctx *c, const float *kinc, const float *einc0, const f
 }
 
 int ddagpu_farfield_noalloc(int device, int i_max, int j_max, int l_max, float d0,
-                            const signed char *occ_dev, const int *mv_dev, const void *p_dev,
-                            int ndir, const float *ksc_dev, float *esc_dev, void *stream)
+                            const signed char *occ_dev, const int *mv_dev, int n_mat,
+                            const void *p_dev, int ndir, const float *ksc_dev, float *esc_dev,
+                            void *stream)
 {
     if (!pow2_in(i_max) || !pow2_in(j_max) || !pow2_in(l_max))
         return fail(DDAGPU_EINVAL, "lattice edges must be powers of two in [2, 128]");
+    if (n_mat < 0 || n_mat + 1 > kMaxMaterials + 1) return fail(DDAGPU_EINVAL, "n_mat outside 0..255");
     if (ndir < 0 || ndir > farfield_noalloc_max_dirs())
         return fail(DDAGPU_EINVAL, "ndir exceeds the allocation-free maximum of " +
                                        std::to_string(farfield_noalloc_max_dirs()) + " directions");
@@ -1711,6 +1725,7 @@ int ddagpu_farfield_noalloc(int device, int i_max, int j_max, int l_max, float d
     a.nl = l_max;
     a.occ = occ_dev;
     a.mv = mv_dev;
+    a.nmat1 = n_mat + 1;   // cells whose material index exceeds n_mat count as empty
     a.p = (const float2 *)p_dev;
     a.d0 = d0;
     a.ndir = ndir;

@@ -80,7 +80,14 @@ struct MatvecArgs {
     float2 *inc_out;        // [nrhs][3][N]
 };
 
+// Dynamic shared memory limit of a kernel on the current device, raised to at least
+// `bytes` and never lowered: the limit is a per-process property of the kernel, shared by
+// every context, so a context on a smaller lattice must not shrink what a larger one set
+// (matvec.cu).
+cudaError_t raise_smem_limit(const void *kernel, int bytes);
+
 // kernels (matvec.cu)
+cudaError_t kernel_binary_version(int *version);   // of the loaded module, e.g. 100
 cudaError_t launch_matvec(const MatvecArgs &a, cudaStream_t st);
 size_t matvec_smem_yz(const Lat &L, int rows_g);
 size_t matvec_smem_x(const Lat &L, int tile_x);

@@ -15,6 +15,10 @@
 // in that split order: index s = h * n + k holds frequency 2k + h.
 #include <cooperative_groups.h>
 
+#include <map>
+#include <mutex>
+#include <utility>
+
 #include "common.cuh"
 #include "internal.h"
 
@@ -205,17 +209,36 @@ size_t matvec_smem_yz(const Lat &L, int rows_g)
 
 size_t matvec_smem_x(const Lat &L, int tile_x) { return (size_t)6 * tile_x * L.ni * sizeof(float2); }
 
+cudaError_t raise_smem_limit(const void *kernel, int bytes)
+{
+    static std::mutex mu;
+    static std::map<std::pair<int, const void *>, int> set;   // (device, kernel) -> limit
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lk(mu);
+    int &cur = set[{dev, kernel}];
+    if (bytes <= cur) return cudaSuccess;
+    e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess) cur = bytes;
+    return e;
+}
+
+cudaError_t kernel_binary_version(int *version)
+{
+    cudaFuncAttributes fa{};
+    const cudaError_t e = cudaFuncGetAttributes(&fa, (const void *)k2_x_product);
+    if (e == cudaSuccess) *version = fa.binaryVersion;
+    return e;
+}
+
 cudaError_t matvec_prepare(const Lat &L, int tile_x, int rows_g)
 {
     cudaError_t e;
     const int syz = (int)matvec_smem_yz(L, rows_g), sx = (int)matvec_smem_x(L, tile_x);
-    if ((e = cudaFuncSetAttribute(k1_forward_yz, cudaFuncAttributeMaxDynamicSharedMemorySize, syz)))
-        return e;
-    if ((e = cudaFuncSetAttribute(k3_inverse_zy, cudaFuncAttributeMaxDynamicSharedMemorySize, syz)))
-        return e;
-    if ((e = cudaFuncSetAttribute(k2_x_product, cudaFuncAttributeMaxDynamicSharedMemorySize, sx)))
-        return e;
-    return cudaSuccess;
+    if ((e = raise_smem_limit((const void *)k1_forward_yz, syz))) return e;
+    if ((e = raise_smem_limit((const void *)k3_inverse_zy, syz))) return e;
+    return raise_smem_limit((const void *)k2_x_product, sx);
 }
 
 cudaError_t launch_matvec(const MatvecArgs &a, cudaStream_t st)

@@ -613,11 +613,11 @@ size_t farfield_smem(int nj, int nl)
 
 cudaError_t post_prepare(int nj, int nl)
 {
+    // raised only: a context or call on a smaller lattice keeps what a larger one needs
     const int bytes = (int)farfield_smem(nj, nl);
-    const cudaFuncAttribute at = cudaFuncAttributeMaxDynamicSharedMemorySize;
-    cudaError_t e = cudaFuncSetAttribute(farfield_sum<true, 1, 4>, at, bytes);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(farfield_sum<true, 2, 2>, at, bytes);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(farfield_sum<false, 1, 4>, at, bytes);
+    cudaError_t e = raise_smem_limit((const void *)farfield_sum<true, 1, 4>, bytes);
+    if (e == cudaSuccess) e = raise_smem_limit((const void *)farfield_sum<true, 2, 2>, bytes);
+    if (e == cudaSuccess) e = raise_smem_limit((const void *)farfield_sum<false, 1, 4>, bytes);
     return e;
 }
 

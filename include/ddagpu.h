@@ -51,6 +51,10 @@ typedef struct {
 
 const char *ddagpu_version(void);
 const char *ddagpu_last_error(void);
+/* Architecture the library's kernels were compiled for, as the CUDA runtime reports it for
+ * the module loaded on `device` (major * 10 + minor: 100 for sm_100a).  No counterpart in
+ * the reference. */
+int ddagpu_binary_version(int device, int *version);
 
 /* Creates a context for one lattice on one CUDA device, builds the Green tensor FFT from kd
  * on the device, and reserves work space for up to max_rhs right-hand sides solved
@@ -280,7 +284,8 @@ int ddagpu_fixed_rotation(double psi, double iota, double kappa, double *rot);
  * (code under CUDA graph capture, real-time loops that forbid allocator calls, hosts that
  * hand the library only pre-allocated buffers).  No counterpart in the reference.  Needs no
  * context: the caller passes device pointers to the occupancy occ_dev [i][j][l], the
- * material activity flags mv_dev (one int per material index found in occ_dev), the
+ * material activity flags mv_dev (n_mat + 1 ints, index 0 = empty; cells whose material
+ * index exceeds n_mat count as empty and mv_dev is never read past n_mat), the
  * dipoles p_dev ([3][i][j][l] complex float, structure of arrays), the directions
  * ksc_dev [ndir][3] float, and receives esc_dev [ndir][6] float (cvector per direction),
  * all on `stream` (cudaStream_t; NULL = legacy default stream).  At most 8192 directions
@@ -289,8 +294,9 @@ int ddagpu_fixed_rotation(double psi, double iota, double kappa, double *rot);
  * device looks up that array's address, so make it before any stream capture.  Calls
  * that overlap on the GPU share the array and race: serialise them (one stream). */
 int ddagpu_farfield_noalloc(int device, int i_max, int j_max, int l_max, float d0,
-                            const signed char *occ_dev, const int *mv_dev, const void *p_dev,
-                            int ndir, const float *ksc_dev, float *esc_dev, void *stream);
+                            const signed char *occ_dev, const int *mv_dev, int n_mat,
+                            const void *p_dev, int ndir, const float *ksc_dev, float *esc_dev,
+                            void *stream);
 
 /* ---------------------------------------------------------------- device-resident form
  * G*p for nrhs fields already in device memory ([nrhs][3][i][j][l] complex float, SoA),
@@ -307,7 +313,7 @@ long long ddagpu_kernel_launches(ddagpu_ctx *ctx);
 int ddagpu_set_tiling(ddagpu_ctx *ctx, int tile_x, int rows_g);
 int ddagpu_get_tiling(ddagpu_ctx *ctx, int *tile_x, int *rows_g);
 /* Kernel family of the matvec: 1 = passes specialised at compile time for lattice edges in
- * {16, 32, 64} (the default where they apply), 0 = the generic passes (any edge 2..128). */
+ * {16, 32, 64, 128} (the default where they apply), 0 = the generic passes (any edge 2..128). */
 int ddagpu_set_kernels(ddagpu_ctx *ctx, int fast);
 int ddagpu_get_kernels(ddagpu_ctx *ctx);
 int ddagpu_autotune(ddagpu_ctx *ctx, int nrhs);

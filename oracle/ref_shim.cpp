@@ -110,38 +110,32 @@ struct green_holder {
     }
 };
 
-/* Capture what a reference call prints on stdout (the per-step discrepancies). */
+/* Capture what a reference call prints on stdout (the per-step discrepancies) in an
+ * anonymous temporary file. */
 struct stdout_capture {
     int saved = -1;
-    char path[64];
-    bool on = false;
+    FILE *tmp = nullptr;
     void begin()
     {
         std::fflush(stdout);
-        std::snprintf(path, sizeof path, "/tmp/ddaref_cap_%d_XXXXXX", (int)getpid());
-        int fd = mkstemp(path);
-        if (fd < 0) return;
+        tmp = std::tmpfile();
+        if (!tmp) return;
         saved = dup(1);
-        dup2(fd, 1);
-        close(fd);
-        on = true;
+        dup2(fileno(tmp), 1);
     }
     std::string end()
     {
-        if (!on) return std::string();
+        if (!tmp) return std::string();
         std::fflush(stdout);
         dup2(saved, 1);
         close(saved);
         std::string s;
-        FILE *f = std::fopen(path, "rb");
-        if (f) {
-            char buf[4096];
-            size_t k;
-            while ((k = std::fread(buf, 1, sizeof buf, f)) > 0) s.append(buf, k);
-            std::fclose(f);
-        }
-        unlink(path);
-        on = false;
+        std::rewind(tmp);
+        char buf[4096];
+        size_t k;
+        while ((k = std::fread(buf, 1, sizeof buf, tmp)) > 0) s.append(buf, k);
+        std::fclose(tmp);
+        tmp = nullptr;
         return s;
     }
 };
