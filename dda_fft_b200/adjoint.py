@@ -163,8 +163,7 @@ class GPUBackend:
     def solve(self, occ, table, rhs_dipoles):
         mv = np.array([0] + [1] * (len(table) - 1), np.int32)
         x, info = self.ctx.solve_linear(occ, table, mv, self.P.field(rhs_dipoles), solver=self.solver,
-                                        err_max=self.err_max, max_step=60, refine=True,
-                                        inner_rel=0.05, inner_max_step=400)
+                                        err_max=self.err_max, max_step=60, refine=True)
         self.matvecs += info["matvecs"]
         return x[tuple(self.P.idx.T)].astype(complex)
 

@@ -84,6 +84,10 @@ def lib():
         L.ddagpu_dda_fft.argtypes = [_p, _i, _i, _f, _i, _i, _i, _p, _p, _i, _p, _i, _f, _f, _p,
                                      _p, _i, _i, _i, _p, _p, _p, _p, C.POINTER(SolveInfo), _p]
         L.ddagpu_farfield.argtypes = [_p, _p, _i, _p, _f, _p, _i, _p, _p]
+        L.ddagpu_solve_fp64.argtypes = [_p, _i, _d, _p, _p, _i, _p, _d, _p, _p, _p, _p, _i, _d,
+                                        _i, _p, _p, C.POINTER(_d), C.POINTER(_d), _p,
+                                        C.POINTER(SolveInfo), _p]
+        L.ddagpu_release_fp64.argtypes = [_p]
         L.ddagpu_solve_linear.argtypes = [_p, _i, _f, _p, _p, _i, _p, _p, _d, _i, _i, _d, _i, _p,
                                           C.POINTER(RefineInfo)]
         L.ddagpu_dda_fft_refined.argtypes = [_p, _i, _f, _p, _p, _i, _p, _f, _p, _p, _d, _i, _d,
@@ -408,8 +412,12 @@ class Context:
         return out
 
     def dda_fft_refined(self, occ, alpha, listmv, d0, kinc, einc, ksc, solver=2, tau=0.0,
-                        err_max=1e-5, max_outer=20, inner_rel=0.05, inner_max_step=200):
-        """FP64-residual iterative refinement around the chosen solver."""
+                        err_max=1e-5, max_outer=20, inner_rel=0.05, inner_max_step=None):
+        """FP64-residual iterative refinement around the chosen solver.  CG (solver 0) is
+        never restarted: inner_max_step (default 100000) only bounds the iterations between
+        true residuals; the other solvers restart every outer step (default 200 steps)."""
+        if inner_max_step is None:
+            inner_max_step = 100000 if solver == 0 else 200
         o = np.ascontiguousarray(occ, np.int8)
         a = _cvec(np.asarray(alpha, np.complex64).reshape(-1, 1)).ravel()
         mv = np.ascontiguousarray(listmv, np.int32)
@@ -430,8 +438,11 @@ class Context:
                     inner_steps=info.inner_steps, matvecs=info.matvecs, err=info.err, history=hist)
 
     def solve_linear(self, occ, alpha, listmv, rhs, solver=0, tau=0.0, err_max=1e-8,
-                     max_step=40, refine=True, inner_rel=0.05, inner_max_step=300):
-        """x with (I - D_alpha G) x = rhs; rhs complex (ni, nj, nl, 3)."""
+                     max_step=40, refine=True, inner_rel=0.05, inner_max_step=None):
+        """x with (I - D_alpha G) x = rhs; rhs complex (ni, nj, nl, 3).  inner_max_step as
+        for dda_fft_refined."""
+        if inner_max_step is None:
+            inner_max_step = 100000 if solver == 0 else 300
         o = np.ascontiguousarray(occ, np.int8)
         a = _cvec(np.asarray(alpha, np.complex64).reshape(-1, 1)).ravel()
         mv = np.ascontiguousarray(listmv, np.int32)
@@ -445,6 +456,40 @@ class Context:
         return x.view(np.complex64).reshape(np.shape(rhs)), dict(
             outer=info.outer, inner_steps=info.inner_steps, matvecs=info.matvecs, err=info.err,
             history=hist)
+
+    def solve_fp64(self, occ, alpha, listmv, d0, kinc, einc, ksc=None, solver=0, tau=0.0,
+                   max_step=100, err_max=1e-3, rhs=None, x0=None, want_p=False, trace=True):
+        """DDA_FFT in FP64 on the GPU (ddagpu_solve_fp64); returns dict(esc complex128
+        (ndir, 3), cabs, cext, steps, step_min, matvecs, err, err_min, trace, p)."""
+        o = np.ascontiguousarray(occ, np.int8)
+        a = np.ascontiguousarray(np.asarray(alpha, np.complex128)).view(np.float64)
+        mv = np.ascontiguousarray(listmv, np.int32)
+        ks = np.zeros((0, 3)) if ksc is None else np.ascontiguousarray(np.asarray(ksc, np.float64).reshape(-1, 3))
+        nd = ks.shape[0]
+        esc = np.zeros((max(nd, 1), 3), np.complex128)
+        k = np.ascontiguousarray(kinc, np.float64)
+        e = np.ascontiguousarray(np.asarray(einc, np.complex128)).view(np.float64)
+        b = None if rhs is None else np.ascontiguousarray(np.asarray(rhs, np.complex128))
+        x = None if x0 is None else np.ascontiguousarray(np.asarray(x0, np.complex128))
+        p = np.zeros(tuple(self.grid) + (3,), np.complex128) if want_p else None
+        tr = np.zeros(max_step + 1) if trace else None
+        ca, ce = C.c_double(), C.c_double()
+        info = SolveInfo()
+        _check(lib().ddagpu_solve_fp64(self._h, solver, tau, _ptr(a), _ptr(mv), len(mv) - 1, _ptr(o),
+                                       d0, _ptr(k), _ptr(e), _ptr(b) if b is not None else None,
+                                       _ptr(x) if x is not None else None, max_step, err_max, nd,
+                                       _ptr(ks), _ptr(esc), C.byref(ca), C.byref(ce),
+                                       _ptr(p) if p is not None else None, C.byref(info),
+                                       _ptr(tr) if trace else None))
+        out = dict(esc=esc[:nd], cabs=ca.value, cext=ce.value, steps=info.steps,
+                   step_min=info.step_min if info.rolled_back else -1, matvecs=info.matvecs,
+                   err=info.err, err_min=info.err_min, rolled_back=info.rolled_back, p=p)
+        if trace:
+            out["trace"] = tr[: info.steps + 1]
+        return out
+
+    def release_fp64(self):
+        _check(lib().ddagpu_release_fp64(self._h))
 
     def farfield(self, occ, listmv, d0, p, ksc) -> np.ndarray:
         o = np.ascontiguousarray(occ, np.int8)

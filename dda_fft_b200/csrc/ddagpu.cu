@@ -22,6 +22,7 @@
 #include "internal.h"
 #include "post.h"
 #include "solver.h"
+#include "fp64.h"
 
 using namespace ddagpu;
 
@@ -138,6 +139,8 @@ struct ddagpu_ctx {
     size_t worm_bytes = 0;
     int wait_selftest = 0;           // 1: the x pass's wait waits for a phase nothing completes
     long long post_key = 0;          // shape of the post-processing recorded with a solve
+    Fp64Buffers *f64 = nullptr;  // FP64 solve buffers (ddagpu_solve_fp64), built on first use
+    MixedCgBuffers *mcg = nullptr;   // FP64 fields of the mixed-precision CG refinement
     long long g_per_iter = 0;    // kernels in one recorded iteration
     long long graph_runs = 0;    // graph launches by this context
     std::mutex mu;
@@ -917,6 +920,8 @@ int ddagpu_destroy(ddagpu_ctx *c)
     for (void *q : ptrs)
         if (q) cudaFree(q);
     if (c->pin) cudaFreeHost(c->pin);
+    delete c->f64;
+    delete c->mcg;
     if (c->st) cudaStreamDestroy(c->st);
     delete c;
     return DDAGPU_OK;
@@ -1441,6 +1446,42 @@ int refine_loop(ddagpu_ctx *c, int solver, float rTau, int nmat1, double d0, int
     return DDAGPU_OK;
 }
 
+// Refinement of CG (solver 0): the reference's CG recurrences with FP64 fields, scalars and
+// true residuals around the FP32 FFT matvec, never restarted (mixed_cg, fp64.cu).  The
+// right-hand side is p_inc in FP64 (kinc, einc) or, with from_b32, the float field in
+// c->b32.  Leaves float(x) in c->p.
+int mixed_refine(ddagpu_ctx *c, const float *cListMaterials, int nmat1, int nact, double d0,
+                 const double *kinc, const double *einc, bool from_b32, double Error_max,
+                 int max_outer, int inner_max_step, ddagpu_refine_info &ri)
+{
+    if (!c->mcg) c->mcg = new MixedCgBuffers();
+    CK(c->mcg->ensure(3 * c->N));
+    std::vector<double2> al((size_t)nmat1);
+    for (int m = 0; m < nmat1; m++) al[(size_t)m] = make_double2(cListMaterials[2 * m], cListMaterials[2 * m + 1]);
+    CK(cudaMemcpyAsync(c->mcg->alpha, al.data(), nmat1 * sizeof(double2), cudaMemcpyHostToDevice, c->st));
+    Field64View f{c->N, c->ni, c->nj, c->nl, c->occ, c->mv, c->mcg->alpha};
+    CK(f64_right_hand_side(f, d0, kinc, einc, from_b32 ? c->b32 : nullptr, c->mcg->b, c->st));
+    c->launches += 1;
+    const ConvFn conv = [&](const float2 *src, float2 *out) {
+        c->launches += 3;
+        return launch_matvec(mv_args(c, 1, src, out, 0, 0.f, nullptr, 0, nmat1, false), c->st);
+    };
+    MixedCgResult R;
+    CK(mixed_cg(*c->mcg, f, al.data(), nmat1, nact, Error_max, max_outer, inner_max_step,
+                conv, c->s, c->w, c->rb, c->p, c->st, R, &c->launches));
+    std::memset(&ri, 0, sizeof ri);
+    ri.outer = R.outer;
+    ri.inner_steps = R.iterations;
+    ri.matvecs = R.matvecs;
+    ri.err = R.err;
+    for (int k = 0; k < 64; k++) ri.err_history[k] = R.history[k];
+    int werr = 0;
+    CK(cudaMemcpyAsync(&werr, c->err_dev, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    RET(device_wait_error(c, werr));
+    return DDAGPU_OK;
+}
+
 void aos_to_soa(const float *in, float2 *out, size_t N)
 {
     for (size_t q = 0; q < N; q++)
@@ -1491,7 +1532,10 @@ int ddagpu_solve_linear(ddagpu_ctx *c, int solver, float rTau, const float *cLis
     CK(cudaMemcpyAsync(c->b32, soa.data(), n3 * sizeof(float2), cudaMemcpyHostToDevice, c->st));
     ddagpu_refine_info ri;
     std::memset(&ri, 0, sizeof ri);
-    if (refine) {
+    if (refine && solver == 0) {
+        RET(mixed_refine(c, cListMaterials, nmat1, nact, c->kd, nullptr, nullptr, true, Error_max,
+                         max_step, inner_max_step, ri));
+    } else if (refine) {
         RhsState S0;
         std::memset(&S0, 0, sizeof S0);
         S0.active = 1;
@@ -1560,24 +1604,29 @@ int ddagpu_dda_fft_refined(ddagpu_ctx *c, int solver, float rTau, const float *c
     if (ndir) CK(cudaMemcpyAsync(c->ksc, kdir.data(), kdir.size() * sizeof(double), cudaMemcpyHostToDevice, c->st));
     // nact: counted by upload_materials
     if (nact == 0) return fail(DDAGPU_EINVAL, "no active dipoles");
-    // outer right-hand side b = p_inc (FirstApproximation), x = b
-    {
-        RhsState S0;
-        std::memset(&S0, 0, sizeof S0);
-        S0.active = 1;
-        S0.nact = nact;
-        int one = 1;
-        CK(cudaMemcpyAsync(c->state, &S0, sizeof S0, cudaMemcpyHostToDevice, c->st));
-        CK(cudaMemcpyAsync(c->active, &one, sizeof one, cudaMemcpyHostToDevice, c->st));
-    }
-    FieldArgs F = fa_args(c, 1, nmat1, d0, rTau);
-    CK(launch_first_approx(F, c->st));
-    CK(cudaMemcpyAsync(c->b32, c->p, n3 * sizeof(float2), cudaMemcpyDeviceToDevice, c->st));
-    c->launches += 1;
     ddagpu_refine_info ri;
     double err = 0.0;
-    RET(refine_loop(c, solver, rTau, nmat1, d0, nact, Error_max, max_outer, inner_rel,
-                    inner_max_step, ri, err));
+    if (solver == 0) {
+        RET(mixed_refine(c, cListMaterials, nmat1, nact, d0, kd3, ed6, false, Error_max, max_outer,
+                         inner_max_step, ri));
+    } else {
+        // outer right-hand side b = p_inc (FirstApproximation), x = b
+        {
+            RhsState S0;
+            std::memset(&S0, 0, sizeof S0);
+            S0.active = 1;
+            S0.nact = nact;
+            int one = 1;
+            CK(cudaMemcpyAsync(c->state, &S0, sizeof S0, cudaMemcpyHostToDevice, c->st));
+            CK(cudaMemcpyAsync(c->active, &one, sizeof one, cudaMemcpyHostToDevice, c->st));
+        }
+        FieldArgs F = fa_args(c, 1, nmat1, d0, rTau);
+        CK(launch_first_approx(F, c->st));
+        CK(cudaMemcpyAsync(c->b32, c->p, n3 * sizeof(float2), cudaMemcpyDeviceToDevice, c->st));
+        c->launches += 1;
+        RET(refine_loop(c, solver, rTau, nmat1, d0, nact, Error_max, max_outer, inner_rel,
+                        inner_max_step, ri, err));
+    }
     RET(run_post(c, 1, nmat1, d0, ndir));
     std::vector<float2> esc((size_t)ndir * 3);
     float ca = 0, ce = 0;
@@ -1592,6 +1641,92 @@ int ddagpu_dda_fft_refined(ddagpu_ctx *c, int solver, float rTau, const float *c
     *rCabs = ca;
     *rCext = ce;
     if (info) *info = ri;
+    return DDAGPU_OK;
+}
+
+int ddagpu_solve_fp64(ddagpu_ctx *c, int solver, double tau, const double *alpha,
+                      const int *iListMV, int n_mat, const signed char *cAlpha, double d0,
+                      const double *kinc, const double *Einc, const double *rhs, const double *x0,
+                      int Max_Step, double Error_max, int ndir, const double *ksc, double *Esc,
+                      double *Cabs, double *Cext, double *p_out, ddagpu_solve_info *info,
+                      double *trace)
+{
+    if (!c || !alpha || !iListMV || !cAlpha || !kinc || !Einc || !Cabs || !Cext)
+        return fail(DDAGPU_EINVAL, "null argument");
+    if (solver < 0 || solver > 3) return fail(DDAGPU_EINVAL, "solver must be 0..3");
+    if (Max_Step < 0 || ndir < 0 || (ndir > 0 && (!ksc || !Esc)))
+        return fail(DDAGPU_EINVAL, "bad solve parameters");
+    std::lock_guard<std::mutex> lk(c->mu);
+    DevGuard dg(c->dev);
+    const int nmat1 = n_mat + 1;
+    int nact = 0;
+    RET(upload_materials(c, iListMV, nmat1, cAlpha, &nact));
+    if (nact == 0) return fail(DDAGPU_EINVAL, "no active dipoles");
+    if (!c->f64) c->f64 = new Fp64Buffers();
+    CK(c->f64->ensure(c->ni, c->nj, c->nl, c->kd, c->st));
+    const size_t N = c->N;
+    // the reference's cvector layout [N][3] <-> structure of arrays [3][N]
+    auto to_soa = [&](const double *in, std::vector<double2> &out) {
+        out.resize(3 * N);
+        for (size_t q = 0; q < N; q++)
+            for (int k = 0; k < 3; k++) out[k * N + q] = make_double2(in[6 * q + 2 * k], in[6 * q + 2 * k + 1]);
+    };
+    std::vector<double2> al((size_t)nmat1), rs, xs, ps;
+    for (int m = 0; m < nmat1; m++) al[(size_t)m] = make_double2(alpha[2 * m], alpha[2 * m + 1]);
+    if (rhs) to_soa(rhs, rs);
+    if (x0) to_soa(x0, xs);
+    if (p_out) ps.resize(3 * N);
+    Fp64Problem P{};
+    P.solver = solver;
+    P.tau = tau;
+    P.nmat1 = nmat1;
+    P.alpha = al.data();
+    P.occ = c->occ;
+    P.mv = c->mv;
+    P.nact = nact;
+    P.d0 = d0;
+    for (int k = 0; k < 3; k++) P.kinc[k] = kinc[k];
+    for (int k = 0; k < 6; k++) P.einc[k] = Einc[k];
+    P.rhs = rhs ? rs.data() : nullptr;
+    P.x0 = x0 ? xs.data() : nullptr;
+    P.max_step = Max_Step;
+    P.err_max = Error_max;
+    P.ndir = ndir;
+    P.ksc = ksc;
+    Fp64Result R;
+    R.esc = Esc;
+    R.p = p_out ? ps.data() : nullptr;
+    R.trace = trace;
+    R.trace_len = trace ? Max_Step + 1 : 0;
+    if (trace) std::fill(trace, trace + Max_Step + 1, 0.0);
+    CK(solve_fp64(*c->f64, P, c->st, R, &c->launches));
+    *Cabs = R.cabs;
+    *Cext = R.cext;
+    if (p_out)
+        for (size_t q = 0; q < N; q++)
+            for (int k = 0; k < 3; k++) {
+                p_out[6 * q + 2 * k] = ps[k * N + q].x;
+                p_out[6 * q + 2 * k + 1] = ps[k * N + q].y;
+            }
+    if (info) {
+        info->steps = R.steps;
+        info->step_min = R.step_min;
+        info->rolled_back = R.rolled_back;
+        info->matvecs = R.matvecs;
+        info->err = R.err;
+        info->err_min = R.err_min;
+    }
+    return DDAGPU_OK;
+}
+
+int ddagpu_release_fp64(ddagpu_ctx *c)
+{
+    if (!c) return fail(DDAGPU_EINVAL, "null context");
+    std::lock_guard<std::mutex> lk(c->mu);
+    DevGuard dg(c->dev);
+    if (c->st) cudaStreamSynchronize(c->st);
+    delete c->f64;
+    c->f64 = nullptr;
     return DDAGPU_OK;
 }
 

@@ -140,17 +140,14 @@ inline unsigned blocks(size_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
 size_t ahat_elems(int ni, int nj, int nl) { return (size_t)6 * (ni + 1) * (nj + 1) * (nl + 1); }
 
-cudaError_t green_build_octant(int ni, int nj, int nl, double kd, float2 *ahat, cudaStream_t st)
+namespace {
+
+// The octant in FP64 into b1 as [comp][kx][ky][kz] (natural kz order); b0 and tab are
+// scratch of ahat_elems and 6 (nmax + 1) nmax doubles.
+void octant_fp64(int ni, int nj, int nl, double kd, double2 *b0, double2 *b1, double *tab,
+                 size_t tabn, cudaStream_t st)
 {
     const size_t big = ahat_elems(ni, nj, nl);
-    double2 *b0 = nullptr, *b1 = nullptr;
-    double *tab = nullptr;
-    const int nmax = ni > nj ? (ni > nl ? ni : nl) : (nj > nl ? nj : nl);
-    const size_t tabn = (size_t)(nmax + 1) * nmax;
-    cudaError_t e;
-    if ((e = cudaMallocAsync(&b0, big * sizeof(double2), st))) return e;
-    if ((e = cudaMallocAsync(&b1, big * sizeof(double2), st))) return e;
-    if ((e = cudaMallocAsync(&tab, 6 * tabn * sizeof(double), st))) return e;
     double *ct[3], *stb[3];
     const int ns[3] = {ni, nj, nl};
     for (int a = 0; a < 3; a++) {
@@ -168,9 +165,43 @@ cudaError_t green_build_octant(int ni, int nj, int nl, double kd, float2 *ahat, 
         b1, b0, ni, nj, nl + 1, ct[1], stb[1], 1);
     // x: a = comp, nt = ni, B = (nj+1)(nl+1)
     axis_sum<<<blocks(big, 256), 256, 0, st>>>(b0, b1, 1, ni, (nj + 1) * (nl + 1), ct[0], stb[0], 0);
+}
+
+size_t trig_elems(int ni, int nj, int nl)
+{
+    const int nmax = ni > nj ? (ni > nl ? ni : nl) : (nj > nl ? nj : nl);
+    return (size_t)(nmax + 1) * nmax;
+}
+
+}  // namespace
+
+cudaError_t green_build_octant(int ni, int nj, int nl, double kd, float2 *ahat, cudaStream_t st)
+{
+    const size_t big = ahat_elems(ni, nj, nl), tabn = trig_elems(ni, nj, nl);
+    double2 *b0 = nullptr, *b1 = nullptr;
+    double *tab = nullptr;
+    cudaError_t e;
+    if ((e = cudaMallocAsync(&b0, big * sizeof(double2), st))) return e;
+    if ((e = cudaMallocAsync(&b1, big * sizeof(double2), st))) return e;
+    if ((e = cudaMallocAsync(&tab, 6 * tabn * sizeof(double), st))) return e;
+    octant_fp64(ni, nj, nl, kd, b0, b1, tab, tabn, st);
     to_octant<<<blocks(big, 256), 256, 0, st>>>(b1, ahat, ni, nj, nl);
     cudaFreeAsync(b0, st);
     cudaFreeAsync(b1, st);
+    cudaFreeAsync(tab, st);
+    return cudaGetLastError();
+}
+
+cudaError_t green_build_octant64(int ni, int nj, int nl, double kd, double2 *out, cudaStream_t st)
+{
+    const size_t big = ahat_elems(ni, nj, nl), tabn = trig_elems(ni, nj, nl);
+    double2 *b0 = nullptr;
+    double *tab = nullptr;
+    cudaError_t e;
+    if ((e = cudaMallocAsync(&b0, big * sizeof(double2), st))) return e;
+    if ((e = cudaMallocAsync(&tab, 6 * tabn * sizeof(double), st))) return e;
+    octant_fp64(ni, nj, nl, kd, b0, out, tab, tabn, st);
+    cudaFreeAsync(b0, st);
     cudaFreeAsync(tab, st);
     return cudaGetLastError();
 }

@@ -89,14 +89,19 @@ int ddagpu_dda_fft(ddagpu_ctx *ctx, int iNoIllumination, int iMode_SolutionMetho
                    int iMode_FFT, int iNoScPl, int iNoA, const float *ksc, float *Esc,
                    float *rCabs, float *rCext, ddagpu_solve_info *info, double *trace);
 
-/* Iterative refinement around DDA_FFT's solvers: the solution and the true residual
- * r = p_inc - (p - alpha G*p) are kept in FP64, each outer step solves A d = r in FP32
- * with solver iMode_SolutionMethod (restarted from d = r, to inner_rel x the current
- * residual, at most inner_max_step iterations, best iterate kept) and adds d to p.  Stops
- * when the mean true residual norm (the reference's discrepancy, dda_func.cpp:784-811, of
- * the true instead of the recursively updated residual) is <= Error_max, or after
- * max_outer steps; info reports the residual of every outer step.  Outputs as
- * ddagpu_dda_fft. */
+/* Iterative refinement around DDA_FFT's solvers, every convolution on the FP32 FFT passes,
+ * the solution and the true residual r = p_inc - (p - alpha G*p) in FP64.  Stops when the
+ * mean true residual norm (the reference's discrepancy, dda_func.cpp:784-811, of the true
+ * instead of the recursively updated residual) is <= Error_max, or after max_outer outer
+ * steps; info reports the true residual of every outer step.  Outputs as ddagpu_dda_fft.
+ *   iMode_SolutionMethod 0 (CG): the reference's CG recurrences (dda_func.cpp:1359-1371)
+ *     run with FP64 fields and FP64 scalars, never restarted; an outer step replaces the
+ *     updated residual by the true one when the updated one meets Error_max, or after
+ *     inner_max_step iterations (inner_rel is not used).  Reaches a discrepancy near 1e-8
+ *     on a 128^3 sphere at x = 16, m = 1.6+0.0005i.
+ *   1..3: each outer step solves A d = r in FP32 with that solver (restarted from d = r, to
+ *     inner_rel x the current residual, at most inner_max_step iterations, best iterate
+ *     kept) and adds d to p. */
 typedef struct {
     int outer;               /* outer steps taken                                       */
     int inner_steps;         /* inner solver iterations, all outer steps                */
@@ -122,6 +127,25 @@ int ddagpu_solve_linear(ddagpu_ctx *ctx, int iMode_SolutionMethod, float rTau,
                         const signed char *cAlpha, const float *rhs, double Error_max,
                         int max_step, int refine, double inner_rel, int inner_max_step,
                         float *x_out, ddagpu_refine_info *info);
+
+/* FP64 solve: DDA_FFT (dda_func.cpp:1075-1570) with every field, transform, product and
+ * scalar in double -- the reference's FP64 build (complex.hpp:10 as `typedef double real`)
+ * run on the GPU, without its float casts of the solver coefficients.  It is the oracle
+ * solve that the precision pattern measures a float solve against, at sizes where the CPU
+ * FP64 build takes hours.  alpha: 2 (n_mat + 1) doubles; kinc, Einc, ksc [ndir][3] and
+ * Esc [ndir][6] doubles; rhs (optional) solves A p = rhs instead of A p = p_inc, x0
+ * (optional) starts the solver from x0 instead of the right-hand side; rhs, x0 and p_out
+ * (optional, the final dipoles) are fields of 6 doubles per cell.  Same stopping rule,
+ * rollback and outputs as ddagpu_dda_fft.  The FP64 work space (about 100 bytes per padded
+ * cell plus 10 fields) is allocated on the first call and kept until ddagpu_release_fp64 or
+ * ddagpu_destroy. */
+int ddagpu_solve_fp64(ddagpu_ctx *ctx, int iMode_SolutionMethod, double rTau, const double *alpha,
+                      const int *iListMV, int n_mat, const signed char *cAlpha, double d0,
+                      const double *kinc, const double *Einc, const double *rhs, const double *x0,
+                      int Max_Step, double Error_max, int ndir, const double *ksc, double *Esc,
+                      double *Cabs, double *Cext, double *p_out, ddagpu_solve_info *info,
+                      double *trace);
+int ddagpu_release_fp64(ddagpu_ctx *ctx);
 
 /* FarField sub-seam (dda_func.cpp:1576-1625) for ndir directions at once. */
 int ddagpu_farfield(ddagpu_ctx *ctx, const int *iListMV, int n_mat, const signed char *cAlpha,
