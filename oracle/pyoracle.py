@@ -252,6 +252,7 @@ class RefLib:
         L.dref_gen_anthrax.argtypes = [C.c_ulonglong, _i, _i, _i, _d, _d, _i, _p, _p, _p]
         L.dref_gen_random_ellipsoid.argtypes = [C.c_ulonglong, _i, _i, _i, _d, _d, _i, _p, _p, _p]
         L.dref_run_samples.argtypes = [C.POINTER(RunCfg), _p, _i, _i, _i, _p, _p, _p, _p, _p]
+        L.dref_set_per_sample.argtypes = [_p]
 
     def green(self, ni, nj, nl, kd, fft_mode=0):
         out = np.zeros((2 * ni, 2 * nj, 2 * nl, 6), self.cdt)
@@ -373,8 +374,9 @@ class RefLib:
                                                _ptr(sps), _ptr(occ), C.byref(nxt))
         return occ, n, nxt.value
 
-    def run_samples(self, cfg: RunCfg, nsamples, nthreads=1, occ=None, verbose=0):
-        """The reference's sample loop; returns (seconds, cabs_sum, cext_sum, mueller_sum)."""
+    def run_samples(self, cfg: RunCfg, nsamples, nthreads=1, occ=None, verbose=0, each=False):
+        """The reference's sample loop; returns (seconds, cabs_sum, cext_sum, mueller_sum),
+        and with each=True also the per-sample (cabs, cext, mueller[angles][4][4])."""
         na = int(round((cfg.theta_max - cfg.theta_min) / cfg.theta_step + 1))
         mm = np.zeros((na + 2, 4, 4), self.rdt)
         ca = np.zeros(1, self.rdt)
@@ -382,9 +384,16 @@ class RefLib:
         secs = C.c_double(0)
         nout = C.c_int(0)
         o = _c(occ, np.int8) if occ is not None else np.zeros(1, np.int8)
+        per = np.zeros(nsamples * (2 + 16 * (na + 2)), self.rdt) if each else None
+        self.lib.dref_set_per_sample(_ptr(per) if each else None)
         self.lib.dref_run_samples(C.byref(cfg), _ptr(o), nthreads, nsamples, verbose,
                                   C.byref(secs), _ptr(ca), _ptr(ce), _ptr(mm), C.byref(nout))
-        return secs.value, float(ca[0]), float(ce[0]), mm[: nout.value].copy()
+        out = (secs.value, float(ca[0]), float(ce[0]), mm[: nout.value].copy())
+        if not each:
+            return out
+        n = nout.value   # the C side writes rows of 2 + 16 n reals
+        per = per[: nsamples * (2 + 16 * n)].reshape(nsamples, 2 + 16 * n)
+        return out + ((per[:, 0].copy(), per[:, 1].copy(), per[:, 2:].reshape(nsamples, n, 4, 4)),)
 
 
 def orientation_solves(O: Oracle, grid, x, materials, nsamples, target=1, b_a=1.0, c_a=1.0,

@@ -483,10 +483,22 @@ struct dref_run_cfg {
     double monomer_radius, monomer_ratio, packing;   /* target 6 (main.cpp:300, 585-586) */
 };
 
+/* Per-sample results of the next dref_run_samples call (null: none): sample k writes
+ * Cabs, Cext and its plane-averaged Mueller matrices, 2 + 16 n_angles reals, at
+ * each + k (2 + 16 n_angles).  Cleared by the call. */
+static ioreal *g_each = nullptr;
+int dref_set_per_sample(ioreal *each)
+{
+    g_each = each;
+    return 0;
+}
+
 int dref_run_samples(const dref_run_cfg *c, const signed char *occ_in, int nthreads, int nsamples,
                      int verbose, double *seconds, ioreal *cabs_sum, ioreal *cext_sum,
                      ioreal *mueller_sum, int *nangles_out)
 {
+    ioreal *each = g_each;
+    g_each = nullptr;
     const int ni = c->ni, nj = c->nj, nl = c->nl;
     const real xr = (real)c->x, tmin = (real)c->theta_min, tmax = (real)c->theta_max,
                tstep = (real)c->theta_step;
@@ -684,6 +696,12 @@ int dref_run_samples(const dref_run_cfg *c, const signed char *occ_in, int nthre
                     mm[(size_t)a] = mm[(size_t)a] + JonesToMuller(mj);
                 }
                 mm[(size_t)a] = mm[(size_t)a] / (real)nP;
+            }
+            if (each) {
+                ioreal *o = each + (size_t)task * (2 + 16 * (size_t)nA);
+                o[0] = scabs;
+                o[1] = scext;
+                for (int a = 0; a < nA; a++) std::memcpy(o + 2 + 16 * a, &mm[(size_t)a], sizeof(mmuller));
             }
             std::lock_guard<std::mutex> lk(mtx);
             fcabs += scabs;

@@ -8,6 +8,7 @@ executable (oracle/_ref/dda_fft.out).  Run in a container that has the reference
     make -f oracle/Makefile all && python tests/golden/make_golden.py
     python tests/golden/make_golden.py targets          # targets_v72.npz
     python tests/golden/make_golden.py configs          # configs_v72.npz (64^3, minutes)
+    python tests/golden/make_golden.py fp64             # fp64_v72.npz (32^3 and 64^3 FP64 solves)
 
 The fixtures are small (.npz, a few MB in all) and are committed; the tests read
 them without needing the reference.
@@ -232,9 +233,58 @@ def full_configs(R, R64, out):
         out[name] = np.concatenate([[ca, ce], mm.ravel()])
         _, ca, ce, mm = R64.run_samples(cfg, ns, 1)
         out[name + "_64"] = np.concatenate([[ca, ce], mm.ravel()])
+    # all 256 Monte-Carlo orientations of the batching configuration, one by one, in both
+    # builds (worker 0's stream, as the single-threaded reference draws them)
+    cfg = make_run_cfg(grid=64, target=2, b_a=0.7, c_a=0.5, x=6.0, materials=((1.55, 0.005),),
+                       orientation=1, seed=7)
+    for tag, L in (("", R), ("_64", R64)):
+        _, _, _, _, (ca, ce, mm) = L.run_samples(cfg, 256, 1, each=True)
+        out["c3a256_cabs" + tag] = ca
+        out["c3a256_cext" + tag] = ce
+        out["c3a256_mueller" + tag] = mm.reshape(256, -1, 16)
+
+
+# FP64 solves of the reference's FP64 build at 32^3 and 64^3: (name, edge, x, m, solver,
+# polarizability model, incident polarisation, steps).  Error_max is below reach, so every
+# step runs; the fixtures keep the final dipoles of the middle plane i = n / 2.
+FP64_SOLVES = [
+    ("s32_bicg", 32, 4.0, 1.6 + 0.0005j, 2, 1, (1, 0, 0), 10),
+    ("s32_cg", 32, 4.0, 1.6 + 0.0005j, 0, 2, (0, 1, 0), 16),
+    ("s64_bicg", 64, 8.0, 1.5 + 0.01j, 2, 5, (1, 0, 0), 6),
+    ("s64_cg", 64, 8.0, 1.6 + 0.0005j, 0, 1, (0, 1, 0), 10),
+]
+
+
+def fp64_solves(R64, out):
+    """DDA_FFT of the reference's FP64 build on spheres at 32^3 and 64^3 (19 angles, one
+    plane), for checking the GPU's FP64 solve."""
+    th = np.deg2rad(np.arange(19) * 10.0)
+    ksc = np.stack([np.sin(th), np.zeros_like(th), np.cos(th)], 1)[None]
+    for name, n, x, m, solver, model, einc, steps in FP64_SOLVES:
+        kd = 2 * x / n
+        occ, _ = R64.gen_ellipsoid(n, n, n)
+        a = R64.polarizability(model, kd, m, (0, 0, 1), einc)
+        alpha = np.array([0, a], np.complex128)
+        r = R64.dda_fft(occ, alpha, np.array([0, 1], np.int32), kd, (0, 0, 1), einc,
+                        R64.green(n, n, n, kd), ksc, solver=solver, max_step=steps, err_max=1e-14)
+        out[f"{name}_cfg"] = np.array([n, kd, solver, steps] + list(einc), np.float64)
+        out[f"{name}_alpha"] = alpha
+        out[f"{name}_trace"] = r["trace"]
+        out[f"{name}_cext"] = r["cext"]
+        out[f"{name}_cabs"] = r["cabs"]
+        out[f"{name}_esc"] = r["esc"].reshape(-1, 3)
+        out[f"{name}_pmid"] = r["p"][n // 2]
+    out["fp64_ksc"] = ksc.reshape(-1, 3)
 
 
 def main():
+    if sys.argv[1:] == ["fp64"]:
+        out: dict = {}
+        fp64_solves(RefLib(REF64_SO), out)
+        path = os.path.join(HERE, "fp64_v72.npz")
+        np.savez_compressed(path, **out)
+        print(f"wrote {path}: {os.path.getsize(path) / 1e6:.2f} MB, {len(out)} arrays")
+        return
     if sys.argv[1:] == ["configs"]:
         out: dict = {}
         full_configs(RefLib(), RefLib(REF64_SO), out)

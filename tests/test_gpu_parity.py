@@ -402,3 +402,29 @@ def test_material_switched_off_with_polarisability(D, oracle):
     for q in ("cext", "cabs"):
         assert abs(r[q] - o[q]) <= 1e-4 * abs(o[q]), (q, r[q], o[q])
     assert rel(r["esc"], o["esc"]) < 1e-3
+
+
+@pytest.mark.parametrize("model", [2, 3, 4])
+@pytest.mark.parametrize("err_max,solver", [(1e-3, 0), (1e-6, 0), (1e-6, 2)])
+def test_batched_polarizability_models_vs_oracle(D, oracle, model, err_max, solver):
+    """CMRR, CMNR and ILDR (dda_func.cpp:1639-1665), computed by the library's batched path,
+    against the FP64 oracle's sample loop: at Error_max 1e-3 the solve stops at step 0, so
+    the cross sections carry alpha itself (Cabs explicitly, dda_func.cpp:1709-1719); at 1e-6
+    the solvers iterate.  Two materials, two planes, fixed orientation (30, 45, 60 deg)."""
+    n, x = 16, 3.0
+    rng = np.random.default_rng(model)
+    occ, _ = oracle.gen_ellipsoid(n, n, n)
+    occ = np.where(occ > 0, rng.integers(1, 3, occ.shape), 0).astype(np.int8)
+    mats = [(1.5, 0.01), (1.3, 0.2)]
+    cfg = D.BatchConfig(occ=occ, materials=mats, polarizability=model, solver=solver, err_max=err_max,
+                        max_step=200, nplanes=2)
+    rot = D.fixed_rotation(30.0, 45.0, 60.0)[None]
+    with D.Context(n, 2 * x / n, max_rhs=2) as ctx:
+        r = ctx.orientation_solves(cfg, rot)
+    o = orientation_solves(oracle, n, x, mats, 1, polarizability=model, solver=solver, err_max=err_max,
+                           max_step=200, nplanes=2, psi=30.0, iota=45.0, kappa=60.0, occ=occ)
+    for q in ("cabs", "cext"):
+        assert abs(r[q][0] - o[q]) < 1e-4 * abs(o[q]), (q, r[q][0], o[q])
+    M, Mo = r["mueller"][0].reshape(-1, 16), o["mueller"].reshape(-1, 16)
+    sig = np.abs(Mo) > 1e-3 * np.abs(Mo).max()
+    assert (np.abs(M - Mo)[sig] / np.abs(Mo)[sig]).max() < 1e-4
