@@ -10,6 +10,7 @@ from .api import (  # noqa: F401
     BatchConfig,
     Context,
     DDAGPUError,
+    Group,
     RandomEllipsoid,
     StateFile,
     build,
@@ -21,6 +22,6 @@ from .api import (  # noqa: F401
     sample_loop,
 )
 
-__all__ = ["Agglomerate", "BatchConfig", "Context", "DDAGPUError", "RandomEllipsoid", "StateFile",
+__all__ = ["Agglomerate", "BatchConfig", "Context", "DDAGPUError", "Group", "RandomEllipsoid", "StateFile",
            "build", "fixed_rotation", "lib", "library_path", "mc_rotations", "num_angles",
            "sample_loop"]

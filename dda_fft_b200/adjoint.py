@@ -174,10 +174,9 @@ class GPUBackend:
 class GPUFP64Backend:
     """FP64 solves on the GPU (ddagpu_solve_fp64: fields, FFTs and scalars in double, the
     reference's CG recurrences), for reference gradients and finite differences at sizes
-    the CPU oracle cannot reach.  x0 (per-dipole start) continues from a nearby solution:
-    a finite-difference solve then only computes the change the perturbation makes."""
+    the CPU oracle cannot reach.  x0 (per-dipole start) continues from a nearby solution."""
 
-    def __init__(self, problem: Problem, err_max=1e-16, solver=0, max_step=20000):
+    def __init__(self, problem: Problem, err_max=1e-13, solver=0, max_step=5000):
         import dda_fft_b200 as D
         self.P = problem
         self.ctx = D.Context(problem.grid, problem.kd, max_rhs=1)
@@ -187,10 +186,11 @@ class GPUFP64Backend:
         self.matvecs = 0
         self.last_err = 0.0
 
-    def solve(self, occ, table, rhs_dipoles, x0=None):
+    def solve(self, occ, table, rhs_dipoles, x0=None, err_max=None):
         mv = np.array([0] + [1] * (len(table) - 1), np.int32)
         r = self.ctx.solve_fp64(occ, table, mv, self.P.kd, self.P.kinc, self.P.einc[0], None,
-                                solver=self.solver, max_step=self.max_step, err_max=self.err_max,
+                                solver=self.solver, max_step=self.max_step,
+                                err_max=self.err_max if err_max is None else err_max,
                                 rhs=self.P.field(rhs_dipoles),
                                 x0=None if x0 is None else self.P.field(x0), want_p=True,
                                 trace=False)

@@ -118,6 +118,12 @@ def lib():
         L.ddagpu_get_tiling.argtypes = [_p, C.POINTER(_i), C.POINTER(_i)]
         L.ddagpu_autotune.argtypes = [_p, _i]
         L.ddagpu_set_kernels.argtypes = [_p, _i]
+        L.ddagpu_group_create.argtypes = [C.POINTER(_p), _p, _i]
+        L.ddagpu_group_destroy.argtypes = [_p]
+        L.ddagpu_group_graph_runs.argtypes = [_p]
+        L.ddagpu_group_graph_runs.restype = C.c_longlong
+        L.ddagpu_group_agglomerate_solves.argtypes = [_p, C.POINTER(_BatchCfg), _p, _p, _p, _p, _p, _p,
+                                                      _p, _p, C.POINTER(BatchInfo)]
         L.ddagpu_farfield_noalloc.argtypes = [_i, _i, _i, _i, _f, _p, _p, _i, _p, _i, _p, _p, _p]
         L.ddagpu_get_kernels.argtypes = [_p]
         L.ddagpu_set_fast_variant.argtypes = [_p, _i, _i]
@@ -412,12 +418,14 @@ class Context:
         return out
 
     def dda_fft_refined(self, occ, alpha, listmv, d0, kinc, einc, ksc, solver=2, tau=0.0,
-                        err_max=1e-5, max_outer=20, inner_rel=0.05, inner_max_step=None):
-        """FP64-residual iterative refinement around the chosen solver.  CG (solver 0) is
-        never restarted: inner_max_step (default 100000) only bounds the iterations between
-        true residuals; the other solvers restart every outer step (default 200 steps)."""
+                        err_max=1e-5, max_outer=20, inner_rel=None, inner_max_step=None):
+        """FP64-residual iterative refinement around the chosen solver.  CG (solver 0) runs
+        with FP64 fields and scalars between true residuals (defaults: inner_rel 1e-3,
+        inner_max_step 5000); the other solvers run in FP32 (defaults 0.05, 200)."""
+        if inner_rel is None:
+            inner_rel = 1e-3 if solver == 0 else 0.05
         if inner_max_step is None:
-            inner_max_step = 100000 if solver == 0 else 200
+            inner_max_step = 5000 if solver == 0 else 200
         o = np.ascontiguousarray(occ, np.int8)
         a = _cvec(np.asarray(alpha, np.complex64).reshape(-1, 1)).ravel()
         mv = np.ascontiguousarray(listmv, np.int32)
@@ -438,11 +446,13 @@ class Context:
                     inner_steps=info.inner_steps, matvecs=info.matvecs, err=info.err, history=hist)
 
     def solve_linear(self, occ, alpha, listmv, rhs, solver=0, tau=0.0, err_max=1e-8,
-                     max_step=40, refine=True, inner_rel=0.05, inner_max_step=None):
-        """x with (I - D_alpha G) x = rhs; rhs complex (ni, nj, nl, 3).  inner_max_step as
-        for dda_fft_refined."""
+                     max_step=40, refine=True, inner_rel=None, inner_max_step=None):
+        """x with (I - D_alpha G) x = rhs; rhs complex (ni, nj, nl, 3).  inner_rel and
+        inner_max_step as for dda_fft_refined."""
+        if inner_rel is None:
+            inner_rel = 1e-3 if solver == 0 else 0.05
         if inner_max_step is None:
-            inner_max_step = 100000 if solver == 0 else 300
+            inner_max_step = 5000 if solver == 0 else 300
         o = np.ascontiguousarray(occ, np.int8)
         a = _cvec(np.asarray(alpha, np.complex64).reshape(-1, 1)).ravel()
         mv = np.ascontiguousarray(listmv, np.int32)
@@ -631,3 +641,78 @@ class Context:
     def autotune(self, nrhs: int = 4):
         _check(lib().ddagpu_autotune(self._h, nrhs))
         return self.tiling()
+
+
+class Group:
+    """Contexts of different lattice sizes whose batched agglomerate solves run as one
+    graph launch per call (ddagpu_group_*)."""
+
+    def __init__(self, contexts):
+        self.contexts = list(contexts)
+        arr = (C.c_void_p * len(self.contexts))(*[c.handle for c in self.contexts])
+        h = C.c_void_p()
+        _check(lib().ddagpu_group_create(C.byref(h), arr, len(self.contexts)))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().ddagpu_group_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def graph_runs(self) -> int:
+        return int(lib().ddagpu_group_graph_runs(self._h))
+
+    def agglomerate_solves(self, cfg: BatchConfig, monomers_per_member, rot_per_member=None):
+        """monomers_per_member[k]: the monomer lists of member k's realisations (at most its
+        max_rhs / 2); returns one result dict per member, as Context.agglomerate_solves."""
+        K = len(self.contexts)
+        assert len(monomers_per_member) == K
+        na = num_angles(cfg.theta_min, cfg.theta_max, cfg.theta_step)
+        m = np.ascontiguousarray(np.asarray(cfg.materials, np.float32).ravel())
+        c = self.contexts[0]._cfg(cfg, m)
+        keep, outs = [], []
+        n_real = np.zeros(K, np.int32)
+        P = C.c_void_p * K
+        mon_p, cnt_p, rot_p, ca_p, ce_p, mm_p, nd_p = P(), P(), P(), P(), P(), P(), P()
+        for k, mons in enumerate(monomers_per_member):
+            counts = np.array([len(x) for x in mons], np.int32)
+            n = len(counts)
+            n_real[k] = n
+            flat = (np.ascontiguousarray(np.concatenate([np.asarray(x, np.float32).reshape(-1, 13)
+                                                         for x in mons]), np.float32)
+                    if counts.sum() else np.zeros((1, 13), np.float32))
+            out = dict(cabs=np.zeros(max(n, 1)), cext=np.zeros(max(n, 1)),
+                       mueller=np.zeros((max(n, 1), na, 4, 4)), ndip=np.zeros(max(n, 1), np.int32))
+            r = None
+            if rot_per_member is not None and rot_per_member[k] is not None:
+                r = np.ascontiguousarray(rot_per_member[k], np.float64).reshape(n, 3, 3)
+            keep += [counts, flat, r]
+            mon_p[k], cnt_p[k] = flat.ctypes.data, counts.ctypes.data
+            rot_p[k] = r.ctypes.data if r is not None else 0
+            ca_p[k], ce_p[k] = out["cabs"].ctypes.data, out["cext"].ctypes.data
+            mm_p[k], nd_p[k] = out["mueller"].ctypes.data, out["ndip"].ctypes.data
+            outs.append(out)
+        info = (BatchInfo * K)()
+        rots = rot_p if rot_per_member is not None else None
+        _check(lib().ddagpu_group_agglomerate_solves(self._h, C.byref(c), _ptr(n_real), mon_p, cnt_p, rots,
+                                                     ca_p, ce_p, mm_p, nd_p, info))
+        res = []
+        for k, out in enumerate(outs):
+            n = int(n_real[k])
+            res.append(dict(cabs=out["cabs"][:n], cext=out["cext"][:n], mueller=out["mueller"][:n],
+                            ndip=out["ndip"][:n], n_rhs=info[k].n_rhs, max_steps=info[k].max_steps,
+                            rolled_back=info[k].rolled_back, max_err=info[k].max_err))
+        return res

@@ -141,6 +141,7 @@ struct ddagpu_ctx {
     long long post_key = 0;          // shape of the post-processing recorded with a solve
     Fp64Buffers *f64 = nullptr;  // FP64 solve buffers (ddagpu_solve_fp64), built on first use
     MixedCgBuffers *mcg = nullptr;   // FP64 fields of the mixed-precision CG refinement
+    long long gen = 0;           // bumped whenever recorded graphs must be dropped
     long long g_per_iter = 0;    // kernels in one recorded iteration
     long long graph_runs = 0;    // graph launches by this context
     std::mutex mu;
@@ -184,6 +185,7 @@ int device_wait_error(ddagpu_ctx *c, int flag)
 // Forget the recorded solve graphs (they hold buffer addresses about to change).
 void drop_graphs(ddagpu_ctx *c)
 {
+    c->gen += 1;   // a group's graph holding this context is rebuilt too
     if (c->gexec) cudaGraphExecDestroy(c->gexec);
     if (c->graph) cudaGraphDestroy(c->graph);
     if (c->wexec) cudaGraphExecDestroy(c->wexec);
@@ -295,21 +297,14 @@ struct SolveResult {
     int matvec0 = 0, matvec_it = 0;
 };
 
-// The solver of DDA_FFT for nrhs right-hand sides whose occ, mv, alpha, kinc and einc are
-// already on the device.  Leaves the final (or rolled-back) dipoles in c->p.
-// The whole solve of a batch as one graph launch: step 0, the iterations as a conditional
+// The whole solve of a batch as graph nodes: step 0, the iterations as a conditional
 // while node, the rollback and the post-processing.  Captured once per solve shape and
-// kept in the context; the inputs (fields, tables, occupancy, nact) are device buffers
-// the host fills before each launch.
-template <class Step0, class Top, class Body>
-int run_whole_graph(ddagpu_ctx *c, int nrhs, int solver, float tau, int max_step, float err_max,
-                    int nmat1, double d0, int nact, const int *nact_per, SolveResult &res,
-                    Step0 &step0, Top &top, Body &body, const std::function<int()> &post)
+// kept in the context (or, for a group of contexts, in the group's graph, one independent
+// branch per context); the inputs (fields, tables, occupancy, nact) are device buffers the
+// host fills before each launch.
+ddagpu_ctx::GraphKey whole_key(ddagpu_ctx *c, int nrhs, int solver, float tau, int max_step, float err_max,
+                               int nmat1, double d0)
 {
-    cudaStream_t st = c->st;
-    std::vector<int> na((size_t)nrhs);
-    for (int k = 0; k < nrhs; k++) na[(size_t)k] = nact_per ? nact_per[k] : nact;
-    CK(cudaMemcpyAsync(c->nact_dev, na.data(), nrhs * sizeof(int), cudaMemcpyHostToDevice, st));
     ddagpu_ctx::GraphKey key{};
     key.solver = solver;
     key.nrhs = nrhs;
@@ -328,97 +323,100 @@ int run_whole_graph(ddagpu_ctx *c, int nrhs, int solver, float tau, int max_step
     key.trace = nullptr;
     key.occ = c->occ_stride ? (const void *)c->occ_b : (const void *)c->occ;
     key.post = c->post_key;
-    const long long l_before = c->launches;
-    if (!c->wexec || std::memcmp(&key, &c->wkey, sizeof key) != 0) {
-        if (c->wexec) cudaGraphExecDestroy(c->wexec);
-        if (c->wgraph) cudaGraphDestroy(c->wgraph);
-        c->wexec = nullptr;
-        c->wgraph = nullptr;
-        cudaGraph_t g = nullptr;
-        CK(cudaGraphCreate(&g, 0));
-        auto give_up = [&](int rc, cudaError_t e, const char *what) {
-            cudaStreamCaptureStatus cs;
-            if (cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone) {
-                cudaGraph_t t = nullptr;
-                cudaStreamEndCapture(st, &t);
-                if (t && t != g) cudaGraphDestroy(t);
-            }
-            cudaGraphDestroy(g);
-            if (rc != DDAGPU_OK) return rc;
-            return fail(DDAGPU_ECUDA, std::string("solve graph (") + what + "): " + cudaGetErrorString(e));
-        };
-        cudaGraphConditionalHandle h;
-        cudaError_t e = cudaGraphConditionalHandleCreate(&h, g, 0, 0);
-        if (e != cudaSuccess) return give_up(DDAGPU_OK, e, "handle");
-        const long long l0 = c->launches;
-        // phase 1: fresh state, step 0, the convergence test of step 1, the loop condition
-        e = cudaStreamBeginCaptureToGraph(st, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
-        if (e != cudaSuccess) return give_up(DDAGPU_OK, e, "capture");
-        int rc = DDAGPU_OK;
-        e = launch_init_state(c->state, c->active, nrhs, (double)err_max, c->nact_dev, st);
-        if (e == cudaSuccess) rc = step0();
-        if (rc == DDAGPU_OK && e == cudaSuccess) e = launch_step_set(c->step_dev, 1, st);
-        if (rc == DDAGPU_OK && e == cudaSuccess) rc = top(max_step, c->step_dev);
-        if (rc == DDAGPU_OK && e == cudaSuccess)
-            e = launch_loop_control(c->active, nrhs, c->step_dev, max_step, h, st);
-        if (rc != DDAGPU_OK || e != cudaSuccess) return give_up(rc, e, "step 0");
+    return key;
+}
+
+// Records the whole solve into graph g as a branch with no dependencies; n_fixed and
+// n_per_iter receive the kernels of the fixed part and of one loop pass.
+template <class Step0, class Top, class Body>
+int record_whole_solve(ddagpu_ctx *c, cudaGraph_t g, int nrhs, int max_step, float err_max, int nmat1,
+                       double d0, float tau, Step0 &step0, Top &top, Body &body,
+                       const std::function<int()> &post, long long &n_fixed, long long &n_per_iter)
+{
+    cudaStream_t st = c->st;
+    const long long l_save = c->launches;
+    auto give_up = [&](int rc, cudaError_t e, const char *what) {
         cudaStreamCaptureStatus cs;
-        const cudaGraphNode_t *deps = nullptr;
-        size_t ndeps = 0;
-        e = cudaStreamGetCaptureInfo(st, &cs, nullptr, nullptr, &deps, &ndeps);
-        if (e != cudaSuccess) return give_up(DDAGPU_OK, e, "capture info");
-        std::vector<cudaGraphNode_t> leaves(deps, deps + ndeps);
-        cudaGraph_t t = nullptr;
-        e = cudaStreamEndCapture(st, &t);
-        if (e != cudaSuccess) return give_up(DDAGPU_OK, e, "end capture");
-        const long long n_head = c->launches - l0 + 3;   // + init, step set, loop control
-        // the while node and its body: one iteration, the next step's test, the condition
-        cudaGraphNodeParams np{};
-        np.type = cudaGraphNodeTypeConditional;
-        np.conditional.handle = h;
-        np.conditional.type = cudaGraphCondTypeWhile;
-        np.conditional.size = 1;
-        cudaGraphNode_t cn;
-        e = cudaGraphAddNode(&cn, g, leaves.data(), leaves.size(), &np);
-        if (e != cudaSuccess) return give_up(DDAGPU_OK, e, "while node");
-        const long long l1 = c->launches;
-        e = cudaStreamBeginCaptureToGraph(st, np.conditional.phGraph_out[0], nullptr, nullptr, 0,
-                                          cudaStreamCaptureModeThreadLocal);
-        if (e != cudaSuccess) return give_up(DDAGPU_OK, e, "body capture");
-        rc = body(max_step, c->step_dev, true);
-        if (rc == DDAGPU_OK) e = launch_step_advance(c->step_dev, st);
-        if (rc == DDAGPU_OK && e == cudaSuccess) rc = top(max_step, c->step_dev);
-        if (rc == DDAGPU_OK && e == cudaSuccess)
-            e = launch_loop_control(c->active, nrhs, c->step_dev, max_step, h, st);
-        if (rc != DDAGPU_OK || e != cudaSuccess) return give_up(rc, e, "body");
-        e = cudaStreamEndCapture(st, &t);
-        if (e != cudaSuccess) return give_up(DDAGPU_OK, e, "end body capture");
-        const long long n_body = c->launches - l1 + 2;
-        // phase 3: rollback and post-processing after the loop
-        const long long l2 = c->launches;
-        e = cudaStreamBeginCaptureToGraph(st, g, &cn, nullptr, 1, cudaStreamCaptureModeThreadLocal);
-        if (e != cudaSuccess) return give_up(DDAGPU_OK, e, "tail capture");
-        FieldArgs F = fa_args(c, nrhs, nmat1, d0, tau);
-        e = launch_scalar(c->state, nullptr, nullptr, nrhs, SC_FINAL, 0, nullptr, 0, st);
-        if (e == cudaSuccess) e = launch_gated_copy(F, 1, st);
-        if (e == cudaSuccess) rc = post();
-        if (rc != DDAGPU_OK || e != cudaSuccess) return give_up(rc, e, "tail");
-        e = cudaStreamEndCapture(st, &t);
-        if (e != cudaSuccess) return give_up(DDAGPU_OK, e, "end tail capture");
-        const long long n_tail = c->launches - l2 + 2;
-        cudaGraphExec_t x = nullptr;
-        e = cudaGraphInstantiate(&x, g, 0);
-        if (e != cudaSuccess) return give_up(DDAGPU_OK, e, "instantiate");
-        c->wgraph = g;
-        c->wexec = x;
-        c->wkey = key;
-        c->w_fixed = n_head + n_tail;
-        c->w_per_iter = n_body;
-        c->w_matvec0 = res.matvec0;
-        c->w_matvec_it = res.matvec_it;
-    }
-    c->launches = l_before;
-    CK(cudaGraphLaunch(c->wexec, st));
+        if (cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone) {
+            cudaGraph_t t = nullptr;
+            cudaStreamEndCapture(st, &t);
+            if (t && t != g) cudaGraphDestroy(t);
+        }
+        c->launches = l_save;
+        if (rc != DDAGPU_OK) return rc;
+        return fail(DDAGPU_ECUDA, std::string("solve graph (") + what + "): " + cudaGetErrorString(e));
+    };
+    cudaGraphConditionalHandle h;
+    cudaError_t e = cudaGraphConditionalHandleCreate(&h, g, 0, 0);
+    if (e != cudaSuccess) return give_up(DDAGPU_OK, e, "handle");
+    const long long l0 = c->launches;
+    // phase 1: fresh state, step 0, the convergence test of step 1, the loop condition
+    e = cudaStreamBeginCaptureToGraph(st, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return give_up(DDAGPU_OK, e, "capture");
+    int rc = DDAGPU_OK;
+    e = launch_init_state(c->state, c->active, nrhs, (double)err_max, c->nact_dev, st);
+    if (e == cudaSuccess) rc = step0();
+    if (rc == DDAGPU_OK && e == cudaSuccess) e = launch_step_set(c->step_dev, 1, st);
+    if (rc == DDAGPU_OK && e == cudaSuccess) rc = top(max_step, c->step_dev);
+    if (rc == DDAGPU_OK && e == cudaSuccess)
+        e = launch_loop_control(c->active, nrhs, c->step_dev, max_step, h, st);
+    if (rc != DDAGPU_OK || e != cudaSuccess) return give_up(rc, e, "step 0");
+    cudaStreamCaptureStatus cs;
+    const cudaGraphNode_t *deps = nullptr;
+    size_t ndeps = 0;
+    e = cudaStreamGetCaptureInfo(st, &cs, nullptr, nullptr, &deps, &ndeps);
+    if (e != cudaSuccess) return give_up(DDAGPU_OK, e, "capture info");
+    std::vector<cudaGraphNode_t> leaves(deps, deps + ndeps);
+    cudaGraph_t t = nullptr;
+    e = cudaStreamEndCapture(st, &t);
+    if (e != cudaSuccess) return give_up(DDAGPU_OK, e, "end capture");
+    const long long n_head = c->launches - l0 + 3;   // + init, step set, loop control
+    // the while node and its body: one iteration, the next step's test, the condition
+    cudaGraphNodeParams np{};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = h;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    cudaGraphNode_t cn;
+    e = cudaGraphAddNode(&cn, g, leaves.data(), leaves.size(), &np);
+    if (e != cudaSuccess) return give_up(DDAGPU_OK, e, "while node");
+    const long long l1 = c->launches;
+    e = cudaStreamBeginCaptureToGraph(st, np.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                      cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return give_up(DDAGPU_OK, e, "body capture");
+    rc = body(max_step, c->step_dev, true);
+    if (rc == DDAGPU_OK) e = launch_step_advance(c->step_dev, st);
+    if (rc == DDAGPU_OK && e == cudaSuccess) rc = top(max_step, c->step_dev);
+    if (rc == DDAGPU_OK && e == cudaSuccess)
+        e = launch_loop_control(c->active, nrhs, c->step_dev, max_step, h, st);
+    if (rc != DDAGPU_OK || e != cudaSuccess) return give_up(rc, e, "body");
+    e = cudaStreamEndCapture(st, &t);
+    if (e != cudaSuccess) return give_up(DDAGPU_OK, e, "end body capture");
+    const long long n_body = c->launches - l1 + 2;
+    // phase 3: rollback and post-processing after the loop
+    const long long l2 = c->launches;
+    e = cudaStreamBeginCaptureToGraph(st, g, &cn, nullptr, 1, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return give_up(DDAGPU_OK, e, "tail capture");
+    FieldArgs F = fa_args(c, nrhs, nmat1, d0, tau);
+    e = launch_scalar(c->state, nullptr, nullptr, nrhs, SC_FINAL, 0, nullptr, 0, st);
+    if (e == cudaSuccess) e = launch_gated_copy(F, 1, st);
+    if (e == cudaSuccess) rc = post();
+    if (rc != DDAGPU_OK || e != cudaSuccess) return give_up(rc, e, "tail");
+    e = cudaStreamEndCapture(st, &t);
+    if (e != cudaSuccess) return give_up(DDAGPU_OK, e, "end tail capture");
+    const long long n_tail = c->launches - l2 + 2;
+    n_fixed = n_head + n_tail;
+    n_per_iter = n_body;
+    c->launches = l_save;
+    return DDAGPU_OK;
+}
+
+// Device results of a launched whole solve (on the context's stream): the solver states,
+// the last step and the bounded-wait flag; counts the launched kernels.
+int read_whole_solve(ddagpu_ctx *c, int nrhs, SolveResult &res, long long n_fixed, long long n_per_iter,
+                     int matvec0, int matvec_it)
+{
+    cudaStream_t st = c->st;
     int last = 1;
     res.st.resize((size_t)nrhs);
     CK(cudaMemcpyAsync(res.st.data(), c->state, nrhs * sizeof(RhsState), cudaMemcpyDeviceToHost, st));
@@ -427,11 +425,73 @@ int run_whole_graph(ddagpu_ctx *c, int nrhs, int solver, float tau, int max_step
     CK(cudaMemcpyAsync(&werr, c->err_dev, sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     RET(device_wait_error(c, werr));
-    c->launches += c->w_fixed + (long long)(last - 1) * c->w_per_iter;
-    res.matvec0 = c->w_matvec0;
-    res.matvec_it = c->w_matvec_it;
+    c->launches += n_fixed + (long long)(last - 1) * n_per_iter;
+    res.matvec0 = matvec0;
+    res.matvec_it = matvec_it;
     c->graph_runs += 1;
     return DDAGPU_OK;
+}
+
+// A whole solve prepared for a group's graph instead of being launched (see ddagpu_group):
+// the inputs are uploaded and the solve's graph key is returned; with graph set, the solve
+// is also recorded into it as an independent branch.
+struct GroupRecord {
+    cudaGraph_t graph = nullptr;
+    ddagpu_ctx::GraphKey key{};
+    long long n_fixed = 0, n_per_iter = 0;
+    int matvec0 = 0, matvec_it = 0;
+};
+
+template <class Step0, class Top, class Body>
+int run_whole_graph(ddagpu_ctx *c, int nrhs, int solver, float tau, int max_step, float err_max,
+                    int nmat1, double d0, int nact, const int *nact_per, SolveResult &res,
+                    Step0 &step0, Top &top, Body &body, const std::function<int()> &post,
+                    GroupRecord *rec)
+{
+    cudaStream_t st = c->st;
+    std::vector<int> na((size_t)nrhs);
+    for (int k = 0; k < nrhs; k++) na[(size_t)k] = nact_per ? nact_per[k] : nact;
+    CK(cudaMemcpyAsync(c->nact_dev, na.data(), nrhs * sizeof(int), cudaMemcpyHostToDevice, st));
+    const ddagpu_ctx::GraphKey key = whole_key(c, nrhs, solver, tau, max_step, err_max, nmat1, d0);
+    if (rec) {   // for the group's graph; the group launches it and reads the results
+        rec->key = key;
+        if (!rec->graph) return DDAGPU_OK;
+        RET(record_whole_solve(c, rec->graph, nrhs, max_step, err_max, nmat1, d0, tau, step0, top, body,
+                               post, rec->n_fixed, rec->n_per_iter));
+        rec->matvec0 = res.matvec0;
+        rec->matvec_it = res.matvec_it;
+        return DDAGPU_OK;
+    }
+    if (!c->wexec || std::memcmp(&key, &c->wkey, sizeof key) != 0) {
+        if (c->wexec) cudaGraphExecDestroy(c->wexec);
+        if (c->wgraph) cudaGraphDestroy(c->wgraph);
+        c->wexec = nullptr;
+        c->wgraph = nullptr;
+        cudaGraph_t g = nullptr;
+        CK(cudaGraphCreate(&g, 0));
+        long long nf = 0, npi = 0;
+        const int rc = record_whole_solve(c, g, nrhs, max_step, err_max, nmat1, d0, tau, step0, top, body,
+                                          post, nf, npi);
+        if (rc != DDAGPU_OK) {
+            cudaGraphDestroy(g);
+            return rc;
+        }
+        cudaGraphExec_t x = nullptr;
+        const cudaError_t e = cudaGraphInstantiate(&x, g, 0);
+        if (e != cudaSuccess) {
+            cudaGraphDestroy(g);
+            return fail(DDAGPU_ECUDA, std::string("solve graph (instantiate): ") + cudaGetErrorString(e));
+        }
+        c->wgraph = g;
+        c->wexec = x;
+        c->wkey = key;
+        c->w_fixed = nf;
+        c->w_per_iter = npi;
+        c->w_matvec0 = res.matvec0;
+        c->w_matvec_it = res.matvec_it;
+    }
+    CK(cudaGraphLaunch(c->wexec, st));
+    return read_whole_solve(c, nrhs, res, c->w_fixed, c->w_per_iter, c->w_matvec0, c->w_matvec_it);
 }
 
 // post (may be null): kernels issued after the solve on the context's stream (far field,
@@ -440,7 +500,7 @@ int run_whole_graph(ddagpu_ctx *c, int nrhs, int solver, float tau, int max_step
 int run_solver(ddagpu_ctx *c, int nrhs, int solver, float tau, int max_step, float err_max,
                int nmat1, double d0, int nact, SolveResult &res, bool want_trace,
                const float2 *rhs_in = nullptr, const int *nact_per = nullptr,
-               const std::function<int()> *post = nullptr)
+               const std::function<int()> *post = nullptr, GroupRecord *rec = nullptr)
 {
     if (solver < 0 || solver > 3) return fail(DDAGPU_EINVAL, "solver must be 0..3");
     if (max_step < 0) return fail(DDAGPU_EINVAL, "Max_Step must be >= 0");
@@ -455,7 +515,8 @@ int run_solver(ddagpu_ctx *c, int nrhs, int solver, float tau, int max_step, flo
     }
     double *trace = want_trace ? c->trace : nullptr;
     const int tlen = want_trace ? tl : 0;
-    const bool whole = post && c->graph_on && !want_trace && !rhs_in;
+    const bool whole = post && (c->graph_on || rec) && !want_trace && !rhs_in;
+    if (rec && !whole) return fail(DDAGPU_EINVAL, "a group records whole batched solves only");
     if (!whole) {
         std::vector<RhsState> init((size_t)nrhs);
         for (int k = 0; k < nrhs; k++) {
@@ -605,7 +666,7 @@ int run_solver(ddagpu_ctx *c, int nrhs, int solver, float tau, int max_step, flo
         return DDAGPU_OK;
     };
     if (whole) return run_whole_graph(c, nrhs, solver, tau, max_step, err_max, nmat1, d0, nact,
-                                      nact_per, res, step0, top, body, *post);
+                                      nact_per, res, step0, top, body, *post, rec);
     RET(step0());
     // iteration 1 (and all of them without the graph) from the host: the loop stops when
     // no right-hand side is left active (read back once per iteration)
@@ -1215,6 +1276,44 @@ int ensure_occ_batch(ddagpu_ctx *c)
     return DDAGPU_OK;
 }
 
+// Rasterises realisations r0 .. r0 + no of a monomer list into the context's batch
+// occupancy (both polarisations of realisation k at right-hand sides 2k, 2k + 1) and
+// returns their dipole counts (ndip, may be null) and active cells per right-hand side.
+int agglomerate_rasterize(ddagpu_ctx *c, const BatchGeom &g, const float *monomers, const int *counts,
+                          const std::vector<size_t> &first, int r0, int no, int *ndip,
+                          std::vector<int> &nact)
+{
+    const size_t N = c->N;
+    for (int k = 0; k < no; k++) {
+        const int r = r0 + k;
+        const size_t need = anthrax_scratch_bytes(counts[r]);
+        if (need > c->worm_bytes) {   // grow the context's monomer buffer (stream-ordered)
+            CK(cudaStreamSynchronize(c->st));
+            cudaFree(c->worm_buf);
+            c->worm_buf = nullptr;
+            c->worm_bytes = 0;
+            CK(cudaMalloc(&c->worm_buf, need));
+            c->worm_bytes = need;
+        }
+        CK(anthrax_rasterize(monomers + 13 * first[(size_t)r], counts[r], c->ni, c->nj, c->nl,
+                             c->occ_b + 2 * k * N, c->ndip + k, c->st, c->worm_buf, c->worm_bytes));
+        CK(cudaMemcpyAsync(c->occ_b + (2 * k + 1) * N, c->occ_b + 2 * k * N, N,
+                           cudaMemcpyDeviceToDevice, c->st));
+        c->launches += 1;
+    }
+    std::vector<int> nd((size_t)no, 0);
+    CK(cudaMemcpyAsync(nd.data(), c->ndip, no * sizeof(int), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    nact.assign((size_t)2 * no, 0);
+    for (int k = 0; k < no; k++) {
+        if (ndip) ndip[r0 + k] = nd[(size_t)k];
+        nact[2 * k] = nact[2 * k + 1] = g.mv[1] ? nd[(size_t)k] : 0;
+        if (nact[2 * k] == 0) return fail(DDAGPU_EINVAL, "a realisation has no active dipoles");
+    }
+    return DDAGPU_OK;
+}
+
+
 // Per-right-hand-side occupancy (c->occ_b) for the lifetime of the guard.
 struct OccBatch {
     ddagpu_ctx *c;
@@ -1235,31 +1334,77 @@ int ensure_pin(ddagpu_ctx *c, size_t bytes)
     return DDAGPU_OK;
 }
 
+// Offsets of a batched chunk's pinned staging: inputs kin, ein, ks, nv (double), al
+// (float2); outputs ca, ce (float), mo (double); every block 16-byte aligned.
+struct ChunkLayout {
+    size_t n_kin, n_ein, n_ks, n_nv, n_al, n_mo;
+    size_t o_ein, o_ks, o_nv, o_al, o_ca, o_ce, o_mo, total;
+    ChunkLayout(int no, int ndir, int nP, int nA, int nmat1)
+    {
+        auto al16 = [](size_t b) { return (b + 15) & ~(size_t)15; };
+        const size_t nr = 2 * (size_t)no;
+        n_kin = nr * 3;
+        n_ein = nr * 6;
+        n_ks = nr * ndir * 3;
+        n_nv = (size_t)no * nP * 3;
+        n_al = nr * nmat1;
+        n_mo = (size_t)no * nA * 16;
+        o_ein = al16(n_kin * 8);
+        o_ks = o_ein + al16(n_ein * 8);
+        o_nv = o_ks + al16(n_ks * 8);
+        o_al = o_nv + al16(n_nv * 8);
+        o_ca = o_al + al16(n_al * 8);
+        o_ce = o_ca + al16(nr * 4);
+        o_mo = o_ce + al16(nr * 4);
+        total = o_mo + al16(n_mo * 8);
+    }
+};
+
+// Results of a solved chunk: reads the outputs on the context's stream into cabs / cext /
+// mueller (this chunk's first orientation) and the batch statistics.
+int batch_chunk_finish(ddagpu_ctx *c, const BatchGeom &g, int no, const SolveResult &res,
+                       double *cabs, double *cext, double *mueller, ddagpu_batch_info &bi)
+{
+    const int nr = 2 * no;
+    const ChunkLayout Lc(no, g.ndir, g.nP, g.nA, g.nmat1);
+    float *ca = (float *)(c->pin + Lc.o_ca), *ce = (float *)(c->pin + Lc.o_ce);
+    double *mo = (double *)(c->pin + Lc.o_mo);
+    CK(cudaMemcpyAsync(ca, c->cabs, nr * sizeof(float), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaMemcpyAsync(ce, c->cext, nr * sizeof(float), cudaMemcpyDeviceToHost, c->st));
+    if (mueller) CK(cudaMemcpyAsync(mo, c->mueller, Lc.n_mo * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    for (int o = 0; o < no; o++) {
+        if (cabs) cabs[o] = 0.5 * ca[(size_t)2 * o] + 0.5 * ca[(size_t)2 * o + 1];
+        if (cext) cext[o] = 0.5 * ce[(size_t)2 * o] + 0.5 * ce[(size_t)2 * o + 1];
+    }
+    if (mueller) std::memcpy(mueller, mo, Lc.n_mo * sizeof(double));
+    bi.n_rhs += nr;
+    for (const RhsState &S : res.st) {
+        bi.max_steps = std::max(bi.max_steps, S.steps);
+        bi.rolled_back += S.restored;
+        bi.max_err = std::max(bi.max_err, S.restored ? S.err_min : S.err);
+    }
+    return DDAGPU_OK;
+}
+
 // Solves no orientations (rotation matrices rot[no][9]) as 2 no right-hand sides -- both
 // incident polarisations, x and y before rotation (main.cpp:153-154) -- whose occupancy is
 // on the device, then far fields, cross sections and the Mueller matrices averaged over the
 // planes (main.cpp:870-949).  cabs / cext / mueller point at this chunk's first orientation.
+// With rec the chunk is only prepared (inputs uploaded, solve recorded into rec's graph if
+// it has one) for a group launch; the group then calls batch_chunk_finish.
 int batch_chunk(ddagpu_ctx *c, const ddagpu_batch_cfg *cfg, const BatchGeom &g, const double *rot,
                 int no, int nact, const int *nact_per, double *cabs, double *cext, double *mueller,
-                ddagpu_batch_info &bi)
+                ddagpu_batch_info &bi, GroupRecord *rec = nullptr)
 {
     const int nr = 2 * no, ndir = g.ndir, nP = g.nP, nA = g.nA, nmat1 = g.nmat1;
     const double d0 = c->kd;
-    // pinned layout: inputs kin, ein, ks, nv (double), al (float2); outputs ca, ce (float),
-    // mo (double); every block 16-byte aligned
-    auto al16 = [](size_t b) { return (b + 15) & ~(size_t)15; };
-    const size_t n_kin = (size_t)nr * 3, n_ein = (size_t)nr * 6, n_ks = (size_t)nr * ndir * 3,
-                 n_nv = (size_t)no * nP * 3, n_al = (size_t)nr * nmat1, n_mo = (size_t)no * nA * 16;
-    const size_t o_ein = al16(n_kin * 8), o_ks = o_ein + al16(n_ein * 8), o_nv = o_ks + al16(n_ks * 8),
-                 o_al = o_nv + al16(n_nv * 8), o_ca = o_al + al16(n_al * 8), o_ce = o_ca + al16((size_t)nr * 4),
-                 o_mo = o_ce + al16((size_t)nr * 4), total = o_mo + al16(n_mo * 8);
-    RET(ensure_pin(c, total));
-    double *kin = (double *)c->pin, *ein = (double *)(c->pin + o_ein), *ks = (double *)(c->pin + o_ks),
-           *nv = (double *)(c->pin + o_nv);
-    float2 *al = (float2 *)(c->pin + o_al);
-    float *ca = (float *)(c->pin + o_ca), *ce = (float *)(c->pin + o_ce);
-    double *mo = (double *)(c->pin + o_mo);
-    std::memset(c->pin, 0, o_ca);
+    const ChunkLayout Lc(no, ndir, nP, nA, nmat1);
+    RET(ensure_pin(c, Lc.total));
+    double *kin = (double *)c->pin, *ein = (double *)(c->pin + Lc.o_ein), *ks = (double *)(c->pin + Lc.o_ks),
+           *nv = (double *)(c->pin + Lc.o_nv);
+    float2 *al = (float2 *)(c->pin + Lc.o_al);
+    std::memset(c->pin, 0, Lc.o_ca);
     for (int o = 0; o < no; o++) {
         const double *T = rot + 9 * (size_t)o;
         auto R = [&](const double *v, double *out) {
@@ -1288,11 +1433,11 @@ int batch_chunk(ddagpu_ctx *c, const ddagpu_batch_cfg *cfg, const BatchGeom &g, 
         }
         for (int pl = 0; pl < nP; pl++) R(g.nrm0.data() + 3 * pl, nv + ((size_t)o * nP + pl) * 3);
     }
-    CK(cudaMemcpyAsync(c->kinc, kin, n_kin * sizeof(double), cudaMemcpyHostToDevice, c->st));
-    CK(cudaMemcpyAsync(c->einc, ein, n_ein * sizeof(double), cudaMemcpyHostToDevice, c->st));
-    CK(cudaMemcpyAsync(c->ksc, ks, n_ks * sizeof(double), cudaMemcpyHostToDevice, c->st));
-    CK(cudaMemcpyAsync(c->normals, nv, n_nv * sizeof(double), cudaMemcpyHostToDevice, c->st));
-    CK(cudaMemcpyAsync(c->alpha, al, n_al * sizeof(float2), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->kinc, kin, Lc.n_kin * sizeof(double), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->einc, ein, Lc.n_ein * sizeof(double), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->ksc, ks, Lc.n_ks * sizeof(double), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->normals, nv, Lc.n_nv * sizeof(double), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->alpha, al, Lc.n_al * sizeof(float2), cudaMemcpyHostToDevice, c->st));
     SolveResult res;
     // far field, cross sections and the plane-averaged Mueller matrices, after the solve
     // (recorded with it when the solve is one graph launch)
@@ -1305,23 +1450,9 @@ int batch_chunk(ddagpu_ctx *c, const ddagpu_batch_cfg *cfg, const BatchGeom &g, 
     };
     c->post_key = ((long long)ndir << 40) | ((long long)no << 24) | ((long long)nP << 12) | nA;
     RET(run_solver(c, nr, cfg->solver, cfg->tau, cfg->max_step, cfg->err_max, nmat1, d0, nact, res,
-                   false, nullptr, nact_per, &post));
-    CK(cudaMemcpyAsync(ca, c->cabs, nr * sizeof(float), cudaMemcpyDeviceToHost, c->st));
-    CK(cudaMemcpyAsync(ce, c->cext, nr * sizeof(float), cudaMemcpyDeviceToHost, c->st));
-    if (mueller) CK(cudaMemcpyAsync(mo, c->mueller, n_mo * sizeof(double), cudaMemcpyDeviceToHost, c->st));
-    CK(cudaStreamSynchronize(c->st));
-    for (int o = 0; o < no; o++) {
-        if (cabs) cabs[o] = 0.5 * ca[(size_t)2 * o] + 0.5 * ca[(size_t)2 * o + 1];
-        if (cext) cext[o] = 0.5 * ce[(size_t)2 * o] + 0.5 * ce[(size_t)2 * o + 1];
-    }
-    if (mueller) std::memcpy(mueller, mo, n_mo * sizeof(double));
-    bi.n_rhs += nr;
-    for (const RhsState &S : res.st) {
-        bi.max_steps = std::max(bi.max_steps, S.steps);
-        bi.rolled_back += S.restored;
-        bi.max_err = std::max(bi.max_err, S.restored ? S.err_min : S.err);
-    }
-    return DDAGPU_OK;
+                   false, nullptr, nact_per, &post, rec));
+    if (rec) return DDAGPU_OK;
+    return batch_chunk_finish(c, g, no, res, cabs, cext, mueller, bi);
 }
 
 }  // namespace
@@ -1452,7 +1583,7 @@ int refine_loop(ddagpu_ctx *c, int solver, float rTau, int nmat1, double d0, int
 // c->b32.  Leaves float(x) in c->p.
 int mixed_refine(ddagpu_ctx *c, const float *cListMaterials, int nmat1, int nact, double d0,
                  const double *kinc, const double *einc, bool from_b32, double Error_max,
-                 int max_outer, int inner_max_step, ddagpu_refine_info &ri)
+                 int max_outer, double inner_rel, int inner_max_step, ddagpu_refine_info &ri)
 {
     if (!c->mcg) c->mcg = new MixedCgBuffers();
     CK(c->mcg->ensure(3 * c->N));
@@ -1467,7 +1598,7 @@ int mixed_refine(ddagpu_ctx *c, const float *cListMaterials, int nmat1, int nact
         return launch_matvec(mv_args(c, 1, src, out, 0, 0.f, nullptr, 0, nmat1, false), c->st);
     };
     MixedCgResult R;
-    CK(mixed_cg(*c->mcg, f, al.data(), nmat1, nact, Error_max, max_outer, inner_max_step,
+    CK(mixed_cg(*c->mcg, f, al.data(), nmat1, nact, Error_max, max_outer, inner_rel, inner_max_step,
                 conv, c->s, c->w, c->rb, c->p, c->st, R, &c->launches));
     std::memset(&ri, 0, sizeof ri);
     ri.outer = R.outer;
@@ -1534,7 +1665,7 @@ int ddagpu_solve_linear(ddagpu_ctx *c, int solver, float rTau, const float *cLis
     std::memset(&ri, 0, sizeof ri);
     if (refine && solver == 0) {
         RET(mixed_refine(c, cListMaterials, nmat1, nact, c->kd, nullptr, nullptr, true, Error_max,
-                         max_step, inner_max_step, ri));
+                         max_step, inner_rel, inner_max_step, ri));
     } else if (refine) {
         RhsState S0;
         std::memset(&S0, 0, sizeof S0);
@@ -1608,7 +1739,7 @@ int ddagpu_dda_fft_refined(ddagpu_ctx *c, int solver, float rTau, const float *c
     double err = 0.0;
     if (solver == 0) {
         RET(mixed_refine(c, cListMaterials, nmat1, nact, d0, kd3, ed6, false, Error_max, max_outer,
-                         inner_max_step, ri));
+                         inner_rel, inner_max_step, ri));
     } else {
         // outer right-hand side b = p_inc (FirstApproximation), x = b
         {
@@ -2158,36 +2289,11 @@ int ddagpu_agglomerate_solves(ddagpu_ctx *c, const ddagpu_batch_cfg *cfg, int n_
     CK(cudaMemcpyAsync(c->mv, g.mv.data(), g.nmat1 * sizeof(int), cudaMemcpyHostToDevice, c->st));
     const int per = c->cap / 2;
     ddagpu_batch_info bi{0, 0, 0, 0.0};
-    std::vector<int> nact, nd;
+    std::vector<int> nact;
     std::vector<double> rots;
     for (int o0 = 0; o0 < n_real; o0 += per) {
         const int no = std::min(per, n_real - o0);
-        for (int k = 0; k < no; k++) {
-            const int r = o0 + k;
-            const size_t need = anthrax_scratch_bytes(counts[r]);
-            if (need > c->worm_bytes) {   // grow the context's monomer buffer (stream-ordered)
-                CK(cudaStreamSynchronize(c->st));
-                cudaFree(c->worm_buf);
-                c->worm_buf = nullptr;
-                c->worm_bytes = 0;
-                CK(cudaMalloc(&c->worm_buf, need));
-                c->worm_bytes = need;
-            }
-            CK(anthrax_rasterize(monomers + 13 * first[(size_t)r], counts[r], c->ni, c->nj, c->nl,
-                                 c->occ_b + 2 * k * N, c->ndip + k, c->st, c->worm_buf, c->worm_bytes));
-            CK(cudaMemcpyAsync(c->occ_b + (2 * k + 1) * N, c->occ_b + 2 * k * N, N,
-                               cudaMemcpyDeviceToDevice, c->st));
-            c->launches += 1;
-        }
-        nd.assign((size_t)no, 0);
-        CK(cudaMemcpyAsync(nd.data(), c->ndip, no * sizeof(int), cudaMemcpyDeviceToHost, c->st));
-        CK(cudaStreamSynchronize(c->st));
-        nact.assign((size_t)2 * no, 0);
-        for (int k = 0; k < no; k++) {
-            if (ndip) ndip[o0 + k] = nd[(size_t)k];
-            nact[2 * k] = nact[2 * k + 1] = g.mv[1] ? nd[(size_t)k] : 0;
-            if (nact[2 * k] == 0) return fail(DDAGPU_EINVAL, "a realisation has no active dipoles");
-        }
+        RET(agglomerate_rasterize(c, g, monomers, counts, first, o0, no, ndip, nact));
         batch_rotations(rot, o0, no, rots);
         OccBatch ob(c);
         RET(batch_chunk(c, cfg, g, rots.data(), no, 0, nact.data(), cabs ? cabs + o0 : nullptr,
@@ -2195,6 +2301,190 @@ int ddagpu_agglomerate_solves(ddagpu_ctx *c, const ddagpu_batch_cfg *cfg, int n_
                         mueller ? mueller + (size_t)o0 * g.nA * 16 : nullptr, bi));
     }
     if (info) *info = bi;
+    return DDAGPU_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------- groups of contexts
+// Lattices of different sizes solved as ONE graph launch: every member context's whole
+// batched solve is an independent branch of one graph (its state set-up, step 0, its own
+// conditional while loop, rollback, far field and Mueller matrices), recorded once per
+// solve shape and replayed.  The members' inputs are uploaded on their own streams, which
+// the group's stream waits for before the launch; the members' streams wait for the
+// launch before the results are read.
+struct ddagpu_group {
+    std::vector<ddagpu_ctx *> ctx;
+    int dev = 0;
+    cudaStream_t st = nullptr;
+    std::vector<cudaEvent_t> ev;          // one per member: its inputs are uploaded
+    cudaEvent_t done = nullptr;           // the launch has finished
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<char> used;               // members with a branch in the graph
+    std::vector<ddagpu_ctx::GraphKey> keys;
+    std::vector<long long> gens;
+    std::vector<GroupRecord> rec;         // per member: kernel counts of its branch
+    long long runs = 0;
+    std::mutex mu;
+};
+
+
+extern "C" {
+
+int ddagpu_group_create(ddagpu_group **out, ddagpu_ctx *const *ctxs, int nctx)
+{
+    if (!out || !ctxs || nctx < 1) return fail(DDAGPU_EINVAL, "null or bad argument");
+    *out = nullptr;
+    for (int k = 0; k < nctx; k++) {
+        if (!ctxs[k]) return fail(DDAGPU_EINVAL, "null context");
+        if (ctxs[k]->dev != ctxs[0]->dev) return fail(DDAGPU_EINVAL, "group members on different devices");
+        for (int q = 0; q < k; q++)
+            if (ctxs[q] == ctxs[k]) return fail(DDAGPU_EINVAL, "a context appears twice in the group");
+    }
+    DevGuard dg(ctxs[0]->dev);
+    ddagpu_group *g = new ddagpu_group();
+    g->ctx.assign(ctxs, ctxs + nctx);
+    g->dev = ctxs[0]->dev;
+    g->ev.assign((size_t)nctx, nullptr);
+    cudaError_t e = cudaStreamCreateWithFlags(&g->st, cudaStreamNonBlocking);
+    for (int k = 0; k < nctx && e == cudaSuccess; k++)
+        e = cudaEventCreateWithFlags(&g->ev[(size_t)k], cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&g->done, cudaEventDisableTiming);
+    if (e != cudaSuccess) {
+        ddagpu_group_destroy(g);
+        return fail(DDAGPU_ECUDA, std::string("group set-up: ") + cudaGetErrorString(e));
+    }
+    *out = g;
+    return DDAGPU_OK;
+}
+
+int ddagpu_group_destroy(ddagpu_group *g)
+{
+    if (!g) return DDAGPU_OK;
+    DevGuard dg(g->dev);
+    if (g->st) cudaStreamSynchronize(g->st);
+    if (g->exec) cudaGraphExecDestroy(g->exec);
+    if (g->graph) cudaGraphDestroy(g->graph);
+    for (cudaEvent_t e : g->ev)
+        if (e) cudaEventDestroy(e);
+    if (g->done) cudaEventDestroy(g->done);
+    if (g->st) cudaStreamDestroy(g->st);
+    delete g;
+    return DDAGPU_OK;
+}
+
+long long ddagpu_group_graph_runs(ddagpu_group *g) { return g ? g->runs : -1; }
+
+int ddagpu_group_agglomerate_solves(ddagpu_group *grp, const ddagpu_batch_cfg *cfg, const int *n_real,
+                                    const float *const *monomers, const int *const *counts,
+                                    const double *const *rot, double *const *cabs, double *const *cext,
+                                    double *const *mueller, int *const *ndip, ddagpu_batch_info *info)
+{
+    if (!grp || !cfg || !n_real || !monomers || !counts) return fail(DDAGPU_EINVAL, "null or bad argument");
+    const int nctx = (int)grp->ctx.size();
+    std::lock_guard<std::mutex> glk(grp->mu);
+    std::vector<std::unique_lock<std::mutex>> locks;
+    std::vector<BatchGeom> geo((size_t)nctx);
+    std::vector<std::vector<double>> rots((size_t)nctx);
+    std::vector<std::vector<int>> nact((size_t)nctx);
+    std::vector<char> used((size_t)nctx, 0);
+    for (int k = 0; k < nctx; k++) {
+        ddagpu_ctx *c = grp->ctx[(size_t)k];
+        RET(batch_check(c, cfg));
+        if (cfg->n_mat != 1) return fail(DDAGPU_EINVAL, "agglomerates are one material (n_mat = 1)");
+        if (n_real[k] < 0 || n_real[k] > c->cap / 2)
+            return fail(DDAGPU_EINVAL, "a member's realisations exceed its max_rhs / 2 (one batch per member)");
+        used[(size_t)k] = n_real[k] > 0;
+        for (int r = 0; r < n_real[k]; r++)
+            if (counts[k][r] < 0) return fail(DDAGPU_EINVAL, "negative monomer count");
+    }
+    for (int k = 0; k < nctx; k++) locks.emplace_back(grp->ctx[(size_t)k]->mu);
+    DevGuard dg(grp->dev);
+    std::vector<ddagpu_batch_info> bi((size_t)nctx, ddagpu_batch_info{0, 0, 0, 0.0});
+    // ---- inputs of every member on its own stream, and the key of its solve
+    std::vector<GroupRecord> rec((size_t)nctx);
+    for (int k = 0; k < nctx; k++) {
+        if (!used[(size_t)k]) continue;
+        ddagpu_ctx *c = grp->ctx[(size_t)k];
+        const int no = n_real[k];
+        std::vector<size_t> first((size_t)no + 1, 0);
+        for (int r = 0; r < no; r++) first[(size_t)r + 1] = first[(size_t)r] + (size_t)counts[k][r];
+        if (first[(size_t)no] && !monomers[k]) return fail(DDAGPU_EINVAL, "null monomers");
+        BatchGeom &g = geo[(size_t)k];
+        RET(batch_setup(c, cfg, g));
+        RET(ensure_occ_batch(c));
+        CK(cudaMemcpyAsync(c->mv, g.mv.data(), g.nmat1 * sizeof(int), cudaMemcpyHostToDevice, c->st));
+        RET(agglomerate_rasterize(c, g, monomers[k], counts[k], first, 0, no, ndip ? ndip[k] : nullptr,
+                                  nact[(size_t)k]));
+        batch_rotations(rot ? rot[k] : nullptr, 0, no, rots[(size_t)k]);
+        OccBatch ob(c);
+        RET(batch_chunk(c, cfg, g, rots[(size_t)k].data(), no, 0, nact[(size_t)k].data(), nullptr, nullptr,
+                        nullptr, bi[(size_t)k], &rec[(size_t)k]));
+    }
+    // ---- the group's graph: rebuilt when a member's solve shape or buffers change
+    bool rebuild = !grp->exec || grp->used != used;
+    for (int k = 0; k < nctx && !rebuild; k++)
+        if (used[(size_t)k] && (std::memcmp(&rec[(size_t)k].key, &grp->keys[(size_t)k], sizeof(ddagpu_ctx::GraphKey)) ||
+                                grp->gens[(size_t)k] != grp->ctx[(size_t)k]->gen))
+            rebuild = true;
+    if (rebuild) {
+        if (grp->exec) cudaGraphExecDestroy(grp->exec);
+        if (grp->graph) cudaGraphDestroy(grp->graph);
+        grp->exec = nullptr;
+        grp->graph = nullptr;
+        cudaGraph_t G = nullptr;
+        CK(cudaGraphCreate(&G, 0));
+        int rc = DDAGPU_OK;
+        for (int k = 0; k < nctx && rc == DDAGPU_OK; k++) {
+            if (!used[(size_t)k]) continue;
+            ddagpu_ctx *c = grp->ctx[(size_t)k];
+            rec[(size_t)k].graph = G;
+            OccBatch ob(c);
+            rc = batch_chunk(c, cfg, geo[(size_t)k], rots[(size_t)k].data(), n_real[k], 0, nact[(size_t)k].data(),
+                             nullptr, nullptr, nullptr, bi[(size_t)k], &rec[(size_t)k]);
+        }
+        cudaGraphExec_t x = nullptr;
+        const cudaError_t e = rc == DDAGPU_OK ? cudaGraphInstantiate(&x, G, 0) : cudaSuccess;
+        if (rc != DDAGPU_OK || e != cudaSuccess) {
+            cudaGraphDestroy(G);
+            if (rc != DDAGPU_OK) return rc;
+            return fail(DDAGPU_ECUDA, std::string("group graph (instantiate): ") + cudaGetErrorString(e));
+        }
+        grp->graph = G;
+        grp->exec = x;
+        grp->used = used;
+        grp->keys.assign((size_t)nctx, ddagpu_ctx::GraphKey{});
+        grp->gens.assign((size_t)nctx, 0);
+        grp->rec = rec;
+        for (int k = 0; k < nctx; k++) {
+            grp->keys[(size_t)k] = rec[(size_t)k].key;
+            grp->gens[(size_t)k] = grp->ctx[(size_t)k]->gen;
+            grp->rec[(size_t)k].graph = nullptr;
+        }
+    }
+    // ---- one launch for every member
+    for (int k = 0; k < nctx; k++) {
+        if (!used[(size_t)k]) continue;
+        CK(cudaEventRecord(grp->ev[(size_t)k], grp->ctx[(size_t)k]->st));
+        CK(cudaStreamWaitEvent(grp->st, grp->ev[(size_t)k], 0));
+    }
+    CK(cudaGraphLaunch(grp->exec, grp->st));
+    CK(cudaEventRecord(grp->done, grp->st));
+    grp->runs += 1;
+    for (int k = 0; k < nctx; k++) {
+        if (!used[(size_t)k]) continue;
+        ddagpu_ctx *c = grp->ctx[(size_t)k];
+        CK(cudaStreamWaitEvent(c->st, grp->done, 0));
+        SolveResult res;
+        const GroupRecord &R = grp->rec[(size_t)k];
+        RET(read_whole_solve(c, 2 * n_real[k], res, R.n_fixed, R.n_per_iter, R.matvec0, R.matvec_it));
+        RET(batch_chunk_finish(c, geo[(size_t)k], n_real[k], res, cabs ? cabs[k] : nullptr,
+                               cext ? cext[k] : nullptr, mueller ? mueller[k] : nullptr, bi[(size_t)k]));
+        c->graph_runs -= 1;   // the launch is the group's
+    }
+    if (info)
+        for (int k = 0; k < nctx; k++) info[k] = bi[(size_t)k];
     return DDAGPU_OK;
 }
 

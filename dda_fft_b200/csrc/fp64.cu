@@ -915,7 +915,7 @@ cudaError_t f64_right_hand_side(const Field64View &f, double d0, const double *k
 }
 
 cudaError_t mixed_cg(MixedCgBuffers &B, const Field64View &f, const double2 *alpha_host, int nmat1,
-                     int nact, double err_max, int max_outer, int inner_max_step,
+                     int nact, double err_max, int max_outer, double inner_rel, int inner_max_step,
                      const ConvFn &conv, float2 *s32, float2 *conv32, float2 *x32, float2 *p32,
                      cudaStream_t st, MixedCgResult &R, long long *launches)
 {
@@ -946,7 +946,7 @@ cudaError_t mixed_cg(MixedCgBuffers &B, const Field64View &f, const double2 *alp
     double err = 0;
     CKE(true_residual(err));
     R.history[0] = err;
-    double err_best = err;
+    double err_best = err, anchor = err;
     CKE(cudaMemcpyAsync(B.best, B.x, bytes, cudaMemcpyDeviceToDevice, st));
     if (err > err_max) {
         CKE(cudaMemcpyAsync(B.s, B.r, bytes, cudaMemcpyDeviceToDevice, st));
@@ -974,7 +974,7 @@ cudaError_t mixed_cg(MixedCgBuffers &B, const Field64View &f, const double2 *alp
             *launches += 2;
             R.iterations++;
             since++;
-            if (err_rec <= err_max || since >= inner_max_step) {
+            if (err_rec <= err_max || err_rec <= inner_rel * anchor || since >= inner_max_step) {
                 CKE(true_residual(err));
                 R.outer++;
                 if (R.outer < 64) R.history[R.outer] = err;
@@ -983,6 +983,11 @@ cudaError_t mixed_cg(MixedCgBuffers &B, const Field64View &f, const double2 *alp
                     CKE(cudaMemcpyAsync(B.best, B.x, bytes, cudaMemcpyDeviceToDevice, st));
                 }
                 if (err <= err_max || R.outer >= max_outer) break;
+                // restart from the current solution: fresh direction s = r (true residual)
+                CKE(cudaMemcpyAsync(B.s, B.r, bytes, cudaMemcpyDeviceToDevice, st));
+                to_f32<<<red, kT, 0, st>>>(B.s, s32, n3);
+                *launches += 1;
+                anchor = err;
                 since = 0;
             }
         }

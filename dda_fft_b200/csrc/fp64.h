@@ -71,15 +71,17 @@ cudaError_t f64_right_hand_side(const Field64View &f, double d0, const double *k
                                 const double *einc, const float2 *from_f32, double2 *out,
                                 cudaStream_t st);
 
-// The reference's CG (COCG, dda_func.cpp:1137-1138, 1359-1371) with FP64 fields, FP64
-// scalars (no float casts) and FP64 true residuals, every convolution on the FP32 FFT
-// passes.  The recursively updated residual is replaced by the true one b - (x - alpha
-// G*x) only when it claims convergence (meets Error_max) or after inner_max_step
-// iterations since the last replacement; the search direction is kept, so the Krylov
-// space is never thrown away.  Replacing more often (every tenfold drop) made the
-// iteration unstable below a relative residual of about 1e-5 on a 128^3 sphere at x = 16;
-// replacing only at convergence claims reached 1e-8 there.  Stops when a true residual
-// meets Error_max or after max_outer replacements; the best true-residual iterate is kept.
+// Iterative refinement whose inner solver is the reference's CG (COCG, dda_func.cpp:
+// 1137-1138, 1359-1371) with FP64 fields and FP64 scalars (no float casts), every
+// convolution on the FP32 FFT passes.  The true residual b - (x - alpha G*x) is computed
+// when the updated residual has fallen to inner_rel times the last true one, meets
+// Error_max, or after inner_max_step iterations; unless it meets Error_max, CG restarts
+// from the current FP64 solution with the true residual (a fresh search direction).
+// Restarting matters: the FP64 reductions sum in a varying order, so runs differ in their
+// last bits, and COCG's occasional near-breakdown steps (very large coefficients) can
+// then inject FP32 matvec error far above the residual; keeping the old direction after
+// such a step made the iteration diverge, a restart does not.  Stops when a true residual
+// meets Error_max or after max_outer outer steps; the best true-residual iterate is kept.
 struct MixedCgBuffers {
     size_t n3 = 0;
     double2 *x = nullptr, *r = nullptr, *s = nullptr, *w = nullptr, *b = nullptr, *best = nullptr,
@@ -102,7 +104,7 @@ using ConvFn = std::function<cudaError_t(const float2 *src, float2 *out)>;
 // B.b holds the FP64 right-hand side; f.alpha must point at B.alpha (filled from
 // alpha_host); three float buffers of 3N are scratch.  Leaves x in B.x and float(x) in p32.
 cudaError_t mixed_cg(MixedCgBuffers &B, const Field64View &f, const double2 *alpha_host, int nmat1,
-                     int nact, double err_max, int max_outer, int inner_max_step,
+                     int nact, double err_max, int max_outer, double inner_rel, int inner_max_step,
                      const ConvFn &conv, float2 *s32, float2 *conv32, float2 *x32, float2 *p32,
                      cudaStream_t st, MixedCgResult &R, long long *launches);
 

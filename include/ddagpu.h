@@ -94,11 +94,12 @@ int ddagpu_dda_fft(ddagpu_ctx *ctx, int iNoIllumination, int iMode_SolutionMetho
  * mean true residual norm (the reference's discrepancy, dda_func.cpp:784-811, of the true
  * instead of the recursively updated residual) is <= Error_max, or after max_outer outer
  * steps; info reports the true residual of every outer step.  Outputs as ddagpu_dda_fft.
- *   iMode_SolutionMethod 0 (CG): the reference's CG recurrences (dda_func.cpp:1359-1371)
- *     run with FP64 fields and FP64 scalars, never restarted; an outer step replaces the
- *     updated residual by the true one when the updated one meets Error_max, or after
- *     inner_max_step iterations (inner_rel is not used).  Reaches a discrepancy near 1e-8
- *     on a 128^3 sphere at x = 16, m = 1.6+0.0005i.
+ *   iMode_SolutionMethod 0 (CG): the inner solver is the reference's CG (dda_func.cpp:
+ *     1359-1371) with FP64 fields and FP64 scalars; an outer step computes the true
+ *     residual when the updated one has fallen to inner_rel x the last true one, meets
+ *     Error_max, or after inner_max_step iterations, and restarts CG from the current FP64
+ *     solution.  Reaches a discrepancy near 1e-8 on a 128^3 sphere at x = 16,
+ *     m = 1.6+0.0005i (inner_rel 1e-3).
  *   1..3: each outer step solves A d = r in FP32 with that solver (restarted from d = r, to
  *     inner_rel x the current residual, at most inner_max_step iterations, best iterate
  *     kept) and adds d to p. */
@@ -214,6 +215,27 @@ int ddagpu_agglomerate_solves(ddagpu_ctx *ctx, const ddagpu_batch_cfg *cfg, int 
                               const float *monomers, const int *counts, const double *rot,
                               double *cabs, double *cext, double *mueller, int *ndip,
                               ddagpu_batch_info *info);
+
+/* Groups: contexts of different lattice sizes on one device whose batched agglomerate
+ * solves run as ONE graph launch per call -- the sample loop of main.cpp:806-985 for
+ * realisations whose lattices differ (main.cpp:812-858), each lattice with its own Green
+ * tensor (main.cpp:466-486).  Member k's whole solve (state set-up, step 0, its iterations
+ * as a conditional while node, rollback, far field, cross sections, Mueller matrices) is an
+ * independent branch of the group's graph, recorded once per solve shape and replayed; the
+ * members' inputs are uploaded on their own streams first.  No counterpart in the reference.
+ * A context may belong to several groups and still be used on its own; calls lock every
+ * member.  Per-member arrays are indexed by member: n_real[k] (0 leaves member k out;
+ * at most max_rhs / 2 of that member), monomers[k], counts[k] as ddagpu_agglomerate_solves,
+ * rot[k] (or rot == NULL: fixed orientation), outputs cabs[k], cext[k], mueller[k], ndip[k]
+ * (each array of pointers may be NULL) and info[k]. */
+typedef struct ddagpu_group ddagpu_group;
+int ddagpu_group_create(ddagpu_group **grp, ddagpu_ctx *const *ctxs, int nctx);
+int ddagpu_group_destroy(ddagpu_group *grp);
+long long ddagpu_group_graph_runs(ddagpu_group *grp);   /* group graph launches so far */
+int ddagpu_group_agglomerate_solves(ddagpu_group *grp, const ddagpu_batch_cfg *cfg, const int *n_real,
+                                    const float *const *monomers, const int *const *counts,
+                                    const double *const *rot, double *const *cabs, double *const *cext,
+                                    double *const *mueller, int *const *ndip, ddagpu_batch_info *info);
 
 /* Number of scattering angles for a configuration (rounding of main.cpp:201). */
 int ddagpu_num_angles(float theta_min, float theta_max, float theta_step);

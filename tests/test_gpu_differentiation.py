@@ -7,10 +7,12 @@
   test_gpu_fp64.py).
 * The FP64 gradient against central finite differences (step 1e-3 on Re m and Im m) at 32
   seeded dipoles.  A dipole's share of Cabs is about 1e-5 of it, so a difference of 1e-3
-  in m moves the observables by about 1e-8 relative: each perturbed solve is FP64, to a
-  discrepancy of 1e-16 (about 4e-13 of the dipoles' size), and starts from the unperturbed
-  solution, so it computes only the change the perturbation makes.  The perturbed dipole
-  becomes a material of its own, as a per-dipole reference would do (main.cpp:645-677).
+  in m moves the observables by about 1e-8 relative, below what a full solve resolves.
+  Each perturbed system (m_k -> m_k +- h, a material of its own as a per-dipole reference
+  would do, main.cpp:645-677) is therefore solved exactly as p + d: with A p = b the
+  converged FP64 solution, A' (p + d) = b' gives A' d = (a'_k - a_k) p_k / a_k at cell k
+  alone (b - A p, the same for both signs, cancels in the central difference), and d is
+  an FP64 solve to 1e-10 of its own right-hand side.
 * The cost: the adjoint pass (any combination of the observables) takes at most 2.5x the
   forward pass, in matvecs and in time."""
 import time
@@ -42,7 +44,7 @@ def _grads(P, B, m):
 def setup():
     filled, m = porous_target(64, seed=11)
     P = Problem(filled, kd=2 * 5.0 / 64, model="cmrr")
-    F = GPUFP64Backend(P, err_max=1e-16)
+    F = GPUFP64Backend(P, err_max=1e-13)
     f64, g64 = _grads(P, F, m)
     yield P, m, F, f64, g64
     F.close()
@@ -77,8 +79,14 @@ def test_fp64_gradient_matches_central_differences_64(setup):
                 mm = m.copy()
                 mm[k] += sgn * step
                 occ_k, table_k, a_k, _ = P.tables(mm)
-                p = [F.solve(occ_k, table_k, P.pinc(a_k, q), x0=base[q]) for q in range(2)]
-                assert F.last_err <= 1e-15
+                p = []
+                for q in range(2):
+                    rhs = np.zeros((P.ndip, 3), complex)
+                    rhs[k] = (a_k[k] - a[k]) * base[q][k] / a[k]
+                    err0 = np.linalg.norm(rhs[k]) / P.ndip          # its discrepancy
+                    d = F.solve(occ_k, table_k, rhs, err_max=1e-10 * err0)
+                    assert F.last_err <= 1e-10 * err0
+                    p.append(base[q] + d)
                 cabs, m11, _ = P.observables(p, a_k)
                 vals.append((cabs, m11))
             fd[part] = (np.array(vals[0]) - np.array(vals[1])) / (2 * h)
@@ -88,7 +96,7 @@ def test_fp64_gradient_matches_central_differences_64(setup):
                 scale = max(abs(fd[part, obs]), np.abs(g64[obs][part]).max() * 1e-3)
                 err = abs(adj - fd[part, obs]) / scale
                 worst = max(worst, err)
-                assert err < 1e-3, (k, obs, part, adj, fd[part, obs])
+                assert err < 1e-4, (k, obs, part, adj, fd[part, obs])
     print(f"32 dipoles: FP64 adjoint vs central differences, worst {worst:.2e} of the scale")
 
 

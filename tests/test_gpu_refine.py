@@ -22,7 +22,7 @@ def test_refined_solve_matches_fp64_oracle(oracle, n, x, solver):
     kd, occ, alpha, ksc = _setup(oracle, n, x, m)
     with D.Context(n, kd) as ctx:
         r = ctx.dda_fft_refined(occ, alpha, [0, 1], kd, (0, 0, 1), (1, 0, 0), ksc, solver=solver,
-                                err_max=1e-7, max_outer=30, inner_rel=0.05)
+                                err_max=1e-7, max_outer=30)
     assert r["err"] <= 1e-7, r["history"]
     o = oracle.dda_fft(occ, alpha, [0, 1], kd, (0, 0, 1), (1, 0, 0), oracle.green_hat(n, n, n, kd),
                        ksc, solver=solver, max_step=2000, err_max=1e-10)
