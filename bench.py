@@ -661,8 +661,9 @@ def realizations_run(args):
     """The realisation half of the batching configuration: every realisation is placed on
     the host (the reference's float geometry, one thread per realisation), rasterised on
     the GPU into the batch of its lattice size and solved for both polarisations; the three
-    lattice sizes run concurrently, one context and stream each.  value: the GPU part
-    (monomer lists to Mueller matrices); e2e: placement included."""
+    lattice sizes are one group (ddagpu_group), so a step is one graph launch with a branch
+    per lattice.  value: the GPU part (monomer lists to Mueller matrices); e2e: placement
+    included."""
     from concurrent.futures import ThreadPoolExecutor
     sizes = agglomerate_sizes()
     if args.impl == "reference":
@@ -690,33 +691,30 @@ def realizations_run(args):
         c.autotune(2 * len(groups[n]))
     cfg = D.BatchConfig(occ=None, materials=[MAT])
     pool = ThreadPoolExecutor(max_workers=os.cpu_count() or 4)
+    members = sorted(ctxs)
+    grp = D.Group([ctxs[n] for n in members])
 
     def place(step, k):
         n = sizes[k]
         return D.Agglomerate(SEED, step * AGG_N + k).place(n, AGG_R, AGG_R * AGG_LR, counts[n])
 
-    def solve_group(n, mons):
-        return ctxs[n].agglomerate_solves(cfg, mons)
-
     def step_device(mons):
-        """the three lattice sizes concurrently, monomers already placed"""
-        futs = {n: pool.submit(solve_group, n, [mons[k] for k in g]) for n, g in groups.items() if g}
-        return {n: f.result() for n, f in futs.items()}
+        """one graph launch for the three lattice sizes, monomers already placed"""
+        res = grp.agglomerate_solves(cfg, [[mons[k] for k in groups[n]] for n in members])
+        return dict(zip(members, res))
 
     def step_e2e(step):
-        def group(n, g):
-            mons = list(pool.map(lambda k: place(step, k), g))
-            return solve_group(n, mons)
-        # the largest lattices first: their placement is the longest
-        with ThreadPoolExecutor(max_workers=len(groups)) as gp:
-            futs = {n: gp.submit(group, n, g) for n, g in sorted(groups.items(), reverse=True) if g}
-            return {n: f.result() for n, f in futs.items()}
+        # the largest lattices' realisations first: their placement is the longest
+        order = sorted(range(AGG_N), key=lambda k: -sizes[k])
+        placed_now = dict(zip(order, pool.map(lambda k: place(step, k), order)))
+        return step_device(placed_now)
 
     placed = [list(pool.map(lambda k: place(s, k), range(AGG_N))) for s in range(W + K)]
     for s in range(W):
         step_device(placed[s])
     clk = ClockSampler(0)
     launches0 = sum(c.kernel_launches for c in ctxs.values())
+    runs0 = grp.graph_runs
     torch.cuda.synchronize()
     clk.start()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -729,6 +727,7 @@ def realizations_run(args):
     torch.cuda.synchronize()
     clocks = clk.stop()
     launches = sum(c.kernel_launches for c in ctxs.values()) - launches0
+    graph_launches = grp.graph_runs - runs0
     ms = e0.elapsed_time(e1)
     value = K * AGG_N / (ms / 1000.0)
     t0 = time.perf_counter()
@@ -775,6 +774,7 @@ def realizations_run(args):
         "steps": K, "warmup": W, "ms_per_step": ms / K, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": AGG_WORKLOAD, "groups": info,
+                   "graph_launches_per_step": graph_launches / K,
                    "l2": "working set per step >> L2 (126 MB): no flush needed"},
         "e2e": {"value": e2e, "unit": "realization-solves/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "includes": "host placement of every realisation"},
@@ -783,6 +783,7 @@ def realizations_run(args):
                      "peak_source": src, "traffic": None, "ms_per_launch": mv_ms,
                      "rhs_per_launch": nrhs, "kernels": "specialised" if ctx.fast_kernels else "generic"},
         "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches}), flush=True)
+    grp.close()
     for c in ctxs.values():
         c.close()
     pool.shutdown()

@@ -186,17 +186,25 @@ class GPUFP64Backend:
         self.matvecs = 0
         self.last_err = 0.0
 
-    def solve(self, occ, table, rhs_dipoles, x0=None, err_max=None):
+    def solve(self, occ, table, rhs_dipoles, x0=None, err_max=None, restart_every=None,
+              restarts=0):
+        """With restart_every, CG runs at most that many steps at a time and restarts from
+        its best iterate (a fresh search direction), up to `restarts` times: COCG can
+        stagnate after a near-breakdown step, and a restart resets that."""
         mv = np.array([0] + [1] * (len(table) - 1), np.int32)
-        r = self.ctx.solve_fp64(occ, table, mv, self.P.kd, self.P.kinc, self.P.einc[0], None,
-                                solver=self.solver, max_step=self.max_step,
-                                err_max=self.err_max if err_max is None else err_max,
-                                rhs=self.P.field(rhs_dipoles),
-                                x0=None if x0 is None else self.P.field(x0), want_p=True,
-                                trace=False)
-        self.matvecs += r["matvecs"]
-        self.last_err = min(r["err"], r["err_min"])
-        return r["p"][tuple(self.P.idx.T)]
+        target = self.err_max if err_max is None else err_max
+        steps = self.max_step if restart_every is None else restart_every
+        x = None if x0 is None else self.P.field(x0)
+        for _ in range(restarts + 1):
+            r = self.ctx.solve_fp64(occ, table, mv, self.P.kd, self.P.kinc, self.P.einc[0], None,
+                                    solver=self.solver, max_step=steps, err_max=target,
+                                    rhs=self.P.field(rhs_dipoles), x0=x, want_p=True, trace=False)
+            self.matvecs += r["matvecs"]
+            self.last_err = min(r["err"], r["err_min"])
+            x = r["p"]
+            if self.last_err <= target:
+                break
+        return x[tuple(self.P.idx.T)]
 
     def close(self):
         self.ctx.close()
