@@ -435,10 +435,10 @@ def profile_matvec(args):
 def precision_run(args):
     """The precision configuration: 128^3 sphere, x = 16, m = 1.6+0.0005i, theta 0..180 step
     2, both polarisations.  The FP64 reference is the FP64 GPU solve (the reference's CG in
-    double, to a discrepancy of 1e-9); beside it: the plain float BiCGStab (the reference's
+    double, to a discrepancy of 3e-10); beside it: the plain float BiCGStab (the reference's
     method, Error_max 1e-5, 100 steps), the FP64 BiCGStab (which diverges on this system),
     and the precision pattern -- FP32 FFT matvec, FP64 fields, residuals and test -- at the
-    configuration's Error_max 1e-5 and at 1e-8.  Errors of Cext, Cabs (averaged over the two
+    configuration's Error_max 1e-5, at 1e-8 and at 1e-9.  Errors of Cext, Cabs (averaged over the two
     polarisations) and of the Mueller matrix against the FP64 solve; one JSON line."""
     import dda_fft_b200 as D
     n, x, m = 128, 16.0, complex(1.6, 0.0005)
@@ -455,7 +455,7 @@ def precision_run(args):
                                np.asarray(esc[0]).reshape(1, -1, 3), np.asarray(esc[1]).reshape(1, -1, 3))
         t0 = time.perf_counter()
         ref = [ctx.solve_fp64(occ, alpha.astype(np.complex128), [0, 1], kd, (0, 0, 1), e, ksc, solver=0,
-                              max_step=10000, err_max=1e-9, trace=False) for e in E]
+                              max_step=12000, err_max=3e-10, trace=False) for e in E]
         out["fp64_cg"] = {"seconds": time.perf_counter() - t0, "steps": [r["steps"] for r in ref],
                           "err": [r["err"] for r in ref]}
         b64 = ctx.solve_fp64(occ, alpha.astype(np.complex128), [0, 1], kd, (0, 0, 1), E[0], None, solver=2,
@@ -479,10 +479,10 @@ def precision_run(args):
                              err_max=1e-5) for e in E]
         out["plain_float_bicgstab"] = {"seconds": time.perf_counter() - t0,
                                        "err_min": [r["err_min"] for r in plain], **errors(plain)}
-        for em in (1e-5, 1e-8):
+        for em in (1e-5, 1e-8, 1e-9):
             t0 = time.perf_counter()
             res = [ctx.dda_fft_refined(occ, alpha, [0, 1], kd, (0, 0, 1), e, ksc[None], solver=0,
-                                       err_max=em, max_outer=20) for e in E]
+                                       err_max=em, max_outer=30) for e in E]
             out[f"mixed_cg_{em:g}"] = {"seconds": time.perf_counter() - t0,
                                        "iterations": [r["inner_steps"] for r in res],
                                        "matvecs": [r["matvecs"] for r in res],

@@ -4,7 +4,7 @@
 orientation, one scattering plane, theta 0..180 deg step 2, both incident polarisations.
 
 The FP64 reference is ddagpu_solve_fp64 running the reference's CG (COCG) recurrences with
-every field, FFT and scalar in double, to a discrepancy of 1e-9 -- validated against the
+every field, FFT and scalar in double, to a discrepancy of 3e-10 -- validated against the
 reference's own FP64 build in test_gpu_fp64.py.  (The configuration names BiCGStab; the
 reference's BiCGStab diverges on this system even in FP64 -- its discrepancy falls to 3e-4
 and then grows without bound -- so it cannot give the reference answer.)
@@ -12,7 +12,7 @@ and then grows without bound -- so it cannot give the reference answer.)
 The measured path is the precision pattern: every convolution on the FP32 FFT passes,
 fields, scalars, residuals and the Error_max test in FP64 (ddagpu_dda_fft_refined, CG).
 Its errors in Cext, Cabs and all 16 Mueller elements against the FP64 solve are printed at
-the configuration's Error_max 1e-5, at 1e-8 and at 3e-9, and gated at 3e-9: Cext and Cabs
+the configuration's Error_max 1e-5, at 1e-8 and at 1e-9, and gated at 1e-9: Cext and Cabs
 to 1e-4 relative, every Mueller element to 1e-4 of M11 at the same angle (the error of the
 normalised matrix M_ij / M11; eight elements vanish by symmetry for a sphere, so an
 element's own magnitude is no scale).  The pointwise relative error of the significant
@@ -58,14 +58,14 @@ def test_precision_config_128_against_fp64_solve(oracle):
     ksc = np.stack([np.sin(th), np.zeros_like(th), np.cos(th)], 1)
     with D.Context(n, kd, max_rhs=2) as ctx:
         ref = [ctx.solve_fp64(occ, alpha.astype(np.complex128), [0, 1], kd, (0, 0, 1), e, ksc, solver=0,
-                              max_step=10000, err_max=1e-9, trace=False) for e in E]
+                              max_step=12000, err_max=3e-10, trace=False) for e in E]
         ctx.release_fp64()
         for r in ref:
-            assert r["err"] <= 1e-9 and not r["rolled_back"]
+            assert r["err"] <= 3e-10 and not r["rolled_back"]
         res = {}
-        for em in (1e-5, 1e-8, 3e-9):
+        for em in (1e-5, 1e-8, 1e-9):
             out = [ctx.dda_fft_refined(occ, alpha, [0, 1], kd, (0, 0, 1), e, ksc[None], solver=0,
-                                       err_max=em, max_outer=20) for e in E]
+                                       err_max=em, max_outer=30) for e in E]
             for o in out:
                 assert o["err"] <= em, o["history"]
             res[em] = errors(oracle, ksc, ref, out)
@@ -74,6 +74,6 @@ def test_precision_config_128_against_fp64_solve(oracle):
                   f"(significant values: median {res[em]['mueller_sig_median']:.2e}, "
                   f"max {res[em]['mueller_sig_max']:.2e})  iterations {[o['inner_steps'] for o in out]}")
             print("  per element:", np.array2string(res[em]["mueller_el"], precision=1))
-    e9 = res[3e-9]
+    e9 = res[1e-9]
     assert e9["cext"] < 1e-4 and e9["cabs"] < 1e-4
     assert e9["mueller_el"].max() < 1e-4
