@@ -119,7 +119,7 @@ struct ddagpu_ctx {
     int graph_on = 1;
     int *step_dev = nullptr;
     struct GraphKey {
-        int solver, nrhs, max_step, nmat1, fast, fx, fyz, tile_x, rows_g, tlen;
+        int solver, nrhs, max_step, nmat1, fast, fx, fyz, tile_x, rows_g, tlen, pair;
         float tau, err_max;
         double d0;
         size_t occ_stride;
@@ -142,6 +142,7 @@ struct ddagpu_ctx {
     Fp64Buffers *f64 = nullptr;  // FP64 solve buffers (ddagpu_solve_fp64), built on first use
     MixedCgBuffers *mcg = nullptr;   // FP64 fields of the mixed-precision CG refinement
     long long gen = 0;           // bumped whenever recorded graphs must be dropped
+    int pair_step0 = 0;          // step 0 of a batched call: polarisation pairs share phi
     long long g_per_iter = 0;    // kernels in one recorded iteration
     long long graph_runs = 0;    // graph launches by this context
     std::mutex mu;
@@ -323,6 +324,7 @@ ddagpu_ctx::GraphKey whole_key(ddagpu_ctx *c, int nrhs, int solver, float tau, i
     key.trace = nullptr;
     key.occ = c->occ_stride ? (const void *)c->occ_b : (const void *)c->occ;
     key.post = c->post_key;
+    key.pair = c->pair_step0;
     return key;
 }
 
@@ -554,6 +556,7 @@ int run_solver(ddagpu_ctx *c, int nrhs, int solver, float tau, int max_step, flo
         CK(launch_inc_tables(F, c->inc_tab, st));
         MatvecArgs m = mv_args(c, nrhs, c->p, c->r, 1, 0.f, nullptr, 0, nmat1, true);
         m.inc = 1;
+        m.pair = (c->pair_step0 && nrhs % 2 == 0) ? 1 : 0;
         m.inc_tab = c->inc_tab;
         m.einc = c->einc;
         m.inc_out = c->p;
@@ -1449,8 +1452,17 @@ int batch_chunk(ddagpu_ctx *c, const ddagpu_batch_cfg *cfg, const BatchGeom &g, 
         return DDAGPU_OK;
     };
     c->post_key = ((long long)ndir << 40) | ((long long)no << 24) | ((long long)nP << 12) | nA;
-    RET(run_solver(c, nr, cfg->solver, cfg->tau, cfg->max_step, cfg->err_max, nmat1, d0, nact, res,
-                   false, nullptr, nact_per, &post, rec));
+    // both polarisations of every orientation with the same polarisabilities (every model
+    // but LDR): step 0 transforms one scalar field per orientation (MatvecArgs::pair)
+    bool same = true;
+    for (int o = 0; o < no && same; o++)
+        same = std::memcmp(al + (size_t)2 * o * nmat1, al + (size_t)(2 * o + 1) * nmat1,
+                           nmat1 * sizeof(float2)) == 0;
+    c->pair_step0 = same ? 1 : 0;
+    const int rc = run_solver(c, nr, cfg->solver, cfg->tau, cfg->max_step, cfg->err_max, nmat1, d0, nact,
+                              res, false, nullptr, nact_per, &post, rec);
+    c->pair_step0 = 0;
+    RET(rc);
     if (rec) return DDAGPU_OK;
     return batch_chunk_finish(c, g, no, res, cabs, cext, mueller, bi);
 }

@@ -75,6 +75,11 @@ struct MatvecArgs {
     // computes its input p = alpha_m exp(i k.(r - c)) E_inc on active cells (0 elsewhere)
     // from the occupancy and materials of ep instead of reading src, and writes it to inc_out
     int inc;
+    // with inc: right-hand sides 2k, 2k+1 are the two polarisations of one orientation with
+    // the same polarisabilities, so p_inc = phi(r) E_q with one scalar phi = alpha_m
+    // exp(i k.(r - c)); the forward passes transform phi once per pair (into component slot
+    // 0 of right-hand side 2k) and the x pass forms G * (phi E_q) for both polarisations
+    int pair;
     const float2 *inc_tab;  // [nrhs][nj + nl + ni] phase tables (y, z, x)
     const double *einc;     // [nrhs][6] incident field
     float2 *inc_out;        // [nrhs][3][N]

@@ -84,15 +84,20 @@ DDA_DEV void row_fft_from_regs(float2 *row, int lane_sub, bool valid, float2 (&v
 // ------------------------------------------------------------------------------ K1
 // CTA (i, component, z half hl): z-forward of the NJ rows of plane i (half hl only), then
 // y-forward of the NL columns for both y halves; writes work rows in split order.
-// INC: the input is the incident field, computed here (and written by the hl = 0 CTAs).
-template <int NJ, int NL, int NT, bool INC>
+// IM 1: the input is the incident field, computed here (and written by the hl = 0 CTAs).
+// IM 2: incident field of a polarisation pair (MatvecArgs::pair): CTA (i, hl, pair k)
+// transforms phi = alpha_m exp(i k.(r - c)) into component slot 0 of right-hand side 2k
+// and writes p = phi E_q of both polarisations.
+template <int NJ, int NL, int NT, int IM>
 __global__ void __launch_bounds__(NT) k1f(MatvecArgs a)
 {
     using SJ = Sp<NJ>;
     using SL = Sp<NL>;
     constexpr int PS = SL::PS;
+    constexpr bool INC = IM != 0, PAIR = IM == 2;
     extern __shared__ float2 Z[];   // [NJ][PS]
-    const int hl = blockIdx.x & 1, i = blockIdx.x >> 1, c = blockIdx.y, rhs = blockIdx.z;
+    const int hl = blockIdx.x & 1, i = blockIdx.x >> 1, c = blockIdx.y;
+    const int rhs = PAIR ? 2 * (int)blockIdx.z : (int)blockIdx.z;
     if (a.rhs_active && !a.rhs_active[rhs]) return;
     const int ni = a.L.ni;
     const float2 *src = a.src + (size_t)rhs * a.fstride + ((size_t)c * ni + i) * (NJ * NL);
@@ -116,6 +121,14 @@ __global__ void __launch_bounds__(NT) k1f(MatvecArgs a)
         for (int r = 0; r < (tz_reg ? R1 : 1); r++) tz[r] = sub < R2 ? tab[NJ + sub + R2 * r] : czero();
         const double *E = a.einc + 6 * rhs;
         const float2 Ef = make_float2((float)E[2 * c], (float)E[2 * c + 1]);
+        float2 Ep[2][3];   // pair: the incident fields of both polarisations
+        if constexpr (PAIR) {
+#pragma unroll
+            for (int q = 0; q < 2; q++)
+#pragma unroll
+                for (int k = 0; k < 3; k++)
+                    Ep[q][k] = make_float2((float)E[6 * q + 2 * k], (float)E[6 * q + 2 * k + 1]);
+        }
         const signed char *ob = ep.occ + (size_t)rhs * ep.occ_stride + (size_t)i * NJ * NL;
         const float2 *al = ep.alpha + (size_t)rhs * ep.nmat1;
         // up to two materials from registers
@@ -147,8 +160,22 @@ __global__ void __launch_bounds__(NT) k1f(MatvecArgs a)
                     const bool act = rt ? ((m & 1) ? mv1 : mv0) : ep.mv[m] != 0;
                     float2 val = czero();
                     const float2 tzr = tz_reg ? tz[tz_reg ? r : 0] : __ldg(&tab[NJ + sub + R2 * r]);
-                    if (act) val = cmul(cmul(cmul(txy, tzr), rt ? ((m & 1) ? al1 : al0) : al[m]), Ef);
-                    if (hl == 0) pout[row * NL + sub + R2 * r] = val;
+                    if constexpr (PAIR) {
+                        // val = phi; the dipoles phi E_q of both polarisations, the same
+                        // float operations as the single form's ((phi) E_c)
+                        if (act) val = cmul(cmul(txy, tzr), rt ? ((m & 1) ? al1 : al0) : al[m]);
+                        if (hl == 0) {
+                            const size_t o = (size_t)row * NL + sub + R2 * r;
+#pragma unroll
+                            for (int q = 0; q < 2; q++)
+#pragma unroll
+                                for (int k = 0; k < 3; k++)
+                                    pout[q * a.fstride + (size_t)k * ni * (NJ * NL) + o] = cmul(val, Ep[q][k]);
+                        }
+                    } else {
+                        if (act) val = cmul(cmul(cmul(txy, tzr), rt ? ((m & 1) ? al1 : al0) : al[m]), Ef);
+                        if (hl == 0) pout[row * NL + sub + R2 * r] = val;
+                    }
                     v[r] = hl ? cmul(val, __ldg(&hwl[sub + R2 * r])) : val;
                 }
             }
@@ -583,6 +610,161 @@ __global__ void __launch_bounds__(Sp<NI>::RM * TL, k2_min_blocks(NI, Sp<NI>::RM 
     }
 }
 
+// Pair form of the x pass (MatvecArgs::pair, step 0): CTA (spectral row js, TL spectral
+// columns, polarisation pair k).  The forward transform of phi (component slot 0 of
+// right-hand side 2k) is done once; then for each polarisation q the spectrum G (E_q phi)
+// is formed -- the product of the single form with v = E_q phi -- inverse-transformed and
+// written to the three component slots of right-hand side 2k + q.  Shared B[c][h][pos][t]
+// with c = 0..2 the output components and c = 3 the spectrum of phi.
+template <int NI, int TL>
+__global__ void __launch_bounds__(Sp<NI>::RM * TL, k2_min_blocks(NI, Sp<NI>::RM * TL)) k2p(MatvecArgs a)
+{
+    using S = Sp<NI>;
+    constexpr int R1 = S::R1, R2 = S::R2;
+    static_assert(R2 > 1, "the pair form needs a two-step line FFT");
+    extern __shared__ __align__(128) float2 B[];   // [4][2][NI][TL]
+    constexpr bool rhs_fast = k2_rhs_fastest(NI);
+    const int js = rhs_fast ? blockIdx.z : blockIdx.x, pr = rhs_fast ? blockIdx.x : blockIdx.z;
+    const int rhs0 = 2 * pr;
+    if (a.rhs_active && !a.rhs_active[rhs0]) return;
+    const int nj = a.L.nj, nl = a.L.nl;
+    const int l0 = blockIdx.y * TL;
+    const int t = threadIdx.x % TL, sub = threadIdx.x / TL;
+    const size_t plane = (size_t)(2 * nj) * (2 * nl), cstr = (size_t)NI * plane;
+    const size_t col = (size_t)js * (2 * nl) + l0 + t;
+    const float2 *tw = a.L.tw_i, *hw = a.L.tw_i + NI;
+    auto Bat = [&](int c, int h, int pos) -> float2 & { return B[((c * 2 + h) * NI + pos) * TL + t]; };
+
+    // ---- forward step A of phi, both halves from one load
+    if (sub < R2) {
+        const float2 *src = a.work + (size_t)rhs0 * a.wstride + col;
+        float2 v[R1], w[R1];
+#pragma unroll
+        for (int r = 0; r < R1; r++) v[r] = src[(size_t)(sub + R2 * r) * plane];
+#pragma unroll
+        for (int r = 0; r < R1; r++) w[r] = cmul(v[r], __ldg(&hw[sub + R2 * r]));
+        dft_reg<R1, false>(v);
+        dft_reg<R1, false>(w);
+#pragma unroll
+        for (int k1 = 0; k1 < R1; k1++) {
+            const float2 tk = k1 ? twid<false>(tw, sub * k1) : make_float2(1.f, 0.f);
+            Bat(3, 0, sub + R2 * k1) = k1 ? cmul(v[k1], tk) : v[k1];
+            Bat(3, 1, sub + R2 * k1) = k1 ? cmul(w[k1], tk) : w[k1];
+        }
+    }
+    __syncthreads();
+    // ---- forward step B of phi, in place: lane k1 keeps frequencies k1 + R1 q at R2 k1 + q
+    if (sub < R1) {
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            float2 X[R2];
+#pragma unroll
+            for (int q = 0; q < R2; q++) X[q] = Bat(3, h, R2 * sub + q);
+            dft_reg<R2, false>(X);
+#pragma unroll
+            for (int q = 0; q < R2; q++) Bat(3, h, R2 * sub + q) = X[q];
+        }
+    }
+    __syncthreads();
+
+    const int hj = js >= nj, kj = js - hj * nj, jp = 2 * kj + hj;
+    const int my = jp > nj, oy = my ? 2 * nj - jp : jp;
+    const int ls = l0 + t, hl = ls >= nl, kl = ls - hl * nl, lp = 2 * kl + hl;
+    const int mz = lp > nl, oz = mz ? 2 * nl - lp : lp;
+    const size_t sz = 6, sy = (size_t)(nl + 1) * 6, sxo = (size_t)(nj + 1) * sy;
+    const float2 *Ayz = a.ahat + (size_t)oy * sy + (size_t)zmapf(oz, nl) * sz;
+#pragma unroll 1
+    for (int pol = 0; pol < 2; pol++) {
+        const double *E = a.einc + 6 * (rhs0 + pol);
+        const float2 Ex = make_float2((float)E[0], (float)E[1]), Ey = make_float2((float)E[2], (float)E[3]),
+                     Ez = make_float2((float)E[4], (float)E[5]);
+        // ---- product with the Green tensor, inverse step A (transposed split)
+        if (sub < R1) {
+            const int k1 = sub;
+#pragma unroll 1
+            for (int h = 0; h < 2; h++) {
+                float2 X[3][R2];
+#pragma unroll
+                for (int q = 0; q < R2; q++) {
+                    const int kx = 2 * (k1 + R1 * q) + h, mx = kx > NI, ox = mx ? 2 * NI - kx : kx;
+                    const float4 *A = reinterpret_cast<const float4 *>(Ayz + (size_t)ox * sxo);
+                    const float4 a01 = __ldg(A), a23 = __ldg(A + 1), a45 = __ldg(A + 2);
+                    float2 g0 = make_float2(a01.x, a01.y), g1 = make_float2(a01.z, a01.w),
+                           g2 = make_float2(a23.x, a23.y), g3 = make_float2(a23.z, a23.w),
+                           g4 = make_float2(a45.x, a45.y), g5 = make_float2(a45.z, a45.w);
+                    if (mx ^ my) g1 = cscale(g1, -1.f);
+                    if (mx ^ mz) g2 = cscale(g2, -1.f);
+                    if (my ^ mz) g4 = cscale(g4, -1.f);
+                    const float2 ps = Bat(3, h, R2 * k1 + q);
+                    const float2 vx = cmul(Ex, ps), vy = cmul(Ey, ps), vz = cmul(Ez, ps);
+                    X[0][q] = cadd(cadd(cmul(g0, vx), cmul(g1, vy)), cmul(g2, vz));
+                    X[1][q] = cadd(cadd(cmul(g1, vx), cmul(g3, vy)), cmul(g4, vz));
+                    X[2][q] = cadd(cadd(cmul(g2, vx), cmul(g4, vy)), cmul(g5, vz));
+                }
+#pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    dft_reg<R2, true>(X[c]);
+#pragma unroll
+                    for (int u = 0; u < R2; u++) {
+                        const float2 y = u ? cmul(X[c][u], twid<true>(tw, k1 * u)) : X[c][u];
+                        Bat(c, h, k1 + R1 * u) = y;
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        // ---- inverse step B, combine the halves, store to right-hand side 2k + pol
+        float2 *base = a.work + (size_t)(rhs0 + pol) * a.wstride + col;
+        if constexpr (R1 == 2 * R2) {
+            const int k1p = sub % R2, hb = sub / R2;
+            constexpr int H = R1 / 2;
+#pragma unroll 1
+            for (int c = 0; c < 3; c++) {
+                float2 e[H], o[H];
+#pragma unroll
+                for (int n = 0; n < H; n++) {
+                    const float2 e0 = Bat(c, 0, R1 * k1p + n), e1 = Bat(c, 0, R1 * k1p + n + H);
+                    const float2 o0 = Bat(c, 1, R1 * k1p + n), o1 = Bat(c, 1, R1 * k1p + n + H);
+                    if (hb) {
+                        const float2 wn = cconj(w16(n * (16 / R1)));
+                        e[n] = n ? cmul(csub(e0, e1), wn) : csub(e0, e1);
+                        o[n] = n ? cmul(csub(o0, o1), wn) : csub(o0, o1);
+                    } else {
+                        e[n] = cadd(e0, e1);
+                        o[n] = cadd(o0, o1);
+                    }
+                }
+                dft_reg<H, true>(e);
+                dft_reg<H, true>(o);
+#pragma unroll
+                for (int m = 0; m < H; m++) {
+                    const int i = k1p + R2 * (2 * m + hb);
+                    base[c * cstr + i * plane] = cadd(e[m], cmulc(o[m], __ldg(&hw[i])));
+                }
+            }
+        } else if (sub < R2) {
+            const int k1p = sub;
+#pragma unroll 1
+            for (int c = 0; c < 3; c++) {
+                float2 e[R1], o[R1];
+#pragma unroll
+                for (int q = 0; q < R1; q++) {
+                    e[q] = Bat(c, 0, R1 * k1p + q);
+                    o[q] = Bat(c, 1, R1 * k1p + q);
+                }
+                dft_reg<R1, true>(e);
+                dft_reg<R1, true>(o);
+#pragma unroll
+                for (int k2 = 0; k2 < R1; k2++) {
+                    const int i = k1p + R2 * k2;
+                    base[c * cstr + i * plane] = cadd(e[k2], cmulc(o[k2], __ldg(&hw[i])));
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
 // ------------------------------------------------------------------------------ K3
 // Cluster pair (rank = z half hl) per (i, component): y-inverse of this half's NL
 // columns (both y halves), z-inverse of the NJ rows restricted to this half, then the two
@@ -766,8 +948,9 @@ void launch_yz_v(const MatvecArgs &a, int fwd, cudaStream_t st)
 {
     constexpr int NT = yz_threads<NJ, NL>(V);
     constexpr size_t S = yz_smem<NJ, NL>();
-    if (fwd && a.inc) k1f<NJ, NL, NT, true><<<dim3(2 * a.L.ni, 3, a.nrhs), NT, S, st>>>(a);
-    else if (fwd) k1f<NJ, NL, NT, false><<<dim3(2 * a.L.ni, 3, a.nrhs), NT, S, st>>>(a);
+    if (fwd && a.inc && a.pair) k1f<NJ, NL, NT, 2><<<dim3(2 * a.L.ni, 1, a.nrhs / 2), NT, S, st>>>(a);
+    else if (fwd && a.inc) k1f<NJ, NL, NT, 1><<<dim3(2 * a.L.ni, 3, a.nrhs), NT, S, st>>>(a);
+    else if (fwd) k1f<NJ, NL, NT, 0><<<dim3(2 * a.L.ni, 3, a.nrhs), NT, S, st>>>(a);
     else k3f<NJ, NL, NT><<<dim3(2 * a.L.ni, 3, a.nrhs), NT, S, st>>>(a);
 }
 
@@ -784,9 +967,11 @@ cudaError_t prep_yz_v()
 {
     constexpr int NT = yz_threads<NJ, NL>(V);
     constexpr int S = (int)yz_smem<NJ, NL>();
-    cudaError_t e = cudaFuncSetAttribute(k1f<NJ, NL, NT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, S);
+    cudaError_t e = cudaFuncSetAttribute(k1f<NJ, NL, NT, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, S);
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k1f<NJ, NL, NT, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, S);
+        e = cudaFuncSetAttribute(k1f<NJ, NL, NT, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, S);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k1f<NJ, NL, NT, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, S);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k3f<NJ, NL, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, S);
     return e;
@@ -821,9 +1006,28 @@ void launch_x_v(const MatvecArgs &a, cudaStream_t st)
     k2f<NI, TL, (V >= 3)><<<grid, Sp<NI>::RM * TL, smem, st>>>(a);
 }
 
+// the pair form of the x pass (step 0 of polarisation pairs), same column tiles
+template <int NI, int V>
+void launch_x_pair_v(const MatvecArgs &a, cudaStream_t st)
+{
+    constexpr int TL = x_tile<NI>(V);
+    const int ncol = 2 * a.L.nl, np = a.nrhs / 2;
+    const size_t smem = (size_t)8 * NI * TL * sizeof(float2);
+    const dim3 grid = k2_rhs_fastest(NI) ? dim3(np, ncol / TL, 2 * a.L.nj) : dim3(2 * a.L.nj, ncol / TL, np);
+    k2p<NI, TL><<<grid, Sp<NI>::RM * TL, smem, st>>>(a);
+}
+
 template <int NI>
 void launch_x(const MatvecArgs &a, cudaStream_t st)
 {
+    if (a.inc && a.pair) {
+        switch (a.fx % 3) {
+        case 2: launch_x_pair_v<NI, 2>(a, st); break;
+        case 1: launch_x_pair_v<NI, 1>(a, st); break;
+        default: launch_x_pair_v<NI, 0>(a, st); break;
+        }
+        return;
+    }
     switch (a.fx) {
     case 5: launch_x_v<NI, 5>(a, st); break;
     case 4: launch_x_v<NI, 4>(a, st); break;
@@ -838,8 +1042,12 @@ template <int NI, int V>
 cudaError_t prep_x_v()
 {
     constexpr int TL = x_tile<NI>(V % 3);
-    return cudaFuncSetAttribute(k2f<NI, TL, (V >= 3)>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)(6 * NI * TL * sizeof(float2)));
+    cudaError_t e = cudaFuncSetAttribute(k2f<NI, TL, (V >= 3)>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)(6 * NI * TL * sizeof(float2)));
+    if (e == cudaSuccess && V < 3)
+        e = cudaFuncSetAttribute(k2p<NI, TL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(8 * NI * TL * sizeof(float2)));
+    return e;
 }
 
 template <int NI>
