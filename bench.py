@@ -133,6 +133,25 @@ def cpu_reference(n_samples: int, threads: int):
     return n_samples / secs, "port", secs, 1
 
 
+def cross_check(ctx, occ, n):
+    """Both arms on the same orientations: the first n draws of worker 0's stream (seed 7),
+    through this library and through the reference's own single-threaded sample loop (the
+    reference arm's workers draw from their own streams, so their orientation sets differ;
+    the cost per orientation does not).  Largest relative differences of Cext and Cabs."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as P
+    import dda_fft_b200 as D
+    if not os.path.exists(P.REF_SO):
+        return None
+    cfg = P.make_run_cfg(grid=GRID, target=2, b_a=BA, c_a=CA, x=X, materials=(MAT,), orientation=1,
+                         seed=SEED)
+    *_, (ca, ce, _) = P.RefLib().run_samples(cfg, n, 1, each=True)
+    r = ctx.orientation_solves(D.BatchConfig(occ=occ, materials=[MAT]), D.mc_rotations(SEED, n))
+    return {"orientations": n, "reference": "float build, worker 0 stream",
+            "cext_max_rel": float(np.max(np.abs(r["cext"] - ce) / np.abs(ce))),
+            "cabs_max_rel": float(np.max(np.abs(r["cabs"] - ca) / np.abs(ca)))}
+
+
 def run_reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -377,6 +396,7 @@ def main():
         cpu = {"value": v, "unit": "orientation-solves/s", "cores": used, "kind": kind,
                "sample": f"{ns} orientation-solves of the same workload, {secs:.1f} s wall "
                          f"(setup excluded)"}
+        cpu["cross_check"] = cross_check(ctx, occ, 8)
 
     if rank == 0:
         line = {

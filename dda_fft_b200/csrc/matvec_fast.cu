@@ -678,6 +678,10 @@ __global__ void __launch_bounds__(Sp<NI>::RM * TL, k2_min_blocks(NI, Sp<NI>::RM 
         const double *E = a.einc + 6 * (rhs0 + pol);
         const float2 Ex = make_float2((float)E[0], (float)E[1]), Ey = make_float2((float)E[2], (float)E[3]),
                      Ez = make_float2((float)E[4], (float)E[5]);
+        // a real incident field (every rotated x or y polarisation): u = G E with real
+        // weights (fused multiply-adds on the components), then u psi -- 30 instead of 54
+        // floating-point instructions per frequency
+        const bool Ereal = Ex.y == 0.f && Ey.y == 0.f && Ez.y == 0.f;
         // ---- product with the Green tensor, inverse step A (transposed split)
         if (sub < R1) {
             const int k1 = sub;
@@ -696,10 +700,21 @@ __global__ void __launch_bounds__(Sp<NI>::RM * TL, k2_min_blocks(NI, Sp<NI>::RM 
                     if (mx ^ mz) g2 = cscale(g2, -1.f);
                     if (my ^ mz) g4 = cscale(g4, -1.f);
                     const float2 ps = Bat(3, h, R2 * k1 + q);
-                    const float2 vx = cmul(Ex, ps), vy = cmul(Ey, ps), vz = cmul(Ez, ps);
-                    X[0][q] = cadd(cadd(cmul(g0, vx), cmul(g1, vy)), cmul(g2, vz));
-                    X[1][q] = cadd(cadd(cmul(g1, vx), cmul(g3, vy)), cmul(g4, vz));
-                    X[2][q] = cadd(cadd(cmul(g2, vx), cmul(g4, vy)), cmul(g5, vz));
+                    if (Ereal) {
+                        const float ex = Ex.x, ey = Ey.x, ez = Ez.x;
+                        auto dot = [&](float2 ga, float2 gb, float2 gc) {
+                            return make_float2(fmaf(ga.x, ex, fmaf(gb.x, ey, gc.x * ez)),
+                                               fmaf(ga.y, ex, fmaf(gb.y, ey, gc.y * ez)));
+                        };
+                        X[0][q] = cmul(dot(g0, g1, g2), ps);
+                        X[1][q] = cmul(dot(g1, g3, g4), ps);
+                        X[2][q] = cmul(dot(g2, g4, g5), ps);
+                    } else {
+                        const float2 vx = cmul(Ex, ps), vy = cmul(Ey, ps), vz = cmul(Ez, ps);
+                        X[0][q] = cadd(cadd(cmul(g0, vx), cmul(g1, vy)), cmul(g2, vz));
+                        X[1][q] = cadd(cadd(cmul(g1, vx), cmul(g3, vy)), cmul(g4, vz));
+                        X[2][q] = cadd(cadd(cmul(g2, vx), cmul(g4, vy)), cmul(g5, vz));
+                    }
                 }
 #pragma unroll
                 for (int c = 0; c < 3; c++) {
