@@ -17,6 +17,8 @@
 // touch distinct banks.
 #include <cooperative_groups.h>
 
+#include <type_traits>
+
 #include "common.cuh"
 #include "internal.h"
 
@@ -682,8 +684,10 @@ __global__ void __launch_bounds__(Sp<NI>::RM * TL, k2_min_blocks(NI, Sp<NI>::RM 
         // weights (fused multiply-adds on the components), then u psi -- 30 instead of 54
         // floating-point instructions per frequency
         const bool Ereal = Ex.y == 0.f && Ey.y == 0.f && Ez.y == 0.f;
-        // ---- product with the Green tensor, inverse step A (transposed split)
-        if (sub < R1) {
+        // ---- product with the Green tensor, inverse step A (transposed split); the branch
+        // on a real field is taken once per polarisation, outside the unrolled loops
+        auto product = [&](auto real_tag) {
+            constexpr bool REAL = decltype(real_tag)::value;
             const int k1 = sub;
 #pragma unroll 1
             for (int h = 0; h < 2; h++) {
@@ -700,7 +704,7 @@ __global__ void __launch_bounds__(Sp<NI>::RM * TL, k2_min_blocks(NI, Sp<NI>::RM 
                     if (mx ^ mz) g2 = cscale(g2, -1.f);
                     if (my ^ mz) g4 = cscale(g4, -1.f);
                     const float2 ps = Bat(3, h, R2 * k1 + q);
-                    if (Ereal) {
+                    if constexpr (REAL) {
                         const float ex = Ex.x, ey = Ey.x, ez = Ez.x;
                         auto dot = [&](float2 ga, float2 gb, float2 gc) {
                             return make_float2(fmaf(ga.x, ex, fmaf(gb.x, ey, gc.x * ez)),
@@ -726,6 +730,10 @@ __global__ void __launch_bounds__(Sp<NI>::RM * TL, k2_min_blocks(NI, Sp<NI>::RM 
                     }
                 }
             }
+        };
+        if (sub < R1) {
+            if (Ereal) product(std::true_type{});
+            else product(std::false_type{});
         }
         __syncthreads();
         // ---- inverse step B, combine the halves, store to right-hand side 2k + pol
