@@ -605,7 +605,8 @@ class Context:
         _check(lib().ddagpu_set_tiling(self._h, tile_x, rows_g))
 
     def set_fast_variant(self, x_variant: int = 0, yz_variant: int = 0):
-        """Launch variants of the compile-time-sized passes (0/1 each)."""
+        """Launch variants of the compile-time-sized passes: x 0..8 (tiles, bulk copies,
+        second line factorisation), y/z 0..2 (block sizes)."""
         _check(lib().ddagpu_set_fast_variant(self._h, x_variant, yz_variant))
 
     @property

@@ -2097,7 +2097,7 @@ int ddagpu_set_fast_variant(ddagpu_ctx *c, int x_variant, int yz_variant)
 {
     if (!c) return fail(DDAGPU_EINVAL, "null context");
     if (x_variant < 0 || x_variant >= kXVariants || yz_variant < 0 || yz_variant >= kYZVariants)
-        return fail(DDAGPU_EINVAL, "launch variants: x 0..5, y/z 0..2");
+        return fail(DDAGPU_EINVAL, "launch variants: x 0..8, y/z 0..2");
     std::lock_guard<std::mutex> lk(c->mu);
     c->fx = x_variant;
     c->fyz = yz_variant;

@@ -100,7 +100,7 @@ cudaError_t matvec_prepare(const Lat &L, int tile_x, int rows_g);
 
 // compile-time-sized passes for edges in {16, 32, 64} (matvec_fast.cu)
 bool matvec_fast_supported(const Lat &L);
-constexpr int kXVariants = 6;      // launch variants of the fast x pass
+constexpr int kXVariants = 9;      // launch variants of the fast x pass
 constexpr int kYZVariants = 3;     // launch variants of the fast y/z passes
 cudaError_t matvec_fast_prepare(const Lat &L);
 cudaError_t launch_matvec_fast(const MatvecArgs &a, cudaStream_t st);

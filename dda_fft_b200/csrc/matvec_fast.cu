@@ -36,6 +36,19 @@ struct Sp {
     static constexpr int PS = N + ((RM % 16) - (N % 16) + 16) % 16;
 };
 
+// The x pass's line factorisation N = R1 R2: ALT 0 is fft_split<N>; ALT 1 the second
+// schedule the autotuner may pick -- the two factors swapped, or for a square split
+// 2 R1 x R2 / 2 (16: 8 x 2, 32: 4 x 8, 64: 16 x 4, 128: 8 x 16).  The reference chooses
+// among radix-8/4/2 stage sequences per length the same way (fft_kernel.hpp:210-263).
+template <int N, int ALT>
+struct Sx {
+    static constexpr int A1 = fft_split<N>::R1, A2 = fft_split<N>::R2;
+    static constexpr int R1 = ALT == 0 ? A1 : (A1 == A2 ? 2 * A1 : A2);
+    static constexpr int R2 = ALT == 0 ? A2 : (A1 == A2 ? A2 / 2 : A1);
+    static constexpr int RM = R1 > R2 ? R1 : R2;
+    static_assert(R1 * R2 == N && R1 <= 16 && R2 <= 16, "bad line factorisation");
+};
+
 DDA_DEV int spos(int p) { return p ^ ((p >> 3) & 7); }
 
 DDA_DEV int zmapf(int oz, int nl) { return (oz & 1) ? (nl / 2 + 1 + (oz >> 1)) : (oz >> 1); }
@@ -310,10 +323,11 @@ DDA_DEV bool mbar_wait(unsigned long long *bar, unsigned parity, int polls = 1 <
     return false;
 }
 
-template <int NI, int TL, bool BULK>
-__global__ void __launch_bounds__(Sp<NI>::RM * TL, k2_min_blocks(NI, Sp<NI>::RM * TL)) k2f(MatvecArgs a)
+template <int NI, int TL, bool BULK, int ALT>
+__global__ void __launch_bounds__(Sx<NI, ALT>::RM * TL, k2_min_blocks(NI, Sx<NI, ALT>::RM * TL)) k2f(MatvecArgs a)
 {
-    using S = Sp<NI>;
+    using S = Sx<NI, ALT>;
+    static_assert(!BULK || ALT == 0, "bulk copies with the default factorisation only");
     constexpr int R1 = S::R1, R2 = S::R2, RM = S::RM;
     extern __shared__ __align__(128) float2 B[];   // [6][NI][TL]
     // at edge 128 the right-hand side is the fastest grid index: CTAs that run together
@@ -1017,16 +1031,18 @@ constexpr int x_tile(int v)
 }
 
 // x variants 0..2: register loads with 32 / 16 / 8 columns (16 / 8 / 4 at edge 128);
-// 3..5: the same tiles fed by bulk asynchronous copies
+// 3..5: the same tiles fed by bulk asynchronous copies; 6..8: register loads with the
+// second line factorisation (Sx<N, 1>)
 template <int NI, int V>
 void launch_x_v(const MatvecArgs &a, cudaStream_t st)
 {
-    constexpr int TL = x_tile<NI>(V % 3);
+    constexpr int TL = x_tile<NI>(V % 3), ALT = V >= 6 ? 1 : 0;
+    constexpr bool BULK = V >= 3 && V < 6;
     const int ncol = 2 * a.L.nl;
     const size_t smem = (size_t)6 * NI * TL * sizeof(float2);
     const dim3 grid = k2_rhs_fastest(NI) ? dim3(a.nrhs, ncol / TL, 2 * a.L.nj)
                                          : dim3(2 * a.L.nj, ncol / TL, a.nrhs);
-    k2f<NI, TL, (V >= 3)><<<grid, Sp<NI>::RM * TL, smem, st>>>(a);
+    k2f<NI, TL, BULK, ALT><<<grid, Sx<NI, ALT>::RM * TL, smem, st>>>(a);
 }
 
 // the pair form of the x pass (step 0 of polarisation pairs), same column tiles
@@ -1052,6 +1068,9 @@ void launch_x(const MatvecArgs &a, cudaStream_t st)
         return;
     }
     switch (a.fx) {
+    case 8: launch_x_v<NI, 8>(a, st); break;
+    case 7: launch_x_v<NI, 7>(a, st); break;
+    case 6: launch_x_v<NI, 6>(a, st); break;
     case 5: launch_x_v<NI, 5>(a, st); break;
     case 4: launch_x_v<NI, 4>(a, st); break;
     case 3: launch_x_v<NI, 3>(a, st); break;
@@ -1064,8 +1083,9 @@ void launch_x(const MatvecArgs &a, cudaStream_t st)
 template <int NI, int V>
 cudaError_t prep_x_v()
 {
-    constexpr int TL = x_tile<NI>(V % 3);
-    cudaError_t e = cudaFuncSetAttribute(k2f<NI, TL, (V >= 3)>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    constexpr int TL = x_tile<NI>(V % 3), ALT = V >= 6 ? 1 : 0;
+    constexpr bool BULK = V >= 3 && V < 6;
+    cudaError_t e = cudaFuncSetAttribute(k2f<NI, TL, BULK, ALT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)(6 * NI * TL * sizeof(float2)));
     if (e == cudaSuccess && V < 3)
         e = cudaFuncSetAttribute(k2p<NI, TL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1081,7 +1101,10 @@ cudaError_t prep_x()
     if (e == cudaSuccess) e = prep_x_v<NI, 2>();
     if (e == cudaSuccess) e = prep_x_v<NI, 3>();
     if (e == cudaSuccess) e = prep_x_v<NI, 4>();
-    return e == cudaSuccess ? prep_x_v<NI, 5>() : e;
+    if (e == cudaSuccess) e = prep_x_v<NI, 5>();
+    if (e == cudaSuccess) e = prep_x_v<NI, 6>();
+    if (e == cudaSuccess) e = prep_x_v<NI, 7>();
+    return e == cudaSuccess ? prep_x_v<NI, 8>() : e;
 }
 
 bool fast_edge(int n) { return n == 16 || n == 32 || n == 64 || n == 128; }

@@ -261,7 +261,9 @@ int ddagpu_anthrax_rasterize(int device, int i_max, int j_max, int l_max, const 
 
 /* Launch variants of the compile-time-sized matvec passes (edges 16..128): x_variant
  * 0/1/2 = 32, 16 or 8 spectral columns per x-pass CTA (16, 8, 4 at edge 128), 3/4/5 = the
- * same with the input rows moved into shared memory by bulk asynchronous copies;
+ * same with the input rows moved into shared memory by bulk asynchronous copies, 6/7/8 =
+ * the same tiles with the x lines' second factorisation (16 = 8 x 2, 32 = 4 x 8,
+ * 64 = 16 x 4, 128 = 8 x 16 instead of 4 x 4, 8 x 4, 8 x 8, 16 x 8: the radix schedule);
  * yz_variant 0/1/2 = the default block size of the y/z passes, the other of 256 / 512, or
  * 128 threads.
  * ddagpu_autotune times every combination (and the generic passes) and keeps the
