@@ -5,6 +5,8 @@
 // per-method recurrences, the absolute Error_max test and the best-iterate rollback.  All
 // fields, reductions and coefficients stay on the device; the host only launches kernels
 // and reads one flag per right-hand side per iteration to stop when all have converged.
+#include <cuda.h>   // CUtensorMap and cuTensorMapEncodeTiled's types (the function comes
+                    // from the runtime's driver entry point, no link to libcuda)
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -139,6 +141,9 @@ struct ddagpu_ctx {
     size_t worm_bytes = 0;
     int wait_selftest = 0;           // 1: the x pass's wait waits for a phase nothing completes
     long long post_key = 0;          // shape of the post-processing recorded with a solve
+    // TMA tensor maps of the work buffer, one per x-pass column tile (x variants 9..11)
+    alignas(64) CUtensorMap tmaps[3];
+    bool has_tmap = false;
     Fp64Buffers *f64 = nullptr;  // FP64 solve buffers (ddagpu_solve_fp64), built on first use
     MixedCgBuffers *mcg = nullptr;   // FP64 fields of the mixed-precision CG refinement
     long long gen = 0;           // bumped whenever recorded graphs must be dropped
@@ -162,6 +167,39 @@ struct DevGuard {
         if (prev >= 0) cudaSetDevice(prev);
     }
 };
+
+// The work buffer [cap][3][ni][2nj][2nl] complex float as a 5-D tensor map per x-pass
+// column tile (box TL x 1 x ni x 1 x 1, 8-byte elements, no swizzle, no multicast), for the
+// TMA variants of the x pass.  false if the driver does not offer the encoder.
+bool encode_work_maps(ddagpu_ctx *c)
+{
+    typedef CUresult (*Encode)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                               const cuuint64_t *, const cuuint32_t *, const cuuint32_t *,
+                               CUtensorMapInterleave, CUtensorMapSwizzle, CUtensorMapL2promotion,
+                               CUtensorMapFloatOOBfill);
+    void *fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !fn)
+        return false;
+    const Encode encode = reinterpret_cast<Encode>(fn);
+    const cuuint64_t e = sizeof(float2);
+    const cuuint64_t dim[5] = {(cuuint64_t)2 * c->nl, (cuuint64_t)2 * c->nj, (cuuint64_t)c->ni, 3,
+                               (cuuint64_t)c->cap};
+    const cuuint64_t str[4] = {dim[0] * e, dim[0] * dim[1] * e, dim[0] * dim[1] * dim[2] * e,
+                               dim[0] * dim[1] * dim[2] * 3 * e};
+    const cuuint32_t one[5] = {1, 1, 1, 1, 1};
+    for (int v = 0; v < 3; v++) {
+        const int tl = matvec_fast_x_tile(c->ni, v);
+        if (tl < 2 || (tl * e) % 16 != 0) return false;
+        const cuuint32_t box[5] = {(cuuint32_t)tl, 1, (cuuint32_t)c->ni, 1, 1};
+        if (encode(&c->tmaps[v], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 5, c->work, dim, str, box, one,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                   CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+            return false;
+    }
+    return true;
+}
 
 // W_n^k (k < n) followed by W_2n^j (j < n), forward sign, built in FP64.
 void twiddles(int n, float2 *out)
@@ -256,6 +294,7 @@ MatvecArgs mv_args(ddagpu_ctx *c, int nrhs, const float2 *src, float2 *out, int 
     a.fyz = c->fyz;
     a.err = c->err_dev;
     a.wait_selftest = c->wait_selftest;
+    a.tmaps = c->has_tmap ? (const void *)c->tmaps : nullptr;
     return a;
 }
 
@@ -957,6 +996,7 @@ int ddagpu_create(ddagpu_ctx **out, int device, int i_max, int j_max, int l_max,
         (e = cudaStreamSynchronize(c->st)) != cudaSuccess)
         return bail(fail(DDAGPU_ECUDA, std::string("setup: ") + cudaGetErrorString(e)));
     c->fast = matvec_fast_supported(c->L) ? 1 : 0;
+    if (c->fast) c->has_tmap = encode_work_maps(c);
     if (cudaMemset(c->err_dev, 0, sizeof(int)) != cudaSuccess)
         return bail(fail(DDAGPU_ECUDA, "setup: error flag"));
     *out = c;
@@ -1104,7 +1144,7 @@ int ddagpu_autotune(ddagpu_ctx *c, int nrhs)
     if (matvec_fast_supported(c->L)) {
         // the compile-time-sized passes in each launch variant
         c->fast = 1;
-        for (int vx = 0; vx < kXVariants; vx++)
+        for (int vx = 0; vx < (c->has_tmap ? kXVariants : 9); vx++)
             for (int vyz = 0; vyz < kYZVariants; vyz++) {
                 c->fx = vx;
                 c->fyz = vyz;
@@ -2097,7 +2137,8 @@ int ddagpu_set_fast_variant(ddagpu_ctx *c, int x_variant, int yz_variant)
 {
     if (!c) return fail(DDAGPU_EINVAL, "null context");
     if (x_variant < 0 || x_variant >= kXVariants || yz_variant < 0 || yz_variant >= kYZVariants)
-        return fail(DDAGPU_EINVAL, "launch variants: x 0..8, y/z 0..2");
+        return fail(DDAGPU_EINVAL, "launch variants: x 0..11, y/z 0..2");
+    if (x_variant >= 9 && !c->has_tmap) return fail(DDAGPU_EINVAL, "no tensor maps on this device");
     std::lock_guard<std::mutex> lk(c->mu);
     c->fx = x_variant;
     c->fyz = yz_variant;

@@ -70,6 +70,7 @@ struct MatvecArgs {
     int fast;               // 1: compile-time-sized kernels of matvec_fast.cu
     int fx, fyz;            // launch variants of the fast x pass (0..5) and y/z passes (0..2)
     int *err;               // device flag set by a kernel whose bounded wait gave up (or null)
+    const void *tmaps;      // host CUtensorMap[3] of the work buffer (TMA x variants), or null
     int wait_selftest;      // 1: the bulk-copy wait waits (briefly) for a phase that never completes
     // step 0 from the incident field (compile-time-sized passes only): the forward y/z pass
     // computes its input p = alpha_m exp(i k.(r - c)) E_inc on active cells (0 elsewhere)
@@ -100,9 +101,10 @@ cudaError_t matvec_prepare(const Lat &L, int tile_x, int rows_g);
 
 // compile-time-sized passes for edges in {16, 32, 64} (matvec_fast.cu)
 bool matvec_fast_supported(const Lat &L);
-constexpr int kXVariants = 9;      // launch variants of the fast x pass
+constexpr int kXVariants = 12;     // launch variants of the fast x pass (9..11: TMA tensor tiles)
 constexpr int kYZVariants = 3;     // launch variants of the fast y/z passes
 cudaError_t matvec_fast_prepare(const Lat &L);
+int matvec_fast_x_tile(int ni, int x_variant);   // spectral columns per CTA of an x variant
 cudaError_t launch_matvec_fast(const MatvecArgs &a, cudaStream_t st);
 
 // Green tensor (green.cu)

@@ -16,6 +16,7 @@
 // positions t2 + R2 r (step A) and a row group reading positions R2 k1 + t (step B) all
 // touch distinct banks.
 #include <cooperative_groups.h>
+#include <cuda.h>   // CUtensorMap (the type only; maps are encoded in ddagpu.cu)
 
 #include <type_traits>
 
@@ -307,6 +308,19 @@ DDA_DEV void bulk_g2s(void *dst, const void *src, unsigned bytes, unsigned long 
                  : "memory");
 }
 
+// One tile of a 5-D tensor map (TMA, no multicast): the box at coordinates (x0 .. x4)
+// into shared memory, completing on the mbarrier.  x0 is the innermost coordinate; its
+// byte offset (x0 x 8) must be a multiple of 16, which the callers' column tiles keep.
+DDA_DEV void tma_load_5d(void *dst, const CUtensorMap *map, int x0, int x1, int x2, int x3, int x4,
+                         unsigned long long *bar)
+{
+    asm volatile("cp.async.bulk.tensor.5d.shared::cluster.global.mbarrier::complete_tx::bytes"
+                 " [%0], [%1, {%2, %3, %4, %5, %6}], [%7];" ::"r"(smem_addr(dst)),
+                 "l"(reinterpret_cast<unsigned long long>(map)), "r"(x0), "r"(x1), "r"(x2), "r"(x3), "r"(x4),
+                 "r"(smem_addr(bar))
+                 : "memory");
+}
+
 // Waits for the barrier's phase `parity` to complete, at most `polls` polls; false if it did
 // not (the caller reports it through the error flag instead of hanging).
 DDA_DEV bool mbar_wait(unsigned long long *bar, unsigned parity, int polls = 1 << 22)
@@ -323,10 +337,15 @@ DDA_DEV bool mbar_wait(unsigned long long *bar, unsigned parity, int polls = 1 <
     return false;
 }
 
-template <int NI, int TL, bool BULK, int ALT>
-__global__ void __launch_bounds__(Sx<NI, ALT>::RM * TL, k2_min_blocks(NI, Sx<NI, ALT>::RM * TL)) k2f(MatvecArgs a)
+// LD: how the input columns reach the CTA -- 0 register loads, 1 one bulk copy per row,
+// 2 one TMA tensor tile per component (tmap: the work buffer as [rhs][c][i][js][ls] with
+// the box TL x 1 x NI; unused otherwise)
+template <int NI, int TL, int LD, int ALT>
+__global__ void __launch_bounds__(Sx<NI, ALT>::RM * TL, k2_min_blocks(NI, Sx<NI, ALT>::RM * TL))
+k2f(MatvecArgs a, const __grid_constant__ CUtensorMap tmap)
 {
     using S = Sx<NI, ALT>;
+    constexpr bool BULK = LD != 0;
     static_assert(!BULK || ALT == 0, "bulk copies with the default factorisation only");
     constexpr int R1 = S::R1, R2 = S::R2, RM = S::RM;
     extern __shared__ __align__(128) float2 B[];   // [6][NI][TL]
@@ -356,11 +375,18 @@ __global__ void __launch_bounds__(Sx<NI, ALT>::RM * TL, k2_min_blocks(NI, Sx<NI,
             mbar_expect_tx(&bar, 3u * NI * TL * (unsigned)sizeof(float2));
         }
         __syncthreads();
-        const float2 *row0 = a.work + (size_t)rhs * a.wstride + (size_t)js * (2 * nl) + l0;
-        for (int q = threadIdx.x; q < 3 * NI; q += blockDim.x) {
-            const int c = q / NI, i = q - c * NI;
-            bulk_g2s(&B[((c * 2) * NI + i) * TL], row0 + c * cstr + (size_t)i * plane,
-                     TL * (unsigned)sizeof(float2), &bar);
+        if constexpr (LD == 2) {
+            // three tensor tiles: component c's NI x TL columns land as [i][t] in half 0
+            if (threadIdx.x == 0)
+#pragma unroll
+                for (int c = 0; c < 3; c++) tma_load_5d(&B[(c * 2) * NI * TL], &tmap, l0, js, 0, c, rhs, &bar);
+        } else {
+            const float2 *row0 = a.work + (size_t)rhs * a.wstride + (size_t)js * (2 * nl) + l0;
+            for (int q = threadIdx.x; q < 3 * NI; q += blockDim.x) {
+                const int c = q / NI, i = q - c * NI;
+                bulk_g2s(&B[((c * 2) * NI + i) * TL], row0 + c * cstr + (size_t)i * plane,
+                         TL * (unsigned)sizeof(float2), &bar);
+            }
         }
         // (self-test: after the copies, wait briefly for the next phase, which nothing completes)
         bool got = mbar_wait(&bar, 0);
@@ -1033,16 +1059,21 @@ constexpr int x_tile(int v)
 // x variants 0..2: register loads with 32 / 16 / 8 columns (16 / 8 / 4 at edge 128);
 // 3..5: the same tiles fed by bulk asynchronous copies; 6..8: register loads with the
 // second line factorisation (Sx<N, 1>)
+// 9..11: the same tiles as 0..2 fed by one TMA tensor tile per component
+template <int V>
+constexpr int x_load(int) { return (V >= 3 && V < 6) ? 1 : (V >= 9 ? 2 : 0); }
+
 template <int NI, int V>
 void launch_x_v(const MatvecArgs &a, cudaStream_t st)
 {
-    constexpr int TL = x_tile<NI>(V % 3), ALT = V >= 6 ? 1 : 0;
-    constexpr bool BULK = V >= 3 && V < 6;
+    constexpr int TL = x_tile<NI>(V % 3), ALT = (V >= 6 && V < 9) ? 1 : 0, LD = x_load<V>(0);
     const int ncol = 2 * a.L.nl;
     const size_t smem = (size_t)6 * NI * TL * sizeof(float2);
     const dim3 grid = k2_rhs_fastest(NI) ? dim3(a.nrhs, ncol / TL, 2 * a.L.nj)
                                          : dim3(2 * a.L.nj, ncol / TL, a.nrhs);
-    k2f<NI, TL, BULK, ALT><<<grid, Sx<NI, ALT>::RM * TL, smem, st>>>(a);
+    static const CUtensorMap none{};
+    const CUtensorMap &map = LD == 2 ? static_cast<const CUtensorMap *>(a.tmaps)[V % 3] : none;
+    k2f<NI, TL, LD, ALT><<<grid, Sx<NI, ALT>::RM * TL, smem, st>>>(a, map);
 }
 
 // the pair form of the x pass (step 0 of polarisation pairs), same column tiles
@@ -1068,6 +1099,9 @@ void launch_x(const MatvecArgs &a, cudaStream_t st)
         return;
     }
     switch (a.fx) {
+    case 11: launch_x_v<NI, 11>(a, st); break;
+    case 10: launch_x_v<NI, 10>(a, st); break;
+    case 9: launch_x_v<NI, 9>(a, st); break;
     case 8: launch_x_v<NI, 8>(a, st); break;
     case 7: launch_x_v<NI, 7>(a, st); break;
     case 6: launch_x_v<NI, 6>(a, st); break;
@@ -1083,9 +1117,8 @@ void launch_x(const MatvecArgs &a, cudaStream_t st)
 template <int NI, int V>
 cudaError_t prep_x_v()
 {
-    constexpr int TL = x_tile<NI>(V % 3), ALT = V >= 6 ? 1 : 0;
-    constexpr bool BULK = V >= 3 && V < 6;
-    cudaError_t e = cudaFuncSetAttribute(k2f<NI, TL, BULK, ALT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    constexpr int TL = x_tile<NI>(V % 3), ALT = (V >= 6 && V < 9) ? 1 : 0, LD = x_load<V>(0);
+    cudaError_t e = cudaFuncSetAttribute(k2f<NI, TL, LD, ALT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)(6 * NI * TL * sizeof(float2)));
     if (e == cudaSuccess && V < 3)
         e = cudaFuncSetAttribute(k2p<NI, TL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1104,12 +1137,26 @@ cudaError_t prep_x()
     if (e == cudaSuccess) e = prep_x_v<NI, 5>();
     if (e == cudaSuccess) e = prep_x_v<NI, 6>();
     if (e == cudaSuccess) e = prep_x_v<NI, 7>();
-    return e == cudaSuccess ? prep_x_v<NI, 8>() : e;
+    if (e == cudaSuccess) e = prep_x_v<NI, 8>();
+    if (e == cudaSuccess) e = prep_x_v<NI, 9>();
+    if (e == cudaSuccess) e = prep_x_v<NI, 10>();
+    return e == cudaSuccess ? prep_x_v<NI, 11>() : e;
 }
 
 bool fast_edge(int n) { return n == 16 || n == 32 || n == 64 || n == 128; }
 
 }  // namespace
+
+int matvec_fast_x_tile(int ni, int v)
+{
+    switch (ni) {
+    case 16: return x_tile<16>(v % 3);
+    case 32: return x_tile<32>(v % 3);
+    case 64: return x_tile<64>(v % 3);
+    case 128: return x_tile<128>(v % 3);
+    }
+    return 0;
+}
 
 bool matvec_fast_supported(const Lat &L)
 {
@@ -1160,6 +1207,7 @@ static void yz(const MatvecArgs &a, int fwd, cudaStream_t st)
 
 cudaError_t launch_matvec_fast(const MatvecArgs &a, cudaStream_t st)
 {
+    if (a.fx >= 9 && !a.tmaps) return cudaErrorInvalidValue;   // no tensor maps for the TMA variants
     yz(a, 1, st);
     switch (a.L.ni) {
     case 16: launch_x<16>(a, st); break;

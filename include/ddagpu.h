@@ -263,7 +263,10 @@ int ddagpu_anthrax_rasterize(int device, int i_max, int j_max, int l_max, const 
  * 0/1/2 = 32, 16 or 8 spectral columns per x-pass CTA (16, 8, 4 at edge 128), 3/4/5 = the
  * same with the input rows moved into shared memory by bulk asynchronous copies, 6/7/8 =
  * the same tiles with the x lines' second factorisation (16 = 8 x 2, 32 = 4 x 8,
- * 64 = 16 x 4, 128 = 8 x 16 instead of 4 x 4, 8 x 4, 8 x 8, 16 x 8: the radix schedule);
+ * 64 = 16 x 4, 128 = 8 x 16 instead of 4 x 4, 8 x 4, 8 x 8, 16 x 8: the radix schedule),
+ * 9/10/11 = the tiles of 0/1/2 moved into shared memory as one TMA tensor tile per
+ * component (cp.async.bulk.tensor over a tensor map of the work buffer; offered where the
+ * driver provides the encoder);
  * yz_variant 0/1/2 = the default block size of the y/z passes, the other of 256 / 512, or
  * 128 threads.
  * ddagpu_autotune times every combination (and the generic passes) and keeps the

@@ -104,15 +104,17 @@ def test_graph_short_runs(D, oracle, solver, max_step):
     assert abs(b["cext"] - a["cext"]) <= 1e-6 * abs(a["cext"])
 
 
-def test_bounded_wait_reports_and_recovers(D, oracle):
-    """The x pass's bounded wait on its bulk copies: a wait made to run out (self-test: a
-    barrier phase nothing completes) fails the call with DDAGPU_ECUDA instead of hanging,
-    and the context computes correctly again afterwards."""
+@pytest.mark.parametrize("xv", [3, 9])
+def test_bounded_wait_reports_and_recovers(D, oracle, xv):
+    """The x pass's bounded wait on its bulk copies (xv 3) and TMA tensor tiles (xv 9): a
+    wait made to run out (self-test: after the copies have landed, a barrier phase nothing
+    completes) fails the call with DDAGPU_ECUDA instead of hanging, and the context
+    computes correctly again afterwards."""
     occ, kd, alpha, ksc = problem(oracle)
     rng = np.random.default_rng(2)
     p = (rng.standard_normal(occ.shape + (3,)) + 1j * rng.standard_normal(occ.shape + (3,))).astype(np.complex64)
     with D.Context(occ.shape, kd) as ctx:
-        ctx.set_fast_variant(3, 0)
+        ctx.set_fast_variant(xv, 0)
         ref = ctx.convolution(p)
         ctx.selftest_wait_timeout(True)
         with pytest.raises(D.DDAGPUError, match="wait ran out"):

@@ -134,9 +134,9 @@ def test_fast_and_generic_agree_128(D, grid):
 
 @pytest.mark.parametrize("grid", [(16, 16, 16), (64, 64, 64), (128, 64, 32), (32, 128, 16)])
 def test_fast_launch_variants_agree(D, oracle, grid):
-    """Every launch variant of the specialised passes -- tiles, bulk copies and both line
-    factorisations of the x pass (the radix schedules) -- gives the oracle's convolution,
-    and the autotuner's pick does too."""
+    """Every launch variant of the specialised passes -- tiles, bulk copies, TMA tensor
+    tiles and both line factorisations of the x pass (the radix schedules) -- gives the
+    oracle's convolution, and the autotuner's pick does too."""
     import torch
     rng = np.random.default_rng(9)
     p = crand(rng, (2, 3) + grid)
@@ -146,7 +146,7 @@ def test_fast_launch_variants_agree(D, oracle, grid):
     with D.Context(grid, kd, max_rhs=2) as ctx:
         x = torch.from_numpy(p).cuda()
         outs = []
-        for vx in range(9):          # 3..5: bulk asynchronous copies; 6..8: second factorisation
+        for vx in range(12):         # 3..5: bulk copies; 6..8: second factorisation; 9..11: TMA tiles
             for vyz in (0, 1, 2):
                 ctx.set_fast_variant(vx, vyz)
                 assert ctx.fast_variant == (vx, vyz)
