@@ -455,7 +455,7 @@ int record_whole_solve(ddagpu_ctx *c, cudaGraph_t g, int nrhs, int max_step, flo
 // Device results of a launched whole solve (on the context's stream): the solver states,
 // the last step and the bounded-wait flag; counts the launched kernels.
 int read_whole_solve(ddagpu_ctx *c, int nrhs, SolveResult &res, long long n_fixed, long long n_per_iter,
-                     int matvec0, int matvec_it)
+                     int matvec0, int matvec_it, bool own_launch = true)
 {
     cudaStream_t st = c->st;
     int last = 1;
@@ -469,7 +469,7 @@ int read_whole_solve(ddagpu_ctx *c, int nrhs, SolveResult &res, long long n_fixe
     c->launches += n_fixed + (long long)(last - 1) * n_per_iter;
     res.matvec0 = matvec0;
     res.matvec_it = matvec_it;
-    c->graph_runs += 1;
+    if (own_launch) c->graph_runs += 1;   // a group's launch is counted by the group
     return DDAGPU_OK;
 }
 
@@ -2452,7 +2452,10 @@ int ddagpu_group_agglomerate_solves(ddagpu_group *grp, const ddagpu_batch_cfg *c
         for (int r = 0; r < n_real[k]; r++)
             if (counts[k][r] < 0) return fail(DDAGPU_EINVAL, "negative monomer count");
     }
-    for (int k = 0; k < nctx; k++) locks.emplace_back(grp->ctx[(size_t)k]->mu);
+    // members locked in address order: groups sharing contexts cannot deadlock
+    std::vector<ddagpu_ctx *> order(grp->ctx);
+    std::sort(order.begin(), order.end());
+    for (ddagpu_ctx *m : order) locks.emplace_back(m->mu);
     DevGuard dg(grp->dev);
     std::vector<ddagpu_batch_info> bi((size_t)nctx, ddagpu_batch_info{0, 0, 0, 0.0});
     // ---- inputs of every member on its own stream, and the key of its solve
@@ -2531,10 +2534,9 @@ int ddagpu_group_agglomerate_solves(ddagpu_group *grp, const ddagpu_batch_cfg *c
         CK(cudaStreamWaitEvent(c->st, grp->done, 0));
         SolveResult res;
         const GroupRecord &R = grp->rec[(size_t)k];
-        RET(read_whole_solve(c, 2 * n_real[k], res, R.n_fixed, R.n_per_iter, R.matvec0, R.matvec_it));
+        RET(read_whole_solve(c, 2 * n_real[k], res, R.n_fixed, R.n_per_iter, R.matvec0, R.matvec_it, false));
         RET(batch_chunk_finish(c, geo[(size_t)k], n_real[k], res, cabs ? cabs[k] : nullptr,
                                cext ? cext[k] : nullptr, mueller ? mueller[k] : nullptr, bi[(size_t)k]));
-        c->graph_runs -= 1;   // the launch is the group's
     }
     if (info)
         for (int k = 0; k < nctx; k++) info[k] = bi[(size_t)k];

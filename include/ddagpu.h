@@ -223,8 +223,8 @@ int ddagpu_agglomerate_solves(ddagpu_ctx *ctx, const ddagpu_batch_cfg *cfg, int 
  * as a conditional while node, rollback, far field, cross sections, Mueller matrices) is an
  * independent branch of the group's graph, recorded once per solve shape and replayed; the
  * members' inputs are uploaded on their own streams first.  No counterpart in the reference.
- * A context may belong to several groups and still be used on its own; calls lock every
- * member.  Per-member arrays are indexed by member: n_real[k] (0 leaves member k out;
+ * A context may belong to several groups and still be used on its own; a call locks every
+ * member (in address order, so calls of groups that share members do not deadlock).  Per-member arrays are indexed by member: n_real[k] (0 leaves member k out;
  * at most max_rhs / 2 of that member), monomers[k], counts[k] as ddagpu_agglomerate_solves,
  * rot[k] (or rot == NULL: fixed orientation), outputs cabs[k], cext[k], mueller[k], ndip[k]
  * (each array of pointers may be NULL) and info[k]. */
