@@ -1839,6 +1839,7 @@ int ddagpu_solve_fp64(ddagpu_ctx *c, int solver, double tau, const double *alpha
     if (solver < 0 || solver > 3) return fail(DDAGPU_EINVAL, "solver must be 0..3");
     if (Max_Step < 0 || ndir < 0 || (ndir > 0 && (!ksc || !Esc)))
         return fail(DDAGPU_EINVAL, "bad solve parameters");
+    if (ndir > 65535) return fail(DDAGPU_EINVAL, "at most 65535 directions per FP64 solve");
     std::lock_guard<std::mutex> lk(c->mu);
     DevGuard dg(c->dev);
     const int nmat1 = n_mat + 1;

@@ -136,7 +136,7 @@ int ddagpu_solve_linear(ddagpu_ctx *ctx, int iMode_SolutionMethod, float rTau,
  * FP64 build takes hours.  alpha: 2 (n_mat + 1) doubles; kinc, Einc, ksc [ndir][3] and
  * Esc [ndir][6] doubles; rhs (optional) solves A p = rhs instead of A p = p_inc, x0
  * (optional) starts the solver from x0 instead of the right-hand side; rhs, x0 and p_out
- * (optional, the final dipoles) are fields of 6 doubles per cell.  Same stopping rule,
+ * (optional, the final dipoles) are fields of 6 doubles per cell; ndir <= 65535.  Same stopping rule,
  * rollback and outputs as ddagpu_dda_fft.  The FP64 work space (about 100 bytes per padded
  * cell plus 10 fields) is allocated on the first call and kept until ddagpu_release_fp64 or
  * ddagpu_destroy. */
