@@ -547,9 +547,10 @@ def plain_run(args):
     """The plain-method mid configuration: 64^3 sphere, x = 8, m = 1.5+0.01i, LDR,
     BiCGStab, Error_max 1e-3, Max_Step 100, 12 planes, theta 0..180 step 1 (2172
     directions), fixed orientation: one sample (both polarisations) through the batched
-    entry point, with the solver loop as a CUDA graph and on the host, the matvec on 2
-    right-hand sides, and the reference's own sample loop on one host thread (the
-    configuration has one sample, so one worker)."""
+    entry point, with the solver loop as a CUDA graph and on the host (far field by kz
+    groups), with the graph and the direct far field, the matvec on 2 right-hand sides,
+    and the reference's own sample loop on one host thread (the configuration has one
+    sample, so one worker)."""
     import torch
     import dda_fft_b200 as D
     n, x, mat = 64, 8.0, (1.5, 0.01)
@@ -562,8 +563,9 @@ def plain_run(args):
     rot = D.fixed_rotation(0, 0, 0)[None]
     with D.Context(n, kd, max_rhs=2) as ctx:
         st = torch.cuda.ExternalStream(ctx.stream_ptr)
-        for graph in (True, False):
+        for graph, ff in ((True, 0), (False, 0), (True, 1)):
             ctx.set_solver_graph(graph)
+            ctx.set_farfield_mode(ff)
             for _ in range(max(args.warmup, 1)):
                 r = ctx.orientation_solves(cfg, rot)
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -574,10 +576,12 @@ def plain_run(args):
                 r = ctx.orientation_solves(cfg, rot)
             e1.record(st)
             torch.cuda.synchronize()
-            out["graph" if graph else "host_loop"] = {
-                "ms_per_sample": e0.elapsed_time(e1) / reps, "steps": r["max_steps"],
-                "kernels_per_sample": (ctx.kernel_launches - l0) / reps}
-        out["cext"], out["cabs"] = float(r["cext"][0]), float(r["cabs"][0])
+            key = ("graph" if graph else "host_loop") + ("_direct_farfield" if ff else "")
+            out[key] = {"ms_per_sample": e0.elapsed_time(e1) / reps, "steps": r["max_steps"],
+                        "kernels_per_sample": (ctx.kernel_launches - l0) / reps}
+            if ff == 0:
+                out["cext"], out["cabs"] = float(r["cext"][0]), float(r["cabs"][0])
+        ctx.set_farfield_mode(0)
         xx = torch.randn(2, 3, n, n, n, dtype=torch.complex64, device="cuda")
         yy = torch.empty_like(xx)
         for _ in range(3):

@@ -127,6 +127,7 @@ def lib():
         L.ddagpu_farfield_noalloc.argtypes = [_i, _i, _i, _i, _f, _p, _p, _i, _p, _i, _p, _p, _p]
         L.ddagpu_get_kernels.argtypes = [_p]
         L.ddagpu_set_fast_variant.argtypes = [_p, _i, _i]
+        L.ddagpu_set_farfield_mode.argtypes = [_p, _i]
         L.ddagpu_get_fast_variant.argtypes = [_p, C.POINTER(_i), C.POINTER(_i)]
         L.ddagpu_set_solver_graph.argtypes = [_p, _i]
         L.ddagpu_selftest_wait_timeout.argtypes = [_p, _i]
@@ -605,9 +606,14 @@ class Context:
         _check(lib().ddagpu_set_tiling(self._h, tile_x, rows_g))
 
     def set_fast_variant(self, x_variant: int = 0, yz_variant: int = 0):
-        """Launch variants of the compile-time-sized passes: x 0..8 (tiles, bulk copies,
-        second line factorisation), y/z 0..2 (block sizes)."""
+        """Launch variants of the compile-time-sized passes: x 0..11 (tiles, bulk copies,
+        second line factorisation, TMA tensor tiles), y/z 0..2 (block sizes)."""
         _check(lib().ddagpu_set_fast_variant(self._h, x_variant, yz_variant))
+
+    def set_farfield_mode(self, mode: int = 0):
+        """Far-field form: 0 by kz groups where that halves the work (default), 1 one sum
+        per direction, 2 by kz groups whenever possible."""
+        _check(lib().ddagpu_set_farfield_mode(self._h, mode))
 
     @property
     def fast_variant(self):

@@ -126,7 +126,7 @@ struct ddagpu_ctx {
         double d0;
         size_t occ_stride;
         const void *trace, *occ;
-        long long post;
+        long long post, kz;
     } gkey{};
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t gexec = nullptr;
@@ -141,6 +141,13 @@ struct ddagpu_ctx {
     size_t worm_bytes = 0;
     int wait_selftest = 0;           // 1: the x pass's wait waits for a phase nothing completes
     long long post_key = 0;          // shape of the post-processing recorded with a solve
+    // far field by kz groups: the plan of the directions last uploaded, its device tables
+    ddagpu::KzPlan kz;
+    int ff_mode = 0;                 // ddagpu_set_farfield_mode
+    int *kz_tab = nullptr;
+    double *kz_val = nullptr;
+    float2 *kz_sum = nullptr;
+    size_t kz_tab_cap = 0, kz_val_cap = 0, kz_sum_cap = 0;
     // TMA tensor maps of the work buffer, one per x-pass column tile (x variants 9..11)
     alignas(64) CUtensorMap tmaps[3];
     bool has_tmap = false;
@@ -363,6 +370,7 @@ ddagpu_ctx::GraphKey whole_key(ddagpu_ctx *c, int nrhs, int solver, float tau, i
     key.trace = nullptr;
     key.occ = c->occ_stride ? (const void *)c->occ_b : (const void *)c->occ;
     key.post = c->post_key;
+    key.kz = c->kz.groups ? ((long long)c->kz.groups << 32) | c->kz.items : 0;
     key.pair = c->pair_step0;
     return key;
 }
@@ -1020,7 +1028,7 @@ int ddagpu_destroy(ddagpu_ctx *c)
                     c->mv,   c->alpha,  c->kinc,   c->einc,    c->ksc,    c->esc_acc,
                     c->cc_acc, c->normals, c->mueller, c->esc, c->cabs,   c->cext,
                     c->occ_b, c->ndip, c->step_dev, c->nact_dev, c->err_dev, c->worm_buf,
-                    c->inc_tab};
+                    c->inc_tab, c->kz_tab, c->kz_val, c->kz_sum};
     for (void *q : ptrs)
         if (q) cudaFree(q);
     if (c->pin) cudaFreeHost(c->pin);
@@ -1224,6 +1232,37 @@ int upload_materials(ddagpu_ctx *c, const int *mv, int nmat1, const signed char 
     return DDAGPU_OK;
 }
 
+// Uploads the scattering directions ks [nrhs][ndir][3] (pinned or pageable host memory)
+// and plans the far field's kz groups for them; the group tables grow here, outside any
+// graph capture, and a grown table drops the recorded graphs (they hold its address).
+// nact: active cells per right-hand side, for the choice between the two forms.
+int upload_directions(ddagpu_ctx *c, const double *ks, int nrhs, int ndir, bool pairs, double nact)
+{
+    c->kz.groups = 0;
+    if (ndir <= 0) return DDAGPU_OK;
+    CK(cudaMemcpyAsync(c->ksc, ks, (size_t)nrhs * ndir * 3 * sizeof(double), cudaMemcpyHostToDevice, c->st));
+    plan_kz_groups(ks, nrhs, ndir, pairs, c->ni, c->nj, c->nl, nact, c->ff_mode, c->kz);
+    if (!c->kz.groups) return DDAGPU_OK;
+    auto grow = [&](auto *&buf, size_t &cap, size_t need) -> int {
+        if (need <= cap) return DDAGPU_OK;
+        drop_graphs(c);
+        CK(cudaStreamSynchronize(c->st));
+        cudaFree(buf);
+        buf = nullptr;
+        cap = 0;
+        CK(dalloc(&buf, need));
+        cap = need;
+        return DDAGPU_OK;
+    };
+    RET(grow(c->kz_tab, c->kz_tab_cap, c->kz.tab.size()));
+    RET(grow(c->kz_val, c->kz_val_cap, c->kz.kz.size()));
+    RET(grow(c->kz_sum, c->kz_sum_cap, c->kz.sum_elems));
+    CK(cudaMemcpyAsync(c->kz_tab, c->kz.tab.data(), c->kz.tab.size() * sizeof(int), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->kz_val, c->kz.kz.data(), c->kz.kz.size() * sizeof(double), cudaMemcpyHostToDevice,
+                       c->st));
+    return DDAGPU_OK;
+}
+
 // pairs: right-hand sides 2k and 2k+1 are the two polarisations of one orientation
 int run_post(ddagpu_ctx *c, int nrhs, int nmat1, double d0, int ndir, bool pairs = false)
 {
@@ -1247,8 +1286,18 @@ int run_post(ddagpu_ctx *c, int nrhs, int nmat1, double d0, int ndir, bool pairs
     pa.ksc = c->ksc;
     pa.esc_acc = c->esc_acc;
     pa.cc_acc = c->cc_acc;
-    CK(launch_post(pa, c->esc, c->cabs, c->cext, c->st));
-    c->launches += 2;
+    if (ndir > 0 && c->kz.groups > 0) {
+        pa.kz_groups = c->kz.groups;
+        pa.kz_items = c->kz.items;
+        pa.kz_slice = c->kz.slice;
+        pa.kz_stride = c->kz.stride;
+        pa.kz_tab = c->kz_tab;
+        pa.kz_val = c->kz_val;
+        pa.kz_sum = c->kz_sum;
+    }
+    int nk = 0;
+    CK(launch_post(pa, c->esc, c->cabs, c->cext, c->st, &nk));
+    c->launches += nk;
     return DDAGPU_OK;
 }
 
@@ -1478,7 +1527,13 @@ int batch_chunk(ddagpu_ctx *c, const ddagpu_batch_cfg *cfg, const BatchGeom &g, 
     }
     CK(cudaMemcpyAsync(c->kinc, kin, Lc.n_kin * sizeof(double), cudaMemcpyHostToDevice, c->st));
     CK(cudaMemcpyAsync(c->einc, ein, Lc.n_ein * sizeof(double), cudaMemcpyHostToDevice, c->st));
-    CK(cudaMemcpyAsync(c->ksc, ks, Lc.n_ks * sizeof(double), cudaMemcpyHostToDevice, c->st));
+    double nact_mean = nact;
+    if (nact_per) {
+        nact_mean = 0.0;
+        for (int r = 0; r < nr; r++) nact_mean += nact_per[r];
+        nact_mean /= nr;
+    }
+    RET(upload_directions(c, ks, nr, ndir, true, nact_mean));
     CK(cudaMemcpyAsync(c->normals, nv, Lc.n_nv * sizeof(double), cudaMemcpyHostToDevice, c->st));
     CK(cudaMemcpyAsync(c->alpha, al, Lc.n_al * sizeof(float2), cudaMemcpyHostToDevice, c->st));
     SolveResult res;
@@ -1543,7 +1598,7 @@ int ddagpu_dda_fft(ddagpu_ctx *c, int iNoIllumination, int solver, float rTau, i
     CK(cudaMemcpyAsync(c->alpha, al.data(), nmat1 * sizeof(float2), cudaMemcpyHostToDevice, c->st));
     CK(cudaMemcpyAsync(c->kinc, kd3, sizeof kd3, cudaMemcpyHostToDevice, c->st));
     CK(cudaMemcpyAsync(c->einc, ed6, sizeof ed6, cudaMemcpyHostToDevice, c->st));
-    if (ndir) CK(cudaMemcpyAsync(c->ksc, kd.data(), kd.size() * sizeof(double), cudaMemcpyHostToDevice, c->st));
+    RET(upload_directions(c, kd.data(), 1, ndir, false, nact));
     // nact: counted by upload_materials
     if (nact == 0) return fail(DDAGPU_EINVAL, "no active dipoles");
     SolveResult res;
@@ -1784,7 +1839,7 @@ int ddagpu_dda_fft_refined(ddagpu_ctx *c, int solver, float rTau, const float *c
     CK(cudaMemcpyAsync(c->alpha, al.data(), nmat1 * sizeof(float2), cudaMemcpyHostToDevice, c->st));
     CK(cudaMemcpyAsync(c->kinc, kd3, sizeof kd3, cudaMemcpyHostToDevice, c->st));
     CK(cudaMemcpyAsync(c->einc, ed6, sizeof ed6, cudaMemcpyHostToDevice, c->st));
-    if (ndir) CK(cudaMemcpyAsync(c->ksc, kdir.data(), kdir.size() * sizeof(double), cudaMemcpyHostToDevice, c->st));
+    RET(upload_directions(c, kdir.data(), 1, ndir, false, nact));
     // nact: counted by upload_materials
     if (nact == 0) return fail(DDAGPU_EINVAL, "no active dipoles");
     ddagpu_refine_info ri;
@@ -1937,7 +1992,7 @@ int ddagpu_farfield(ddagpu_ctx *c, const int *iListMV, int n_mat, const signed c
     CK(cudaMemcpyAsync(c->alpha, zero_alpha.data(), nmat1 * sizeof(float2), cudaMemcpyHostToDevice, c->st));
     CK(cudaMemcpyAsync(c->kinc, z3, sizeof z3, cudaMemcpyHostToDevice, c->st));
     CK(cudaMemcpyAsync(c->einc, z6, sizeof z6, cudaMemcpyHostToDevice, c->st));
-    if (ndir) CK(cudaMemcpyAsync(c->ksc, kd.data(), kd.size() * sizeof(double), cudaMemcpyHostToDevice, c->st));
+    RET(upload_directions(c, kd.data(), 1, ndir, false, nact));
     RET(run_post(c, 1, nmat1, d0, ndir));
     std::vector<float2> esc((size_t)ndir * 3);
     if (ndir) CK(cudaMemcpyAsync(esc.data(), c->esc, esc.size() * sizeof(float2), cudaMemcpyDeviceToHost, c->st));
@@ -2143,6 +2198,15 @@ int ddagpu_set_fast_variant(ddagpu_ctx *c, int x_variant, int yz_variant)
     std::lock_guard<std::mutex> lk(c->mu);
     c->fx = x_variant;
     c->fyz = yz_variant;
+    return DDAGPU_OK;
+}
+
+int ddagpu_set_farfield_mode(ddagpu_ctx *c, int mode)
+{
+    if (!c) return fail(DDAGPU_EINVAL, "null context");
+    if (mode < 0 || mode > 2) return fail(DDAGPU_EINVAL, "far-field mode 0..2");
+    std::lock_guard<std::mutex> lk(c->mu);
+    c->ff_mode = mode;
     return DDAGPU_OK;
 }
 

@@ -8,6 +8,7 @@
 // projection S - k (k.S), equal by linearity to the reference's per-dipole projection.
 // The phase is separable, exp(i kx x) exp(i ky y) exp(i kz z), so each CTA builds small
 // tables and the inner loop is three complex multiply-adds per dipole and direction.
+#include <algorithm>
 #include <mutex>
 
 #include "common.cuh"
@@ -482,6 +483,194 @@ __global__ void __launch_bounds__(256) cabs_cext_sum(PostArgs a)
     block_sum_atomic<2>(v, scratch, a.cc_acc + 2 * rhs);
 }
 
+// ---- Far field by kz groups
+//
+// The scattering planes of a fixed orientation turn about the incident direction, the
+// lattice z axis (main.cpp:376-387 rotates each plane's directions about z), so the
+// directions at one scattering angle share kz.  When a block's directions take few
+// distinct kz, the z sum of the separable phase is done once per distinct value:
+//   T_g(i, j) = sum_l exp(i kz_g (z_l - cz)) P(i, j, l)                        (ff_zsum)
+//   S(k) = sum_{i,j} exp(i ky (y_j - cy)) exp(i kx (x_i - cx)) T_{g(k)}(i, j)  (ff_xysum)
+// -- farfield_sum's sum (dda_func.cpp:1576-1625 by linearity) in another order, with the
+// same phase arguments.  ff_zsum is a complex product (groups x z) . (z x rows) per
+// plane: a thread holds 4 groups x 3 NR components of one row, the plane's dipoles go
+// through shared memory masked by the activity list, 32 z at a time.
+constexpr int ZG = 32;   // kz groups per CTA (8 warps x 4)
+constexpr int ZR = 32;   // rows per row block (one per lane)
+constexpr int ZL = 32;   // z positions per staged chunk
+
+__host__ __device__ inline int kz_dirs_at(int G) { return 3 + G; }
+__host__ __device__ inline int kz_items_at(int G, int ndir) { return 3 + G + ndir; }
+
+__host__ __device__ inline size_t zsum_smem(int nl, int nr)
+{
+    return (size_t)nl * ZG * sizeof(float2) + (size_t)ZL * (3 * nr * ZR + 1) * sizeof(float2) + 256 * sizeof(int);
+}
+
+// grid (ni, group tiles of ZG, blocks), 256 threads
+template <int NR>
+__global__ void __launch_bounds__(256) ff_zsum(PostArgs a)
+{
+    constexpr int Q = 3 * NR, ZS = Q * ZR + 1;   // ZS: z stride of the staged chunk (float2)
+    extern __shared__ __align__(16) unsigned char smraw[];
+    const int nj = a.nj, nl = a.nl, G = a.kz_groups, nmat1 = a.nmat1;
+    const int i = blockIdx.x, g0 = blockIdx.y * ZG, b = blockIdx.z, rhs = NR * b;
+    const int *tab = a.kz_tab + (size_t)b * a.kz_stride;
+    const int gb = tab[0];
+    if (g0 >= gb) return;   // uniform over the block
+    float2 *ez = reinterpret_cast<float2 *>(smraw);              // [nl][ZG]
+    float2 *ps = ez + (size_t)nl * ZG;                           // [ZL][ZS]: [z][q][row]
+    int *mvs = reinterpret_cast<int *>(ps + (size_t)ZL * ZS);    // [nmat1]
+    const double czf = (nl - 1) * a.d0 / 2;
+    const double *kz = a.kz_val + (size_t)b * G;
+    for (int e = threadIdx.x; e < nl * ZG; e += blockDim.x) {
+        const int l = e / ZG, g = g0 + e % ZG;
+        ez[e] = g < gb ? expi_reduced(kz[g] * (l * a.d0 - czf)) : czero();
+    }
+    for (int e = threadIdx.x; e < nmat1; e += blockDim.x) mvs[e] = a.mv[e];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const size_t N = a.N, q0 = (size_t)i * nj * nl;
+    const float2 *pr = a.p + (size_t)rhs * 3 * N;
+    const signed char *occr = a.occ + (size_t)rhs * a.occ_stride;
+    const size_t gstride = (size_t)a.ni * nj * Q;
+    float2 *out = a.kz_sum + (size_t)b * G * gstride + (size_t)i * nj * Q;
+#pragma unroll 1
+    for (int j0 = 0; j0 < nj; j0 += ZR) {
+        float2 acc[4][Q];
+#pragma unroll
+        for (int g = 0; g < 4; g++)
+#pragma unroll
+            for (int q = 0; q < Q; q++) acc[g][q] = czero();
+#pragma unroll 1
+        for (int l0 = 0; l0 < nl; l0 += ZL) {
+            __syncthreads();   // the tables are written / the previous chunk is consumed
+            for (int e = threadIdx.x; e < ZL * ZR; e += blockDim.x) {
+                const int l = e % ZL, r = e / ZL, j = j0 + r, ll = l0 + l;
+                bool act = false;
+                size_t cell = 0;
+                if (j < nj && ll < nl) {
+                    cell = q0 + (size_t)j * nl + ll;
+                    const int m = occr[cell];
+                    act = (unsigned)m < (unsigned)nmat1 && mvs[m] != 0;
+                }
+#pragma unroll
+                for (int q = 0; q < Q; q++)
+                    ps[l * ZS + q * ZR + r] = act ? pr[(size_t)(q / 3) * 3 * N + (size_t)(q % 3) * N + cell] : czero();
+            }
+            __syncthreads();
+            const int lc = nl - l0 < ZL ? nl - l0 : ZL;
+#pragma unroll 4
+            for (int l = 0; l < lc; l++) {
+                const float4 e01 = *reinterpret_cast<const float4 *>(ez + (size_t)(l0 + l) * ZG + 4 * warp);
+                const float4 e23 = *reinterpret_cast<const float4 *>(ez + (size_t)(l0 + l) * ZG + 4 * warp + 2);
+                const float2 ev[4] = {make_float2(e01.x, e01.y), make_float2(e01.z, e01.w),
+                                      make_float2(e23.x, e23.y), make_float2(e23.z, e23.w)};
+#pragma unroll
+                for (int q = 0; q < Q; q++) {
+                    const float2 pv = ps[l * ZS + q * ZR + lane];
+#pragma unroll
+                    for (int g = 0; g < 4; g++) acc[g][q] = cfma(ev[g], pv, acc[g][q]);
+                }
+            }
+        }
+        const int j = j0 + lane;
+        if (j < nj) {
+#pragma unroll
+            for (int g = 0; g < 4; g++) {
+                const int gg = g0 + 4 * warp + g;
+                if (gg < gb) {
+#pragma unroll
+                    for (int q = 0; q < Q; q++) out[gg * gstride + (size_t)j * Q + q] = acc[g][q];
+                }
+            }
+        }
+    }
+}
+
+__host__ __device__ inline size_t xysum_smem(int nj, int slice, int nr)
+{
+    return ((size_t)slice * nj * 3 * nr + (size_t)kKzItem * (slice + nj)) * sizeof(float2);
+}
+
+// grid (items, plane slices of a.kz_slice, blocks), 256 threads: an item's directions
+// (one kz group), two per warp, over the group sums of the slice's planes
+template <int NR>
+__global__ void __launch_bounds__(256) ff_xysum(PostArgs a)
+{
+    constexpr int Q = 3 * NR;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    const int nj = a.nj, G = a.kz_groups, b = blockIdx.z, rhs = NR * b, slice = a.kz_slice;
+    const int *tab = a.kz_tab + (size_t)b * a.kz_stride;
+    if ((int)blockIdx.x >= tab[1]) return;   // uniform over the block
+    const int *dirs = tab + kz_dirs_at(G);
+    const int *item = tab + kz_items_at(G, a.ndir) + 2 * blockIdx.x;
+    const int g = item[0], s0 = item[1], send = tab[2 + g + 1];
+    const int nd = send - s0 < kKzItem ? send - s0 : kKzItem;
+    const int i0 = blockIdx.y * slice, np = a.ni - i0 < slice ? a.ni - i0 : slice;
+    float2 *ts = reinterpret_cast<float2 *>(smraw);     // [np][nj][Q]
+    float2 *ex = ts + (size_t)slice * nj * Q;           // [kKzItem][slice]
+    float2 *ey = ex + (size_t)kKzItem * slice;          // [kKzItem][nj]
+    const float2 *src = a.kz_sum + (((size_t)b * G + g) * a.ni + i0) * nj * Q;
+    const int cnt = np * nj * Q;   // even: nj is
+    for (int e = threadIdx.x; e < cnt / 2; e += blockDim.x)
+        reinterpret_cast<float4 *>(ts)[e] = reinterpret_cast<const float4 *>(src)[e];
+    if ((cnt & 1) && threadIdx.x == 0) ts[cnt - 1] = src[cnt - 1];
+    const double cxf = (a.ni - 1) * a.d0 / 2, cyf = (nj - 1) * a.d0 / 2;
+    const double *K = a.ksc + (size_t)rhs * a.ndir * 3;
+    const int w = slice + nj;
+    for (int e = threadIdx.x; e < kKzItem * w; e += blockDim.x) {
+        const int d = e / w, pos = e - d * w;
+        float2 v = czero();
+        if (d < nd) {
+            const int dd = dirs[s0 + d];
+            if (pos < slice) {
+                if (pos < np) v = expi_reduced(K[3 * dd + 0] * ((i0 + pos) * a.d0 - cxf));
+            } else {
+                v = expi_reduced(K[3 * dd + 1] * ((pos - slice) * a.d0 - cyf));
+            }
+        }
+        if (pos < slice) ex[d * slice + pos] = v;
+        else ey[d * nj + pos - slice] = v;
+    }
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, d0 = 2 * warp;
+    if (d0 >= nd) return;   // uniform over the warp; no barrier follows
+    float2 acc[2][Q];
+#pragma unroll
+    for (int u = 0; u < 2; u++)
+#pragma unroll
+        for (int q = 0; q < Q; q++) acc[u][q] = czero();
+    for (int e = lane; e < np * nj; e += 32) {
+        const int ii = e / nj, j = e - ii * nj;
+        float2 tv[Q];
+#pragma unroll
+        for (int q = 0; q < Q; q++) tv[q] = ts[(size_t)e * Q + q];
+        const float2 f0 = cmul(ey[d0 * nj + j], ex[d0 * slice + ii]);
+        const float2 f1 = cmul(ey[(d0 + 1) * nj + j], ex[(d0 + 1) * slice + ii]);
+#pragma unroll
+        for (int q = 0; q < Q; q++) {
+            acc[0][q] = cfma(f0, tv[q], acc[0][q]);
+            acc[1][q] = cfma(f1, tv[q], acc[1][q]);
+        }
+    }
+    // the warp's sum in FP64, added by lane 0
+#pragma unroll
+    for (int u = 0; u < 2; u++) {
+        const bool have = d0 + u < nd;
+        const int dd = have ? dirs[s0 + d0 + u] : 0;
+#pragma unroll
+        for (int q = 0; q < Q; q++)
+#pragma unroll
+            for (int part = 0; part < 2; part++) {
+                double v = part ? acc[u][q].y : acc[u][q].x;
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+                if (lane == 0 && have && v != 0.0)
+                    atomicAdd(a.esc_acc + ((size_t)(rhs + q / 3) * a.ndir + dd) * 6 + 2 * (q % 3) + part, v);
+            }
+    }
+}
+
 // Esc = S - k (k.S); Cext, Cabs = 4 pi / |E|^2 * sums
 __global__ void post_finalize(PostArgs a, float2 *esc, float *cabs, float *cext)
 {
@@ -618,15 +807,103 @@ cudaError_t post_prepare(int nj, int nl)
     cudaError_t e = raise_smem_limit((const void *)farfield_sum<true, 1, 4>, bytes);
     if (e == cudaSuccess) e = raise_smem_limit((const void *)farfield_sum<true, 2, 2>, bytes);
     if (e == cudaSuccess) e = raise_smem_limit((const void *)farfield_sum<false, 1, 4>, bytes);
+    if (e == cudaSuccess) e = raise_smem_limit((const void *)ff_zsum<1>, (int)zsum_smem(nl, 1));
+    if (e == cudaSuccess) e = raise_smem_limit((const void *)ff_zsum<2>, (int)zsum_smem(nl, 2));
     return e;
 }
 
-cudaError_t launch_post(const PostArgs &a, float2 *esc, float *cabs, float *cext, cudaStream_t st)
+// plane slice of ff_xysum: about 32 KB of group sums, 64 planes at most
+static int kz_slice_for(int ni, int nj, int nr)
+{
+    int sl = 32768 / (nj * 3 * nr * (int)sizeof(float2));
+    if (sl < 1) sl = 1;
+    if (sl > 64) sl = 64;
+    return sl < ni ? sl : ni;
+}
+
+void plan_kz_groups(const double *ks, int nrhs, int ndir, bool pairs, int ni, int nj, int nl,
+                    double nact, int mode, KzPlan &P)
+{
+    P.groups = 0;
+    P.tab.clear();
+    P.kz.clear();
+    if (mode == 1 || ndir <= 0 || nrhs <= 0 || !ks) return;
+    const int NR = pairs && nrhs % 2 == 0 ? 2 : 1, nb = nrhs / NR;
+    // per block: direction indices sorted by kz (ties in index order), groups of equal kz
+    std::vector<std::vector<int>> order((size_t)nb);
+    std::vector<std::vector<int>> offs((size_t)nb);
+    int G = 0, items = 0;
+    for (int b = 0; b < nb; b++) {
+        const double *K = ks + (size_t)b * NR * ndir * 3;
+        std::vector<int> &o = order[(size_t)b];
+        o.resize((size_t)ndir);
+        for (int d = 0; d < ndir; d++) o[(size_t)d] = d;
+        std::stable_sort(o.begin(), o.end(), [&](int x, int y) { return K[3 * x + 2] < K[3 * y + 2]; });
+        std::vector<int> &f = offs[(size_t)b];
+        int it = 0;
+        for (int d = 0; d < ndir; d++)
+            if (d == 0 || K[3 * o[(size_t)d] + 2] != K[3 * o[(size_t)d - 1] + 2]) f.push_back(d);
+        f.push_back(ndir);
+        const int gb = (int)f.size() - 1;
+        for (int g = 0; g < gb; g++) it += (f[(size_t)g + 1] - f[(size_t)g] + kKzItem - 1) / kKzItem;
+        G = std::max(G, gb);
+        items = std::max(items, it);
+    }
+    const double plane = (double)nj * nl, cells = (double)ni * plane;
+    const size_t elems = (size_t)nb * G * ni * nj * 3 * NR;
+    if (elems * sizeof(float2) > ((size_t)1 << 30)) return;   // group sums above 1 GiB: direct
+    if (zsum_smem(nl, NR) > 200 * 1024 || xysum_smem(nj, kz_slice_for(ni, nj, NR), NR) > 48 * 1024) return;
+    // work: a complex multiply-add per (group, cell) and per (direction, row) against one
+    // per (direction, active cell)
+    if (mode == 0 && 2.0 * (G * cells + 2.0 * ndir * ni * nj) > (double)ndir * nact) return;
+    P.groups = G;
+    P.items = items;
+    P.blocks = nb;
+    P.slice = kz_slice_for(ni, nj, NR);
+    P.stride = kz_items_at(G, ndir) + 2 * items;
+    P.sum_elems = elems;
+    P.tab.assign((size_t)nb * P.stride, 0);
+    P.kz.assign((size_t)nb * G, 0.0);
+    for (int b = 0; b < nb; b++) {
+        const double *K = ks + (size_t)b * NR * ndir * 3;
+        int *t = P.tab.data() + (size_t)b * P.stride;
+        const std::vector<int> &o = order[(size_t)b], &f = offs[(size_t)b];
+        const int gb = (int)f.size() - 1;
+        t[0] = gb;
+        for (int g = 0; g <= G; g++) t[2 + g] = g <= gb ? f[(size_t)g] : ndir;
+        for (int d = 0; d < ndir; d++) t[kz_dirs_at(G) + d] = o[(size_t)d];
+        int it = 0;
+        for (int g = 0; g < gb; g++) {
+            P.kz[(size_t)b * G + g] = K[3 * o[(size_t)f[(size_t)g]] + 2];
+            for (int s0 = f[(size_t)g]; s0 < f[(size_t)g + 1]; s0 += kKzItem, it++) {
+                t[kz_items_at(G, ndir) + 2 * it] = g;
+                t[kz_items_at(G, ndir) + 2 * it + 1] = s0;
+            }
+        }
+        t[1] = it;
+    }
+}
+
+cudaError_t launch_post(const PostArgs &a, float2 *esc, float *cabs, float *cext, cudaStream_t st, int *kernels)
 {
     cudaError_t e;
+    int nk = 1;
     if ((e = cudaMemsetAsync(a.esc_acc, 0, (size_t)a.nrhs * a.ndir * 6 * sizeof(double), st))) return e;
     if ((e = cudaMemsetAsync(a.cc_acc, 0, (size_t)a.nrhs * 2 * sizeof(double), st))) return e;
-    if (a.ndir > 0) {
+    if (a.ndir > 0 && a.kz_groups > 0) {
+        // far field by kz groups, then the cross sections
+        const int NR = a.pairs && a.nrhs % 2 == 0 ? 2 : 1, nb = a.nrhs / NR;
+        const dim3 gz(a.ni, nblk(a.kz_groups, ZG), nb), gx(a.kz_items, nblk(a.ni, a.kz_slice), nb);
+        if (NR == 2) {
+            ff_zsum<2><<<gz, 256, zsum_smem(a.nl, 2), st>>>(a);
+            ff_xysum<2><<<gx, 256, xysum_smem(a.nj, a.kz_slice, 2), st>>>(a);
+        } else {
+            ff_zsum<1><<<gz, 256, zsum_smem(a.nl, 1), st>>>(a);
+            ff_xysum<1><<<gx, 256, xysum_smem(a.nj, a.kz_slice, 1), st>>>(a);
+        }
+        cabs_cext_sum<<<dim3(a.ni, a.nrhs), 256, (a.nj + a.nl) * sizeof(float2), st>>>(a);
+        nk += 3;
+    } else if (a.ndir > 0) {
         // far field with the cross sections summed by the first direction chunk
         if (a.nj >= 4096 || a.nl >= 4096) return cudaErrorInvalidValue;   // packed list words
         if (a.pairs && a.nrhs % 2 == 0) {
@@ -638,12 +915,15 @@ cudaError_t launch_post(const PostArgs &a, float2 *esc, float *cabs, float *cext
             farfield_sum<true, 1, 4><<<dim3(nblk(a.ndir, s.D), nblk(a.ni, s.planes), a.nrhs), s.threads,
                                        ff_layout(s, a.nj, a.nl, a.nmat1, true, 1).total, st>>>(a, s);
         }
+        nk += 1;
     } else {
         cabs_cext_sum<<<dim3(a.ni, a.nrhs), 256, (a.nj + a.nl) * sizeof(float2), st>>>(a);
+        nk += 1;
     }
     const size_t nd = (size_t)a.nrhs * a.ndir;
     const size_t nt = nd > (size_t)a.nrhs ? nd : (size_t)a.nrhs;
     post_finalize<<<nblk(nt, 256), 256, 0, st>>>(a, esc, cabs, cext);
+    if (kernels) *kernels = nk;
     return cudaGetLastError();
 }
 

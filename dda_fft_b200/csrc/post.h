@@ -1,5 +1,7 @@
 // Post-processing kernels of libddagpu (far field, cross sections, Mueller matrices).
 #pragma once
+#include <vector>
+
 #include "internal.h"
 
 namespace ddagpu {
@@ -22,7 +24,30 @@ struct PostArgs {
     double *cc_acc;           // [nrhs][2] scratch (Cext sum, Cabs sum)
     int pairs;                // right-hand sides 2k, 2k+1 share directions, incident
                               // direction and occupancy (both polarisations of one orientation)
+    // far field by kz groups (KzPlan; kz_groups 0: one sum per direction)
+    int kz_groups, kz_items, kz_slice, kz_stride;
+    const int *kz_tab;        // [blocks][kz_stride]
+    const double *kz_val;     // [blocks][kz_groups]
+    float2 *kz_sum;           // [blocks][kz_groups][ni][nj][3 NR]
 };
+
+// Directions of a right-hand side (or of a pair) grouped by their z component.  A block is
+// one right-hand side, or one pair when PostArgs::pairs and the count is even.  Per block,
+// kz_stride ints: [0] groups, [1] items, [2 .. 2 + G] the groups' offsets into the sorted
+// list, [3 + G ..) the directions sorted by kz, then items of (group, first position), each
+// at most kKzItem directions of one group.
+constexpr int kKzItem = 16;
+struct KzPlan {
+    int groups = 0;           // the most groups of a block; 0: the direct far field
+    int items = 0, slice = 0, stride = 0, blocks = 0;
+    size_t sum_elems = 0;     // float2 elements of the group sums
+    std::vector<int> tab;
+    std::vector<double> kz;
+};
+// ks: [nrhs][ndir][3] directions; nact: active cells per right-hand side (for the choice);
+// mode 0: the grouped form when it saves at least half the work, 1: never, 2: always
+void plan_kz_groups(const double *ks, int nrhs, int ndir, bool pairs, int ni, int nj, int nl,
+                    double nact, int mode, KzPlan &P);
 
 struct MuellerArgs {
     int norient, nplanes, nangles, ndir;   // ndir = nplanes * nangles
@@ -36,7 +61,9 @@ struct MuellerArgs {
 
 size_t farfield_smem(int nj, int nl);
 cudaError_t post_prepare(int nj, int nl);
-cudaError_t launch_post(const PostArgs &a, float2 *esc, float *cabs, float *cext, cudaStream_t st);
+// *kernels (may be null) receives the number of kernels launched
+cudaError_t launch_post(const PostArgs &a, float2 *esc, float *cabs, float *cext, cudaStream_t st,
+                        int *kernels = nullptr);
 cudaError_t launch_mueller(const MuellerArgs &m, cudaStream_t st);
 
 // allocation-free far field (scratch in a file-scope device array of post.cu)

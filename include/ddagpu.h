@@ -272,6 +272,17 @@ int ddagpu_anthrax_rasterize(int device, int i_max, int j_max, int l_max, const 
  * ddagpu_autotune times every combination (and the generic passes) and keeps the
  * fastest.  No counterpart in the reference. */
 int ddagpu_set_fast_variant(ddagpu_ctx *ctx, int x_variant, int yz_variant);
+
+/* Form of the far-field sum (FarField, dda_func.cpp:1576-1625).  When the scattering
+ * directions of a right-hand side take few distinct z components (the planes of a fixed
+ * orientation turn about the incident direction, the lattice z axis: every plane's
+ * direction at one angle has the same kz), the z sum of the separable phase is done once
+ * per distinct kz and the x/y sum once per direction; otherwise every direction sums over
+ * every active dipole.  mode 0 (default): the grouped form where it does at most half the
+ * work of the direct one; 1: always the direct form; 2: the grouped form whenever its group
+ * sums fit in 1 GiB.  The two forms agree to FP32 rounding.  No counterpart in the
+ * reference, whose sum is per direction. */
+int ddagpu_set_farfield_mode(ddagpu_ctx *ctx, int mode);
 int ddagpu_get_fast_variant(ddagpu_ctx *ctx, int *x_variant, int *yz_variant);
 
 /* Self-test of the bounded device waits: on != 0 makes the bulk-copy x-pass variants

@@ -83,8 +83,9 @@ def test_fixed_rotation_and_angles():
 
 
 def test_new_entry_points_reject_bad_arguments_without_a_device():
-    """The FP64 solve, groups and the architecture query fail loudly on bad arguments (and,
-    on a machine without a GPU, report that instead of computing anything)."""
+    """The FP64 solve, groups, the far-field mode and the architecture query fail loudly on
+    bad arguments (and, on a machine without a GPU, report that instead of computing
+    anything)."""
     import torch
     from dda_fft_b200 import lib
     L = lib()
@@ -97,6 +98,7 @@ def test_new_entry_points_reject_bad_arguments_without_a_device():
     assert L.ddagpu_solve_fp64(None, 0, 0.0, None, None, 1, None, 0.5, None, None, None, None, 5, 1e-3,
                                0, None, None, C.byref(z), C.byref(z), None, None, None) == -1
     assert L.ddagpu_release_fp64(None) == -1
+    assert L.ddagpu_set_farfield_mode(None, 0) == -1
     v = C.c_int(0)
     assert L.ddagpu_binary_version(0, None) == -1
     if not torch.cuda.is_available():
