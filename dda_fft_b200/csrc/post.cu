@@ -440,12 +440,13 @@ __global__ void __launch_bounds__(256) farfield_sum(PostArgs a, FFShape s)
     }
 }
 
-// Cext and Cabs sums (before the 4 pi / |E|^2 factor), grid (ni, nrhs)
-__global__ void __launch_bounds__(256) cabs_cext_sum(PostArgs a)
+// Cext and Cabs sums (before the 4 pi / |E|^2 factor), grid (ni x parts, nrhs): CTA
+// (i, part) sums the part-th of plane i's cells
+__global__ void __launch_bounds__(256) cabs_cext_sum(PostArgs a, int parts)
 {
     extern __shared__ float2 tab[];   // [nj] then [nl]
     __shared__ double scratch[8 * 2];
-    const int i = blockIdx.x, rhs = blockIdx.y, nj = a.nj, nl = a.nl;
+    const int i = blockIdx.x / parts, part = blockIdx.x - i * parts, rhs = blockIdx.y, nj = a.nj, nl = a.nl;
     const double *k = a.kinc + 3 * rhs, *E = a.einc + 6 * rhs;
     // centre n d0 / 2 (dda_func.cpp:1685), phase -k.(r - c')
     const double cx = a.ni * a.d0 / 2, cy = nj * a.d0 / 2, cz = nl * a.d0 / 2;
@@ -460,7 +461,8 @@ __global__ void __launch_bounds__(256) cabs_cext_sum(PostArgs a)
     const float2 *al = a.alpha + (size_t)rhs * a.nmat1;
     const signed char *occ = a.occ + (size_t)rhs * a.occ_stride;
     double v[2] = {0.0, 0.0};
-    for (int e = threadIdx.x; e < nj * nl; e += blockDim.x) {
+    const int e0 = (int)((long long)part * nj * nl / parts), e1 = (int)((long long)(part + 1) * nj * nl / parts);
+    for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
         const size_t q = (size_t)i * nj * nl + e;
         const int m = occ[q];
         const float2 alpha = al[m];
@@ -509,7 +511,7 @@ __host__ __device__ inline size_t zsum_smem(int nl, int nr)
 
 // grid (ni, group tiles of ZG, blocks), 256 threads
 template <int NR>
-__global__ void __launch_bounds__(256) ff_zsum(PostArgs a)
+__global__ void __launch_bounds__(256, 3) ff_zsum(PostArgs a)
 {
     constexpr int Q = 3 * NR, ZS = Q * ZR + 1;   // ZS: z stride of the staged chunk (float2)
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -711,75 +713,90 @@ __device__ inline dc rdotc(const double *v, const dc *e)
 }
 
 // One Mueller matrix per (orientation, angle), averaged over the scattering planes.
-// The two polarisations of orientation o are right-hand sides 2o and 2o+1.
-__global__ void mueller_avg(MuellerArgs m)
+// The two polarisations of orientation o are right-hand sides 2o and 2o+1.  Block of
+// MU_T threads: ppb (orientation, angle) pairs, a thread per (pair, plane) -- planes
+// pl, pl + npl, ... when there are more than MU_T -- then the planes' matrices are summed
+// in plane order (the order of the single-thread loop, so the same bits).
+constexpr int MU_T = 128;
+__global__ void __launch_bounds__(MU_T) mueller_avg(MuellerArgs m, int npl, int ppb)
 {
-    const int q = blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= m.norient * m.nangles) return;
-    const int o = q / m.nangles, ang = q % m.nangles;
-    const double *ki = m.kinc + 6 * o;      // rhs 2o
+    __shared__ double part[MU_T][17];
+    const int t = threadIdx.x, pr = t / npl, pl0 = t - pr * npl;
+    const int q = blockIdx.x * ppb + pr;
     double M[16];
     for (int k = 0; k < 16; k++) M[k] = 0.0;
-    dc E0[3], E1[3];
-    for (int c = 0; c < 3; c++) {
-        E0[c] = {m.einc[12 * o + 2 * c], m.einc[12 * o + 2 * c + 1]};
-        E1[c] = {m.einc[12 * o + 6 + 2 * c], m.einc[12 * o + 6 + 2 * c + 1]};
-    }
-    for (int pl = 0; pl < m.nplanes; pl++) {
-        const size_t dir = (size_t)pl * m.nangles + ang;
-        const double *ks = m.ksc + ((size_t)(2 * o) * m.ndir + dir) * 3;
-        const double *nv = m.normals + ((size_t)o * m.nplanes + pl) * 3;
-        const float2 *s0 = m.esc + ((size_t)(2 * o) * m.ndir + dir) * 3;
-        const float2 *s1 = m.esc + ((size_t)(2 * o + 1) * m.ndir + dir) * 3;
-        dc S0[3], S1[3];
+    if (pr < ppb && q < m.norient * m.nangles) {
+        const int o = q / m.nangles, ang = q % m.nangles;
+        const double *ki = m.kinc + 6 * o;      // rhs 2o
+        dc E0[3], E1[3];
         for (int c = 0; c < 3; c++) {
-            S0[c] = {s0[c].x, s0[c].y};
-            S1[c] = {s1[c].x, s1[c].y};
+            E0[c] = {m.einc[12 * o + 2 * c], m.einc[12 * o + 2 * c + 1]};
+            E1[c] = {m.einc[12 * o + 6 + 2 * c], m.einc[12 * o + 6 + 2 * c + 1]};
         }
-        // plane basis: across = normal, along = (k x n)/|k x n| for the incident beam and
-        // -(k_sc x n)/|k_sc x n| for the scattered one (mmuller.cpp:181-182)
-        double pin[3] = {ki[1] * nv[2] - ki[2] * nv[1], ki[2] * nv[0] - ki[0] * nv[2],
-                         ki[0] * nv[1] - ki[1] * nv[0]};
-        double psc[3] = {ks[1] * nv[2] - ks[2] * nv[1], ks[2] * nv[0] - ks[0] * nv[2],
-                         ks[0] * nv[1] - ks[1] * nv[0]};
-        const double a1 = sqrt(pin[0] * pin[0] + pin[1] * pin[1] + pin[2] * pin[2]);
-        const double a2 = sqrt(psc[0] * psc[0] + psc[1] * psc[1] + psc[2] * psc[2]);
-        for (int c = 0; c < 3; c++) {
-            pin[c] /= a1;
-            psc[c] = -psc[c] / a2;
+        for (int pl = pl0; pl < m.nplanes; pl += npl) {
+            const size_t dir = (size_t)pl * m.nangles + ang;
+            const double *ks = m.ksc + ((size_t)(2 * o) * m.ndir + dir) * 3;
+            const double *nv = m.normals + ((size_t)o * m.nplanes + pl) * 3;
+            const float2 *s0 = m.esc + ((size_t)(2 * o) * m.ndir + dir) * 3;
+            const float2 *s1 = m.esc + ((size_t)(2 * o + 1) * m.ndir + dir) * 3;
+            dc S0[3], S1[3];
+            for (int c = 0; c < 3; c++) {
+                S0[c] = {s0[c].x, s0[c].y};
+                S1[c] = {s1[c].x, s1[c].y};
+            }
+            // plane basis: across = normal, along = (k x n)/|k x n| for the incident beam and
+            // -(k_sc x n)/|k_sc x n| for the scattered one (mmuller.cpp:181-182)
+            double pin[3] = {ki[1] * nv[2] - ki[2] * nv[1], ki[2] * nv[0] - ki[0] * nv[2],
+                             ki[0] * nv[1] - ki[1] * nv[0]};
+            double psc[3] = {ks[1] * nv[2] - ks[2] * nv[1], ks[2] * nv[0] - ks[0] * nv[2],
+                             ks[0] * nv[1] - ks[1] * nv[0]};
+            const double a1 = sqrt(pin[0] * pin[0] + pin[1] * pin[1] + pin[2] * pin[2]);
+            const double a2 = sqrt(psc[0] * psc[0] + psc[1] * psc[1] + psc[2] * psc[2]);
+            for (int c = 0; c < 3; c++) {
+                pin[c] /= a1;
+                psc[c] = -psc[c] / a2;
+            }
+            const dc i0n = rdotc(nv, E0), i1n = rdotc(nv, E1), i0p = rdotc(pin, E0), i1p = rdotc(pin, E1);
+            const dc det = dcs(dcm(i0n, i1p), dcm(i1n, i0p));
+            const dc den = {-det.i, det.r};   // i * det
+            const dc s0n = rdotc(nv, S0), s1n = rdotc(nv, S1), s0p = rdotc(psc, S0), s1p = rdotc(psc, S1);
+            const dc A = dcdiv(dcs(dcm(s1p, i0n), dcm(s0p, i1n)), den);
+            const dc B = dcdiv(dcs(dcm(s0p, i1p), dcm(s1p, i0p)), den);
+            const dc C = dcdiv(dcs(dcm(s1n, i0n), dcm(s0n, i1n)), den);
+            const dc D = dcdiv(dcs(dcm(s0n, i1p), dcm(s1n, i0p)), den);
+            const double aa = A.r * A.r + A.i * A.i, bb = B.r * B.r + B.i * B.i,
+                         cc = C.r * C.r + C.i * C.i, dd = D.r * D.r + D.i * D.i;
+            const dc ab = dcm(A, dcc(B)), dc_ = dcm(D, dcc(C)), ac = dcm(A, dcc(C)),
+                     db = dcm(D, dcc(B)), da = dcm(D, dcc(A)), bc = dcm(B, dcc(C)),
+                     ad = dcm(A, dcc(D)), cb = dcm(C, dcc(B)), ca = dcm(C, dcc(A));
+            // JonesToMuller, mmuller.cpp:254-314
+            M[0] += 0.5 * (aa + bb + cc + dd);
+            M[1] += 0.5 * (aa - bb + cc - dd);
+            M[2] += dca(ab, dc_).r;
+            M[3] += dcs(ab, dc_).i;
+            M[4] += 0.5 * (aa + bb - cc - dd);
+            M[5] += 0.5 * (aa - bb - cc + dd);
+            M[6] += dcs(ab, dc_).r;
+            M[7] += dca(ab, dc_).i;
+            M[8] += dca(ac, db).r;
+            M[9] += dcs(ac, db).r;
+            M[10] += dca(da, bc).r;
+            M[11] += dca(ad, cb).i;
+            M[12] += dca(ca, db).i;
+            M[13] += dcs(ca, db).i;
+            M[14] += dcs(da, bc).i;
+            M[15] += dcs(da, bc).r;
         }
-        const dc i0n = rdotc(nv, E0), i1n = rdotc(nv, E1), i0p = rdotc(pin, E0), i1p = rdotc(pin, E1);
-        const dc det = dcs(dcm(i0n, i1p), dcm(i1n, i0p));
-        const dc den = {-det.i, det.r};   // i * det
-        const dc s0n = rdotc(nv, S0), s1n = rdotc(nv, S1), s0p = rdotc(psc, S0), s1p = rdotc(psc, S1);
-        const dc A = dcdiv(dcs(dcm(s1p, i0n), dcm(s0p, i1n)), den);
-        const dc B = dcdiv(dcs(dcm(s0p, i1p), dcm(s1p, i0p)), den);
-        const dc C = dcdiv(dcs(dcm(s1n, i0n), dcm(s0n, i1n)), den);
-        const dc D = dcdiv(dcs(dcm(s0n, i1p), dcm(s1n, i0p)), den);
-        const double aa = A.r * A.r + A.i * A.i, bb = B.r * B.r + B.i * B.i,
-                     cc = C.r * C.r + C.i * C.i, dd = D.r * D.r + D.i * D.i;
-        const dc ab = dcm(A, dcc(B)), dc_ = dcm(D, dcc(C)), ac = dcm(A, dcc(C)),
-                 db = dcm(D, dcc(B)), da = dcm(D, dcc(A)), bc = dcm(B, dcc(C)),
-                 ad = dcm(A, dcc(D)), cb = dcm(C, dcc(B)), ca = dcm(C, dcc(A));
-        // JonesToMuller, mmuller.cpp:254-314
-        M[0] += 0.5 * (aa + bb + cc + dd);
-        M[1] += 0.5 * (aa - bb + cc - dd);
-        M[2] += dca(ab, dc_).r;
-        M[3] += dcs(ab, dc_).i;
-        M[4] += 0.5 * (aa + bb - cc - dd);
-        M[5] += 0.5 * (aa - bb - cc + dd);
-        M[6] += dcs(ab, dc_).r;
-        M[7] += dca(ab, dc_).i;
-        M[8] += dca(ac, db).r;
-        M[9] += dcs(ac, db).r;
-        M[10] += dca(da, bc).r;
-        M[11] += dca(ad, cb).i;
-        M[12] += dca(ca, db).i;
-        M[13] += dcs(ca, db).i;
-        M[14] += dcs(da, bc).i;
-        M[15] += dcs(da, bc).r;
     }
-    for (int k = 0; k < 16; k++) m.out[(size_t)q * 16 + k] = M[k] / m.nplanes;
+    for (int k = 0; k < 16; k++) part[t][k] = M[k];
+    __syncthreads();
+    for (int e = t; e < ppb * 16; e += MU_T) {
+        const int p = e >> 4, k = e & 15, qq = blockIdx.x * ppb + p;
+        if (qq >= m.norient * m.nangles) continue;
+        double v = 0.0;
+        for (int u = 0; u < npl; u++) v += part[p * npl + u][k];
+        m.out[(size_t)qq * 16 + k] = v / m.nplanes;
+    }
 }
 
 inline unsigned nblk(size_t n, int t) { return (unsigned)((n + t - 1) / t); }
@@ -809,6 +826,11 @@ cudaError_t post_prepare(int nj, int nl)
     if (e == cudaSuccess) e = raise_smem_limit((const void *)farfield_sum<false, 1, 4>, bytes);
     if (e == cudaSuccess) e = raise_smem_limit((const void *)ff_zsum<1>, (int)zsum_smem(nl, 1));
     if (e == cudaSuccess) e = raise_smem_limit((const void *)ff_zsum<2>, (int)zsum_smem(nl, 2));
+    // three group-sum CTAs per SM want the largest shared-memory carveout
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute((const void *)ff_zsum<1>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute((const void *)ff_zsum<2>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     return e;
 }
 
@@ -884,6 +906,15 @@ void plan_kz_groups(const double *ks, int nrhs, int ndir, bool pairs, int ni, in
     }
 }
 
+// parts of a plane per cross-section CTA: about four CTAs per SM, 256 cells per CTA at least
+static int cc_parts(const PostArgs &a)
+{
+    int parts = 1;
+    while (parts < 16 && (long long)a.ni * a.nrhs * parts < 4 * 148 && (long long)a.nj * a.nl / (2 * parts) >= 256)
+        parts *= 2;
+    return parts;
+}
+
 cudaError_t launch_post(const PostArgs &a, float2 *esc, float *cabs, float *cext, cudaStream_t st, int *kernels)
 {
     cudaError_t e;
@@ -901,7 +932,8 @@ cudaError_t launch_post(const PostArgs &a, float2 *esc, float *cabs, float *cext
             ff_zsum<1><<<gz, 256, zsum_smem(a.nl, 1), st>>>(a);
             ff_xysum<1><<<gx, 256, xysum_smem(a.nj, a.kz_slice, 1), st>>>(a);
         }
-        cabs_cext_sum<<<dim3(a.ni, a.nrhs), 256, (a.nj + a.nl) * sizeof(float2), st>>>(a);
+        const int parts = cc_parts(a);
+        cabs_cext_sum<<<dim3(a.ni * parts, a.nrhs), 256, (a.nj + a.nl) * sizeof(float2), st>>>(a, parts);
         nk += 3;
     } else if (a.ndir > 0) {
         // far field with the cross sections summed by the first direction chunk
@@ -917,7 +949,8 @@ cudaError_t launch_post(const PostArgs &a, float2 *esc, float *cabs, float *cext
         }
         nk += 1;
     } else {
-        cabs_cext_sum<<<dim3(a.ni, a.nrhs), 256, (a.nj + a.nl) * sizeof(float2), st>>>(a);
+        const int parts = cc_parts(a);
+        cabs_cext_sum<<<dim3(a.ni * parts, a.nrhs), 256, (a.nj + a.nl) * sizeof(float2), st>>>(a, parts);
         nk += 1;
     }
     const size_t nd = (size_t)a.nrhs * a.ndir;
@@ -931,7 +964,8 @@ cudaError_t launch_mueller(const MuellerArgs &m, cudaStream_t st)
 {
     const size_t n = (size_t)m.norient * m.nangles;
     if (n == 0) return cudaSuccess;
-    mueller_avg<<<nblk(n, 128), 128, 0, st>>>(m);
+    const int npl = m.nplanes < MU_T ? m.nplanes : MU_T, ppb = MU_T / npl;
+    mueller_avg<<<nblk(n, ppb), MU_T, 0, st>>>(m, npl, ppb);
     return cudaGetLastError();
 }
 
