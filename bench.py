@@ -210,6 +210,8 @@ def main():
     ap.add_argument("--plain", type=int, default=8, help="orientations timed on the plain path")
     ap.add_argument("--cpu-samples", type=int, default=0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the other configurations appended to the headline line")
     ap.add_argument("--profile-matvec", type=int, default=0, metavar="NRHS",
                     help="only run the matvec on NRHS right-hand sides (for ncu captures)")
     ap.add_argument("--grid", type=int, default=GRID)
@@ -425,10 +427,50 @@ def main():
             "check": {"cext_mean": job["cext"] / job["count"], "cabs_mean": job["cabs"] / job["count"],
                       "samples": job["count"]},
         }
-        print(json.dumps(line), flush=True)
     ctx.close()
     if distributed:
         dist.destroy_process_group()
+    if rank == 0:
+        if world == 1 and not args.no_extras:
+            line["other_configs"] = other_configs(args)
+        print(json.dumps(line), flush=True)
+
+
+def other_configs(args):
+    """The other configurations, measured in the same run after the headline (one GPU):
+    the plain mid configuration (per-sample time, far field by kz groups and direct), the
+    realisations of the three lattice sizes as one group graph (device and end-to-end
+    rates, the 128^3 matvec's roofline fraction) and the differentiation configuration's
+    adjoint pass (backward / forward time and matvecs).  Each runs its own workload
+    function with shortened step counts; its JSON line is condensed here."""
+    import contextlib
+    import io
+    runs = (("plain_mid", plain_run, {"steps": 5, "warmup": 2, "no_cpu": True}),
+            ("realizations", realizations_run, {"steps": 3, "warmup": 3, "no_cpu": True}),
+            ("adjoint", adjoint_run, {"grid": 64}))
+    keep = {"plain_mid": lambda r: {"ms_per_sample": r["graph"]["ms_per_sample"],
+                                    "ms_per_sample_direct_farfield": r["graph_direct_farfield"]["ms_per_sample"],
+                                    "ms_per_sample_host_loop": r["host_loop"]["ms_per_sample"],
+                                    "cext": r["cext"], "cabs": r["cabs"], "workload": r["workload"]},
+            "realizations": lambda r: {"value": r["value"], "unit": r["unit"], "e2e": r["e2e"]["value"],
+                                       "graph_launches_per_step": r["config"]["graph_launches_per_step"],
+                                       "matvec_roofline_frac": r["roofline"]["frac"],
+                                       "matvec_kernel": r["roofline"]["kernel"], "steps": r["steps"]},
+            "adjoint": lambda r: {k: r[k] for k in ("workload", "dipoles", "forward_s", "backward_s",
+                                                    "backward_over_forward", "forward_matvecs",
+                                                    "backward_matvecs")}}
+    out = {}
+    for name, fn, kw in runs:
+        a = argparse.Namespace(**vars(args))
+        a.__dict__.update(kw)
+        buf = io.StringIO()
+        try:
+            with contextlib.redirect_stdout(buf):
+                fn(a)
+            out[name] = keep[name](json.loads(buf.getvalue().strip().splitlines()[-1]))
+        except Exception as e:   # reported in the line, never fatal to the headline
+            out[name] = {"error": repr(e)[:300]}
+    return out
 
 
 def profile_matvec(args):
