@@ -97,6 +97,64 @@ DDA_DEV void row_fft_from_regs(float2 *row, int lane_sub, bool valid, float2 (&v
     __syncwarp();
 }
 
+// Row role for two lines at once when N = R1 R2 with R1 = 2 R2 (32 = 8 x 4, 128 = 16 x 8):
+// lanes [0, R2) of the group hold line A's step-A inputs and lanes [R2, R1) line B's (the
+// positions t2 + R2 r with t2 = lane_sub mod R2), so every lane works in step A, where the
+// single-line form idles half of them; step B takes both lines on all R1 lanes.
+template <int N, bool INV>
+DDA_DEV void row_fft2_from_regs(float2 *rowA, float2 *rowB, int lane_sub, bool validA, bool validB,
+                                float2 (&v)[Sp<N>::R1], const float2 *__restrict__ tw)
+{
+    constexpr int R1 = Sp<N>::R1, R2 = Sp<N>::R2;
+    static_assert(R1 == 2 * R2, "two lines per lane group need R1 = 2 R2");
+    const int h = lane_sub >= R2, t2 = lane_sub - h * R2;
+    float2 *row = h ? rowB : rowA;
+    if (h ? validB : validA) {
+        dft_reg<R1, INV>(v);
+#pragma unroll
+        for (int k1 = 1; k1 < R1; k1++) v[k1] = cmul(v[k1], twid<INV>(tw, t2 * k1));
+#pragma unroll
+        for (int k1 = 0; k1 < R1; k1++) row[spos(t2 + R2 * k1)] = v[k1];
+    }
+    __syncwarp();
+    // step B, line A then line B (one line's R2 values live at a time)
+    const int k1 = lane_sub;
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+        float2 *ln = q ? rowB : rowA;
+        const bool ok = q ? validB : validA;
+        float2 u[R2];
+        if (ok) {
+#pragma unroll
+            for (int t = 0; t < R2; t++) u[t] = ln[spos(R2 * k1 + t)];
+            dft_reg<R2, INV>(u);
+        }
+        __syncwarp();
+        if (ok) {
+#pragma unroll
+            for (int k2 = 0; k2 < R2; k2++) ln[spos(k1 + R1 * k2)] = u[k2];
+        }
+    }
+    __syncwarp();
+}
+
+// Two lines per lane group in the row role of a yz pass of NT threads: R1 = 2 R2 and the
+// rows fill at least two passes of one line per group.
+template <int NJ, int NL, int NT>
+__host__ __device__ constexpr bool rows_paired()
+{
+    return Sp<NL>::R1 == 2 * Sp<NL>::R2 && NJ >= 2 * (NT / Sp<NL>::RM);
+}
+
+// Both y halves' step A at once in the column role (R1 = 2 R2 on the y lines): the
+// sub-lines [0, R2) take half 0 in place and [R2, R1) half 1 into a scratch block of NJ x
+// (NT / RM) elements after the plane.
+template <int NJ>
+__host__ __device__ constexpr bool halves_paired()
+{
+    return Sp<NJ>::R1 == 2 * Sp<NJ>::R2;
+}
+
 // ------------------------------------------------------------------------------ K1
 // CTA (i, component, z half hl): z-forward of the NJ rows of plane i (half hl only), then
 // y-forward of the NL columns for both y halves; writes work rows in split order.
@@ -125,7 +183,12 @@ __global__ void __launch_bounds__(NT) k1f(MatvecArgs a)
         // dda_func.cpp:654-689) with the products of the separate pass, in its order:
         // ((x phase * y phase) * z phase) * alpha_m * E_c
         constexpr int RM = SL::RM, RPP = NT / RM, R1 = SL::R1, R2 = SL::R2;
+        // PR: two rows per lane group (lane half h, step-A index t2); else one row
+        constexpr bool PR = rows_paired<NJ, NL, NT>();
+        constexpr int ROWS = PR ? 2 * RPP : RPP;
         const int sub = threadIdx.x % RM, rr = threadIdx.x / RM;
+        const int h = PR ? (sub >= R2) : 0, t2 = sub - h * R2, rbase = PR ? 2 * rr : rr;
+        const bool lane_a = PR || sub < R2;   // holds step-A inputs
         const Epilogue &ep = a.ep;
         const float2 *tab = a.inc_tab + (size_t)rhs * (NJ + NL + ni);
         const float2 tx = tab[NJ + NL + i];
@@ -134,7 +197,7 @@ __global__ void __launch_bounds__(NT) k1f(MatvecArgs a)
         constexpr bool tz_reg = NL <= 64;
         float2 tz[tz_reg ? R1 : 1];
 #pragma unroll
-        for (int r = 0; r < (tz_reg ? R1 : 1); r++) tz[r] = sub < R2 ? tab[NJ + sub + R2 * r] : czero();
+        for (int r = 0; r < (tz_reg ? R1 : 1); r++) tz[r] = lane_a ? tab[NJ + t2 + R2 * r] : czero();
         const double *E = a.einc + 6 * rhs;
         const float2 Ef = make_float2((float)E[2 * c], (float)E[2 * c + 1]);
         float2 Ep[2][3];   // pair: the incident fields of both polarisations
@@ -154,34 +217,34 @@ __global__ void __launch_bounds__(NT) k1f(MatvecArgs a)
         float2 *pout = a.inc_out + (size_t)rhs * a.fstride + ((size_t)c * ni + i) * (NJ * NL);
         // the occupancy of the next pass's row is loaded while this pass's row is transformed
         auto load = [&](int row, int (&o)[R1], float2 &ty) {
-            if (row < NJ && sub < R2) {
+            if (row < NJ && lane_a) {
 #pragma unroll
-                for (int r = 0; r < R1; r++) o[r] = ob[row * NL + sub + R2 * r];
+                for (int r = 0; r < R1; r++) o[r] = ob[row * NL + t2 + R2 * r];
                 ty = tab[row];
             }
         };
         int o[R1], on[R1];
         float2 ty = czero(), tyn = czero();
-        load(rr, o, ty);
+        load(rbase + h, o, ty);
 #pragma unroll 1
-        for (int r0 = 0; r0 < NJ; r0 += RPP) {
-            const int row = r0 + rr;
-            if (r0 + RPP < NJ) load(row + RPP, on, tyn);
+        for (int r0 = 0; r0 < NJ; r0 += ROWS) {
+            const int row0 = r0 + rbase, row = row0 + h;
+            if (r0 + ROWS < NJ) load(row + ROWS, on, tyn);
             float2 v[R1];
-            if (row < NJ && sub < R2) {
+            if (row < NJ && lane_a) {
                 const float2 txy = cmul(tx, ty);
 #pragma unroll
                 for (int r = 0; r < R1; r++) {
                     const int m = o[r];
                     const bool act = rt ? ((m & 1) ? mv1 : mv0) : ep.mv[m] != 0;
                     float2 val = czero();
-                    const float2 tzr = tz_reg ? tz[tz_reg ? r : 0] : __ldg(&tab[NJ + sub + R2 * r]);
+                    const float2 tzr = tz_reg ? tz[tz_reg ? r : 0] : __ldg(&tab[NJ + t2 + R2 * r]);
                     if constexpr (PAIR) {
                         // val = phi; the dipoles phi E_q of both polarisations, the same
                         // float operations as the single form's ((phi) E_c)
                         if (act) val = cmul(cmul(txy, tzr), rt ? ((m & 1) ? al1 : al0) : al[m]);
                         if (hl == 0) {
-                            const size_t o = (size_t)row * NL + sub + R2 * r;
+                            const size_t o = (size_t)row * NL + t2 + R2 * r;
 #pragma unroll
                             for (int q = 0; q < 2; q++)
 #pragma unroll
@@ -190,39 +253,51 @@ __global__ void __launch_bounds__(NT) k1f(MatvecArgs a)
                         }
                     } else {
                         if (act) val = cmul(cmul(cmul(txy, tzr), rt ? ((m & 1) ? al1 : al0) : al[m]), Ef);
-                        if (hl == 0) pout[row * NL + sub + R2 * r] = val;
+                        if (hl == 0) pout[row * NL + t2 + R2 * r] = val;
                     }
-                    v[r] = hl ? cmul(val, __ldg(&hwl[sub + R2 * r])) : val;
+                    v[r] = hl ? cmul(val, __ldg(&hwl[t2 + R2 * r])) : val;
                 }
             }
-            row_fft_from_regs<NL, false>(Z + (row < NJ ? row : 0) * PS, sub, row < NJ, v, twl);
+            if constexpr (PR)
+                row_fft2_from_regs<NL, false>(Z + (row0 < NJ ? row0 : 0) * PS, Z + (row0 + 1 < NJ ? row0 + 1 : 0) * PS,
+                                              sub, row0 < NJ, row0 + 1 < NJ, v, twl);
+            else
+                row_fft_from_regs<NL, false>(Z + (row < NJ ? row : 0) * PS, sub, row < NJ, v, twl);
 #pragma unroll
             for (int r = 0; r < R1; r++) o[r] = on[r];
             ty = tyn;
         }
     } else {
-        constexpr int RM = SL::RM, RPP = NT / RM;   // rows per pass
+        constexpr int RM = SL::RM, RPP = NT / RM, R1 = SL::R1, R2 = SL::R2;
+        constexpr bool PR = rows_paired<NJ, NL, NT>();
+        constexpr int ROWS = PR ? 2 * RPP : RPP;   // rows per pass
         const int sub = threadIdx.x % RM, rr = threadIdx.x / RM;
+        const int h = PR ? (sub >= R2) : 0, t2 = sub - h * R2, rbase = PR ? 2 * rr : rr;
+        const bool lane_a = PR || sub < R2;
         // the next pass's row is loaded while this pass's row is transformed
-        auto load = [&](int row, float2 (&v)[SL::R1]) {
-            if (row < NJ && sub < SL::R2) {
+        auto load = [&](int row, float2 (&v)[R1]) {
+            if (row < NJ && lane_a) {
 #pragma unroll
-                for (int r = 0; r < SL::R1; r++) v[r] = src[row * NL + sub + SL::R2 * r];
+                for (int r = 0; r < R1; r++) v[r] = src[row * NL + t2 + R2 * r];
             }
         };
-        float2 v[SL::R1], vn[SL::R1];
-        load(rr, v);
+        float2 v[R1], vn[R1];
+        load(rbase + h, v);
 #pragma unroll 1
-        for (int r0 = 0; r0 < NJ; r0 += RPP) {
-            const int row = r0 + rr;
-            if (r0 + RPP < NJ) load(row + RPP, vn);
-            if (hl && row < NJ && sub < SL::R2) {
+        for (int r0 = 0; r0 < NJ; r0 += ROWS) {
+            const int row0 = r0 + rbase, row = row0 + h;
+            if (r0 + ROWS < NJ) load(row + ROWS, vn);
+            if (hl && row < NJ && lane_a) {
 #pragma unroll
-                for (int r = 0; r < SL::R1; r++) v[r] = cmul(v[r], __ldg(&hwl[sub + SL::R2 * r]));
+                for (int r = 0; r < R1; r++) v[r] = cmul(v[r], __ldg(&hwl[t2 + R2 * r]));
             }
-            row_fft_from_regs<NL, false>(Z + (row < NJ ? row : 0) * PS, sub, row < NJ, v, twl);
+            if constexpr (PR)
+                row_fft2_from_regs<NL, false>(Z + (row0 < NJ ? row0 : 0) * PS, Z + (row0 + 1 < NJ ? row0 + 1 : 0) * PS,
+                                              sub, row0 < NJ, row0 + 1 < NJ, v, twl);
+            else
+                row_fft_from_regs<NL, false>(Z + (row < NJ ? row : 0) * PS, sub, row < NJ, v, twl);
 #pragma unroll
-            for (int r = 0; r < SL::R1; r++) v[r] = vn[r];
+            for (int r = 0; r < R1; r++) v[r] = vn[r];
         }
     }
     __syncthreads();
@@ -234,6 +309,54 @@ __global__ void __launch_bounds__(NT) k1f(MatvecArgs a)
         static_assert(CPP >= 1, "block too small");
         const int col0 = threadIdx.x % CPP, sub = threadIdx.x / CPP;
         float2 *dst = a.work + (size_t)rhs * a.wstride + ((size_t)c * ni + i) * (2 * NJ) * (2 * NL);
+        if constexpr (halves_paired<NJ>()) {
+            // sub-lines [0, R2) transform half 0 in place, [R2, R1) half 1 into the scratch
+            // block S [NJ][CPP]; then every sub-line finishes both halves (step B)
+            float2 *S = Z + NJ * PS;
+            const int hy = sub >= R2, t2 = sub - hy * R2;
+#pragma unroll 1
+            for (int cbase = 0; cbase < NL; cbase += CPP) {
+                const int col = cbase + col0;
+                const bool ok = col < NL;
+                float2 v[R1];
+                if (ok) {
+#pragma unroll
+                    for (int r = 0; r < R1; r++) v[r] = Z[(t2 + R2 * r) * PS + spos(col)];
+                }
+                __syncthreads();
+                if (ok) {
+                    if (hy) {
+#pragma unroll
+                        for (int r = 0; r < R1; r++) v[r] = cmul(v[r], __ldg(&hwj[t2 + R2 * r]));
+                    }
+                    dft_reg<R1, false>(v);
+#pragma unroll
+                    for (int k1 = 1; k1 < R1; k1++) v[k1] = cmul(v[k1], twid<false>(twj, t2 * k1));
+                    if (hy) {
+#pragma unroll
+                        for (int k1 = 0; k1 < R1; k1++) S[(t2 + R2 * k1) * CPP + col0] = v[k1];
+                    } else {
+#pragma unroll
+                        for (int k1 = 0; k1 < R1; k1++) Z[(t2 + R2 * k1) * PS + spos(col)] = v[k1];
+                    }
+                }
+                __syncthreads();
+                if (ok) {
+#pragma unroll
+                    for (int h2 = 0; h2 < 2; h2++) {
+                        float2 u[R2];
+#pragma unroll
+                        for (int t = 0; t < R2; t++)
+                            u[t] = h2 ? S[(R2 * sub + t) * CPP + col0] : Z[(R2 * sub + t) * PS + spos(col)];
+                        dft_reg<R2, false>(u);
+                        float2 *d = dst + (size_t)(h2 * NJ) * (2 * NL) + hl * NL + col;
+#pragma unroll
+                        for (int k2 = 0; k2 < R2; k2++) d[(size_t)(sub + R1 * k2) * (2 * NL)] = u[k2];
+                    }
+                }
+                __syncthreads();
+            }
+        } else {
 #pragma unroll 1
         for (int cbase = 0; cbase < NL; cbase += CPP) {
             const int col = cbase + col0;
@@ -269,6 +392,7 @@ __global__ void __launch_bounds__(NT) k1f(MatvecArgs a)
                 }
                 __syncthreads();
             }
+        }
         }
     }
 }
@@ -849,7 +973,54 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(NT) k3f(MatvecArgs a
     const float2 *twl = a.L.tw_l, *hwl = a.L.tw_l + NL, *twj = a.L.tw_j, *hwj = a.L.tw_j + NJ;
 
     // ---- y inverse on this half's columns: x[j] = IDFT(even)[j] + W^-j IDFT(odd)[j]
-    {
+    if constexpr (halves_paired<NJ>()) {
+        // sub-lines [0, R2) take the even half (step A in place), [R2, R1) the odd half
+        // (into the scratch block S [NJ][CPP]); every sub-line then finishes both and sums
+        constexpr int R1 = SJ::R1, R2 = SJ::R2, RM = SJ::RM;
+        constexpr int CPP = NT / RM;
+        const int col0 = threadIdx.x % CPP, sub = threadIdx.x / CPP;
+        const int hy = sub >= R2, t2 = sub - hy * R2;
+        float2 *S = Q + NJ * PS;
+#pragma unroll 1
+        for (int cbase = 0; cbase < NL; cbase += CPP) {
+            const int col = cbase + col0;
+            const bool ok = col < NL;
+            if (ok) {
+                float2 v[R1];
+#pragma unroll
+                for (int r = 0; r < R1; r++) v[r] = src[(size_t)(hy * NJ + t2 + R2 * r) * (2 * NL) + col];
+                dft_reg<R1, true>(v);
+#pragma unroll
+                for (int k1 = 1; k1 < R1; k1++) v[k1] = cmul(v[k1], twid<true>(twj, t2 * k1));
+                if (hy) {
+#pragma unroll
+                    for (int k1 = 0; k1 < R1; k1++) S[(t2 + R2 * k1) * CPP + col0] = v[k1];
+                } else {
+#pragma unroll
+                    for (int k1 = 0; k1 < R1; k1++) Q[(t2 + R2 * k1) * PS + spos(col)] = v[k1];
+                }
+            }
+            __syncthreads();
+            float2 y[R2];
+            if (ok) {
+                float2 u0[R2], u1[R2];
+#pragma unroll
+                for (int t = 0; t < R2; t++) {
+                    u0[t] = Q[(R2 * sub + t) * PS + spos(col)];
+                    u1[t] = S[(R2 * sub + t) * CPP + col0];
+                }
+                dft_reg<R2, true>(u0);
+                dft_reg<R2, true>(u1);
+#pragma unroll
+                for (int k2 = 0; k2 < R2; k2++) y[k2] = cadd(u0[k2], cmulc(u1[k2], __ldg(&hwj[sub + R1 * k2])));
+            }
+            __syncthreads();
+            if (ok) {
+#pragma unroll
+                for (int k2 = 0; k2 < R2; k2++) Q[(sub + R1 * k2) * PS + spos(col)] = y[k2];
+            }
+        }
+    } else {
         constexpr int R1 = SJ::R1, R2 = SJ::R2, RM = SJ::RM;
         constexpr int CPP = NT / RM;
         const int col0 = threadIdx.x % CPP, sub = threadIdx.x / CPP;
@@ -906,21 +1077,35 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(NT) k3f(MatvecArgs a
 
     // ---- z inverse of the rows (this half's spectral columns), row role
     {
-        constexpr int RM = SL::RM, RPP = NT / RM;
+        constexpr int RM = SL::RM, RPP = NT / RM, R1 = SL::R1, R2 = SL::R2;
+        // PR: two rows per lane group (lane half h, step-A index t2); else one row
+        constexpr bool PR = rows_paired<NJ, NL, NT>();
+        constexpr int ROWS = PR ? 2 * RPP : RPP;
         const int sub = threadIdx.x % RM, rr = threadIdx.x / RM;
+        const int h = PR ? (sub >= R2) : 0, t2 = sub - h * R2, rbase = PR ? 2 * rr : rr;
+        const bool lane_a = PR || sub < R2;
 #pragma unroll 1
-        for (int r0 = 0; r0 < NJ; r0 += RPP) {
-            const int row = r0 + rr;
-            float2 v[SL::R1];
-            if (row < NJ && sub < SL::R2) {
+        for (int r0 = 0; r0 < NJ; r0 += ROWS) {
+            const int row0 = r0 + rbase, row = row0 + h;
+            float2 v[R1];
+            if (row < NJ && lane_a) {
 #pragma unroll
-                for (int r = 0; r < SL::R1; r++) v[r] = Q[row * PS + spos(sub + SL::R2 * r)];
+                for (int r = 0; r < R1; r++) v[r] = Q[row * PS + spos(t2 + R2 * r)];
             }
             __syncwarp();
-            row_fft_from_regs<NL, true>(Q + (row < NJ ? row : 0) * PS, sub, row < NJ, v, twl);
-            if (hl == 1 && row < NJ) {
+            if constexpr (PR)
+                row_fft2_from_regs<NL, true>(Q + (row0 < NJ ? row0 : 0) * PS, Q + (row0 + 1 < NJ ? row0 + 1 : 0) * PS,
+                                             sub, row0 < NJ, row0 + 1 < NJ, v, twl);
+            else
+                row_fft_from_regs<NL, true>(Q + (row < NJ ? row : 0) * PS, sub, row < NJ, v, twl);
+            if (hl == 1) {
                 // odd half: times W_2NL^-l
-                for (int l = sub; l < NL; l += RM) Q[row * PS + spos(l)] = cmulc(Q[row * PS + spos(l)], __ldg(&hwl[l]));
+#pragma unroll
+                for (int q = 0; q < (PR ? 2 : 1); q++) {
+                    const int rw = row0 + q;
+                    if (rw < NJ)
+                        for (int l = sub; l < NL; l += RM) Q[rw * PS + spos(l)] = cmulc(Q[rw * PS + spos(l)], __ldg(&hwl[l]));
+                }
             }
         }
     }
@@ -1000,17 +1185,19 @@ constexpr int yz_threads(int v)
     return v == 0 ? t0 : v == 1 ? (t0 == 512 ? 256 : 512) : 128;
 }
 
-template <int NJ, int NL>
+template <int NJ, int NL, int NT>
 constexpr size_t yz_smem()
 {
-    return (size_t)NJ * Sp<NL>::PS * sizeof(float2);   // one plane, 128 KB at 128 x 128
+    // one plane (128 KB at 128 x 128), and the odd y half's scratch when the halves pair
+    return (size_t)NJ * Sp<NL>::PS * sizeof(float2) +
+           (halves_paired<NJ>() ? (size_t)NJ * (NT / Sp<NJ>::RM) * sizeof(float2) : 0);
 }
 
 template <int NJ, int NL, int V>
 void launch_yz_v(const MatvecArgs &a, int fwd, cudaStream_t st)
 {
     constexpr int NT = yz_threads<NJ, NL>(V);
-    constexpr size_t S = yz_smem<NJ, NL>();
+    constexpr size_t S = yz_smem<NJ, NL, NT>();
     if (fwd && a.inc && a.pair) k1f<NJ, NL, NT, 2><<<dim3(2 * a.L.ni, 1, a.nrhs / 2), NT, S, st>>>(a);
     else if (fwd && a.inc) k1f<NJ, NL, NT, 1><<<dim3(2 * a.L.ni, 3, a.nrhs), NT, S, st>>>(a);
     else if (fwd) k1f<NJ, NL, NT, 0><<<dim3(2 * a.L.ni, 3, a.nrhs), NT, S, st>>>(a);
@@ -1029,7 +1216,7 @@ template <int NJ, int NL, int V>
 cudaError_t prep_yz_v()
 {
     constexpr int NT = yz_threads<NJ, NL>(V);
-    constexpr int S = (int)yz_smem<NJ, NL>();
+    constexpr int S = (int)yz_smem<NJ, NL, NT>();
     cudaError_t e = cudaFuncSetAttribute(k1f<NJ, NL, NT, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, S);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k1f<NJ, NL, NT, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, S);
