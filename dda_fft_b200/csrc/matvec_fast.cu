@@ -12,9 +12,9 @@
 //                  contiguous run of the warp.
 // Shared planes use the swizzled row layout pos(p) = p ^ ((p >> 3) & 7), a permutation
 // inside each aligned block of 8 elements, with a row stride PS = N + 8 or N + 4 float2
-// (PS = RM mod 16).  A warp reading 32 consecutive columns of one row, a row group reading
-// positions t2 + R2 r (step A) and a row group reading positions R2 k1 + t (step B) all
-// touch distinct banks.
+// (PS = RM mod 16, or 8 mod 16 where two rows share a half-warp).  A warp reading 32
+// consecutive columns of one row, a row group reading positions t2 + R2 r (step A) and a
+// row group reading positions R2 k1 + t (step B) all touch distinct banks.
 #include <cooperative_groups.h>
 #include <cuda.h>   // CUtensorMap (the type only; maps are encoded in ddagpu.cu)
 
@@ -33,8 +33,9 @@ template <int N>
 struct Sp {
     static constexpr int R1 = fft_split<N>::R1, R2 = fft_split<N>::R2;
     static constexpr int RM = R1 > R2 ? R1 : R2;
-    // row stride = RM (mod 16) float2: the rows of one half-warp land in disjoint banks
-    static constexpr int PS = N + ((RM % 16) - (N % 16) + 16) % 16;
+    // row stride = RM (mod 16) float2: the rows of one half-warp land in disjoint banks; 8
+    // (mod 16) when R1 = 2 R2, where a half-warp holds two rows in step A (row_fft2_from_regs)
+    static constexpr int PS = N + (((R1 == 2 * R2 ? 8 : RM % 16) - (N % 16) + 16) % 16);
 };
 
 // The x pass's line factorisation N = R1 R2: ALT 0 is fft_split<N>; ALT 1 the second
