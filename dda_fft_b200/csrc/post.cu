@@ -9,6 +9,7 @@
 // The phase is separable, exp(i kx x) exp(i ky y) exp(i kz z), so each CTA builds small
 // tables and the inner loop is three complex multiply-adds per dipole and direction.
 #include <algorithm>
+#include <cmath>
 #include <mutex>
 
 #include "common.cuh"
@@ -851,6 +852,9 @@ void plan_kz_groups(const double *ks, int nrhs, int ndir, bool pairs, int ni, in
     P.kz.clear();
     if (mode == 1 || ndir <= 0 || nrhs <= 0 || !ks) return;
     const int NR = pairs && nrhs % 2 == 0 ? 2 : 1, nb = nrhs / NR;
+    // a direction that is not finite keeps the direct form (and the sort its strict order)
+    for (size_t q = 0; q < (size_t)nrhs * ndir * 3; q++)
+        if (!std::isfinite(ks[q])) return;
     // per block: direction indices sorted by kz (ties in index order), groups of equal kz
     std::vector<std::vector<int>> order((size_t)nb);
     std::vector<std::vector<int>> offs((size_t)nb);
