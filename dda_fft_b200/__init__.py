@@ -14,6 +14,7 @@ from .api import (  # noqa: F401
     RandomEllipsoid,
     StateFile,
     build,
+    farfield_plan,
     fixed_rotation,
     lib,
     library_path,
@@ -23,5 +24,5 @@ from .api import (  # noqa: F401
 )
 
 __all__ = ["Agglomerate", "BatchConfig", "Context", "DDAGPUError", "Group", "RandomEllipsoid", "StateFile",
-           "build", "fixed_rotation", "lib", "library_path", "mc_rotations", "num_angles",
+           "build", "farfield_plan", "fixed_rotation", "lib", "library_path", "mc_rotations", "num_angles",
            "sample_loop"]

@@ -128,6 +128,7 @@ def lib():
         L.ddagpu_get_kernels.argtypes = [_p]
         L.ddagpu_set_fast_variant.argtypes = [_p, _i, _i]
         L.ddagpu_set_farfield_mode.argtypes = [_p, _i]
+        L.ddagpu_farfield_plan.argtypes = [_p, _i, _i, _i, _i, _i, _i, C.c_double, _i, _p, _p]
         L.ddagpu_get_fast_variant.argtypes = [_p, C.POINTER(_i), C.POINTER(_i)]
         L.ddagpu_set_solver_graph.argtypes = [_p, _i]
         L.ddagpu_selftest_wait_timeout.argtypes = [_p, _i]
@@ -174,6 +175,19 @@ def mc_rotations(base_seed: int, count: int, worker: int = 0) -> np.ndarray:
     out = np.zeros((count, 3, 3))
     _check(lib().ddagpu_mc_rotations(C.c_ulonglong(base_seed), worker, count, _ptr(out)))
     return out
+
+
+def farfield_plan(ksc, grid, nact: float, nrhs: int = 1, pairs: bool = False, mode: int = 0):
+    """(groups, items) of the far field over the directions ksc of nrhs right-hand sides
+    (any shape of nrhs x ndir x 3 values) on a lattice `grid` with `nact` active cells per
+    right-hand side: groups 0 means one sum per direction (ddagpu_farfield_plan; no device
+    needed)."""
+    k = np.ascontiguousarray(ksc, np.float64).reshape(nrhs, -1, 3)
+    ni, nj, nl = (grid,) * 3 if np.isscalar(grid) else grid
+    g, it = C.c_int(), C.c_int()
+    _check(lib().ddagpu_farfield_plan(_ptr(k), k.shape[0], k.shape[1], int(pairs), ni, nj, nl,
+                                      float(nact), mode, C.byref(g), C.byref(it)))
+    return g.value, it.value
 
 
 def fixed_rotation(psi=0.0, iota=0.0, kappa=0.0) -> np.ndarray:

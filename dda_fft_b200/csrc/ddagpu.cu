@@ -2201,6 +2201,19 @@ int ddagpu_set_fast_variant(ddagpu_ctx *c, int x_variant, int yz_variant)
     return DDAGPU_OK;
 }
 
+int ddagpu_farfield_plan(const double *ksc, int nrhs, int ndir, int pairs, int ni, int nj, int nl,
+                         double nact, int mode, int *groups, int *items)
+{
+    if (!groups || nrhs < 0 || ndir < 0 || (nrhs > 0 && ndir > 0 && !ksc) || ni < 1 || nj < 1 || nl < 1 ||
+        mode < 0 || mode > 2)
+        return fail(DDAGPU_EINVAL, "bad far-field plan arguments");
+    KzPlan P;
+    plan_kz_groups(ksc, nrhs, ndir, pairs != 0, ni, nj, nl, nact, mode, P);
+    *groups = P.groups;
+    if (items) *items = P.groups ? P.items : 0;
+    return DDAGPU_OK;
+}
+
 int ddagpu_set_farfield_mode(ddagpu_ctx *c, int mode)
 {
     if (!c) return fail(DDAGPU_EINVAL, "null context");

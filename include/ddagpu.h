@@ -283,6 +283,14 @@ int ddagpu_set_fast_variant(ddagpu_ctx *ctx, int x_variant, int yz_variant);
  * sums fit in 1 GiB.  The two forms agree to FP32 rounding.  No counterpart in the
  * reference, whose sum is per direction. */
 int ddagpu_set_farfield_mode(ddagpu_ctx *ctx, int mode);
+
+/* How a far field of these directions is summed, without a device: ksc [nrhs][ndir][3]
+ * (pairs != 0: right-hand sides 2k, 2k+1 share theirs), lattice ni x nj x nl, nact active
+ * cells per right-hand side, mode as ddagpu_set_farfield_mode.  *groups receives the most
+ * distinct kz of a right-hand side (or pair) when the grouped form is chosen, else 0;
+ * *items (may be null) the most work items (at most 16 directions of one group each). */
+int ddagpu_farfield_plan(const double *ksc, int nrhs, int ndir, int pairs, int ni, int nj, int nl,
+                         double nact, int mode, int *groups, int *items);
 int ddagpu_get_fast_variant(ddagpu_ctx *ctx, int *x_variant, int *yz_variant);
 
 /* Self-test of the bounded device waits: on != 0 makes the bulk-copy x-pass variants
