@@ -174,3 +174,30 @@ def test_rectangular_batches_vs_oracle(D, oracle, grid, solver):
     M, Mo = r["mueller"].sum(axis=0).ravel(), o["mueller"].ravel()
     sig = np.abs(Mo) > 1e-3 * np.abs(Mo).max()
     assert (np.abs(M[sig] - Mo[sig]) / np.abs(Mo[sig])).max() < 1e-3
+
+
+def test_realizations_far_field_by_kz_groups(D, oracle):
+    """Realisations of different occupancies (fixed orientation, 12 scattering planes of 37
+    angles: 37 distinct kz, 12 directions each) with the far field by kz groups (mode 2,
+    each realisation's pair of right-hand sides reading its own occupancy) and by direction
+    (mode 1): equal to FP32 rounding, and each realisation against the FP64 sample loop."""
+    n, x = 16, 3.0
+    mats = [(1.5, 0.01), (1.7, 0.1)]
+    occs = targets(oracle, n)
+    cfg = D.BatchConfig(occ=None, materials=mats, nplanes=12, theta_step=5.0, err_max=1e-4,
+                        max_step=60)
+    res = {}
+    with D.Context(n, 2 * x / n, max_rhs=16) as ctx:
+        for mode in (1, 2):
+            ctx.set_farfield_mode(mode)
+            res[mode] = ctx.realization_solves(cfg, np.stack(occs))
+    for q in ("cabs", "cext"):
+        assert np.array_equal(res[1][q], res[2][q]) or \
+            (np.abs(res[1][q] - res[2][q]) / np.abs(res[1][q])).max() < 1e-6, q
+    M1, M2 = res[1]["mueller"], res[2]["mueller"]
+    sig = np.abs(M1) > 1e-3 * np.abs(M1).max()
+    assert (np.abs(M2 - M1)[sig] / np.abs(M1)[sig]).max() < 1e-5
+    for k, occ in enumerate(occs):
+        o = orientation_solves(oracle, n, x, mats, 1, occ=occ, nplanes=12, theta_step=5.0,
+                               err_max=1e-4, max_step=60)
+        check(res[2], k, o)
